@@ -1,0 +1,236 @@
+"""ctypes binding of the C-ABI in ``include/axhel_cuda.h``.
+
+Loads the in-tree ``axhel_b200/libaxhel.so`` (built by ``axhel_b200.build``)
+and raises if it is missing: there is no CPU fallback.  Data arguments are
+raw device addresses (``int``), e.g. ``torch.Tensor.data_ptr()``; streams are
+``cudaStream_t`` values as ``int`` (``torch.cuda.Stream.cuda_stream``) or 0.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libaxhel.so")
+
+u64 = C.c_uint64
+u32 = C.c_uint32
+vp = C.c_void_p
+st_t = C.c_int32
+
+OK = 0
+STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4: "unsupported", 5: "busy",
+          6: "timeout", 7: "rejected", 8: "cancelled"}
+
+
+class AxhelError(RuntimeError):
+    def __init__(self, status, where, msg):
+        super().__init__(f"{where}: {STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib():
+    """The loaded shared library (loaded once)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"AXHEL CUDA library not built: {LIB_PATH} (run python -m axhel_b200.build)")
+        L = C.CDLL(LIB_PATH)
+        _declare(L)
+        _lib = L
+    return _lib
+
+
+def _declare(L):
+    def d(name, res, *args):
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = list(args)
+
+    d("axhel_status_string", C.c_char_p, st_t)
+    d("axhel_last_error", C.c_char_p)
+    d("axhel_version", C.c_int)
+    d("axhel_cuda_ntt_create", st_t, u64, u64, u64, C.POINTER(vp))
+    d("axhel_cuda_ntt_create_external", st_t, u64, u64, vp, vp, vp, C.POINTER(vp))
+    d("axhel_cuda_ntt_retain", st_t, vp)
+    d("axhel_cuda_ntt_release", st_t, vp)
+    d("axhel_cuda_ntt_degree", u64, vp)
+    d("axhel_cuda_ntt_modulus", u64, vp)
+    d("axhel_cuda_ntt_read_tables", st_t, vp, vp, vp, vp)
+    d("axhel_cuda_ntt_forward", st_t, vp, vp, vp, u64, u64, vp)
+    d("axhel_cuda_ntt_inverse", st_t, vp, vp, vp, u64, u64, vp)
+    d("axhel_cuda_ntt_forward_batch", st_t, C.POINTER(vp), u64, vp, vp, u64, u64, u64, vp)
+    d("axhel_cuda_ntt_inverse_batch", st_t, C.POINTER(vp), u64, vp, vp, u64, u64, u64, vp)
+    d("axhel_cuda_ntt_chain_mul_batch", st_t, C.POINTER(vp), u64, vp, vp, vp, u64, u64, u64, vp)
+    d("axhel_cuda_ntt_chain_fma_batch", st_t, C.POINTER(vp), u64, vp, vp, vp, vp, u64, u64, u64, vp)
+    d("axhel_cuda_eltwise_add_vv", st_t, vp, vp, vp, u64, u64, vp)
+    d("axhel_cuda_eltwise_add_vs", st_t, vp, vp, u64, u64, u64, vp)
+    d("axhel_cuda_eltwise_sub_vv", st_t, vp, vp, vp, u64, u64, vp)
+    d("axhel_cuda_eltwise_sub_vs", st_t, vp, vp, u64, u64, u64, vp)
+    d("axhel_cuda_eltwise_mul", st_t, vp, vp, vp, u64, u64, u64, vp)
+    d("axhel_cuda_eltwise_fma", st_t, vp, vp, u64, vp, u64, u64, u64, vp)
+    d("axhel_cuda_eltwise_reduce", st_t, vp, vp, u64, u64, u64, u64, vp)
+    d("axhel_cuda_tensor_product", st_t, vp, vp, vp, vp, vp, vp, vp, u64, u64, vp, u64, u64, vp)
+    d("axhel_cuda_plan_set", st_t, C.c_int, u32, u32, vp, vp, vp)
+    d("axhel_cuda_plan_get", st_t, C.c_int, u32, u64, vp, vp, vp, vp)
+    d("axhel_cuda_plan_load", st_t, C.c_char_p, C.POINTER(u32))
+    d("axhel_cuda_is_device_pointer", C.c_int, vp)
+    d("axhel_cuda_launch_count", u64)
+    d("axhel_cuda_profile_enable", st_t, C.c_int)
+    d("axhel_cuda_profile_report", st_t, C.c_char_p, u64, C.POINTER(u64))
+
+
+def check(status, where):
+    if status != OK:
+        raise AxhelError(status, where, lib().axhel_last_error().decode())
+
+
+def launch_count():
+    return int(lib().axhel_cuda_launch_count())
+
+
+def profile_enable(on=True):
+    check(lib().axhel_cuda_profile_enable(1 if on else 0), "profile_enable")
+
+
+def profile_report():
+    """Drains the event records: {kernel configuration: (launches, total_ms)}."""
+    need = u64()
+    buf = C.create_string_buffer(1 << 16)
+    check(lib().axhel_cuda_profile_report(buf, len(buf), C.byref(need)), "profile_report")
+    out = {}
+    for line in buf.value.decode().splitlines():
+        parts = line.rsplit(" ", 2)
+        if len(parts) == 3:
+            out[parts[0]] = (int(parts[1]), float(parts[2]))
+    return out
+
+
+def _arr64(values):
+    a = (u64 * len(values))(*[int(v) for v in values])
+    return a
+
+
+class NTT:
+    """A device-resident (N, q) table context (``axhel_ntt_t``)."""
+
+    def __init__(self, degree, modulus, root=None, tables=None):
+        h = vp()
+        if tables is None:
+            check(lib().axhel_cuda_ntt_create(degree, modulus, root, C.byref(h)), "ntt_create")
+        else:
+            import numpy as np
+
+            fwd, inv, ninv = (np.ascontiguousarray(t, dtype=np.uint64) for t in tables)
+            check(lib().axhel_cuda_ntt_create_external(degree, modulus, fwd.ctypes.data, inv.ctypes.data,
+                                                       ninv.ctypes.data, C.byref(h)), "ntt_create_external")
+        self.h = h
+        self.degree = degree
+        self.modulus = modulus
+
+    def close(self):
+        if self.h:
+            lib().axhel_cuda_ntt_release(self.h)
+            self.h = vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def read_tables(self):
+        import numpy as np
+
+        fwd = np.zeros((self.degree, 2), np.uint64)
+        inv = np.zeros((self.degree, 2), np.uint64)
+        ninv = np.zeros(2, np.uint64)
+        check(lib().axhel_cuda_ntt_read_tables(self.h, fwd.ctypes.data, inv.ctypes.data, ninv.ctypes.data),
+              "read_tables")
+        return fwd, inv, ninv
+
+    def forward(self, dst, src, in_f=1, out_f=1, stream=0):
+        check(lib().axhel_cuda_ntt_forward(self.h, dst, src, in_f, out_f, stream), "ntt_forward")
+
+    def inverse(self, dst, src, in_f=1, out_f=1, stream=0):
+        check(lib().axhel_cuda_ntt_inverse(self.h, dst, src, in_f, out_f, stream), "ntt_inverse")
+
+
+def _handles(ntts):
+    return (vp * len(ntts))(*[t.h.value for t in ntts])
+
+
+def forward_batch(ntts, dst, src, count, in_f=1, out_f=1, stream=0):
+    check(lib().axhel_cuda_ntt_forward_batch(_handles(ntts), len(ntts), dst, src, count, in_f, out_f, stream),
+          "ntt_forward_batch")
+
+
+def inverse_batch(ntts, dst, src, count, in_f=1, out_f=1, stream=0):
+    check(lib().axhel_cuda_ntt_inverse_batch(_handles(ntts), len(ntts), dst, src, count, in_f, out_f, stream),
+          "ntt_inverse_batch")
+
+
+def chain_mul_batch(ntts, dst, src, multiplicand, count, in_f=2, out_f=1, stream=0):
+    check(lib().axhel_cuda_ntt_chain_mul_batch(_handles(ntts), len(ntts), dst, src, multiplicand, count, in_f, out_f,
+                                               stream), "ntt_chain_mul_batch")
+
+
+def chain_fma_batch(ntts, dst, src, scalars, addend, count, in_f=2, out_f=1, stream=0):
+    sc = _arr64(scalars)
+    check(lib().axhel_cuda_ntt_chain_fma_batch(_handles(ntts), len(ntts), dst, src, C.cast(sc, vp), addend, count,
+                                               in_f, out_f, stream), "ntt_chain_fma_batch")
+
+
+def add(dst, a, b, n, q, stream=0, scalar=False):
+    f = lib().axhel_cuda_eltwise_add_vs if scalar else lib().axhel_cuda_eltwise_add_vv
+    check(f(dst, a, b, n, q, stream), "eltwise_add")
+
+
+def sub(dst, a, b, n, q, stream=0, scalar=False):
+    f = lib().axhel_cuda_eltwise_sub_vs if scalar else lib().axhel_cuda_eltwise_sub_vv
+    check(f(dst, a, b, n, q, stream), "eltwise_sub")
+
+
+def mul(dst, a, b, n, q, factor, stream=0):
+    check(lib().axhel_cuda_eltwise_mul(dst, a, b, n, q, factor, stream), "eltwise_mul")
+
+
+def fma(dst, a, s, c, n, q, factor, stream=0):
+    check(lib().axhel_cuda_eltwise_fma(dst, a, s, c, n, q, factor, stream), "eltwise_fma")
+
+
+def reduce(dst, a, n, q, in_f, out_f, stream=0):
+    check(lib().axhel_cuda_eltwise_reduce(dst, a, n, q, in_f, out_f, stream), "eltwise_reduce")
+
+
+def tensor_product(r0, r1, r2, c0, c1, d0, d1, n, count, moduli, factor=1, stream=0):
+    m = _arr64(moduli)
+    check(lib().axhel_cuda_tensor_product(r0, r1, r2, c0, c1, d0, d1, n, count, C.cast(m, vp), len(moduli), factor,
+                                          stream), "tensor_product")
+
+
+def plan_set(inverse, logn, passes):
+    """passes: list of (lg, lr, tg); [] restores the default."""
+    n = len(passes)
+    lg = (u32 * 3)(*[p[0] for p in passes])
+    lr = (u32 * 3)(*[p[1] for p in passes])
+    tg = (u32 * 3)(*[p[2] for p in passes])
+    check(lib().axhel_cuda_plan_set(int(inverse), logn, n, C.cast(lg, vp), C.cast(lr, vp), C.cast(tg, vp)),
+          "plan_set")
+
+
+def plan_get(inverse, logn, count):
+    npass = u32()
+    lg, lr, tg = (u32 * 3)(), (u32 * 3)(), (u32 * 3)()
+    check(lib().axhel_cuda_plan_get(int(inverse), logn, count, C.byref(npass), C.cast(lg, vp), C.cast(lr, vp),
+                                    C.cast(tg, vp)), "plan_get")
+    return [(lg[i], lr[i], tg[i]) for i in range(npass.value)]
+
+
+def plan_load(path=None):
+    n = u32()
+    check(lib().axhel_cuda_plan_load(path.encode() if path else None, C.byref(n)), "plan_load")
+    return n.value

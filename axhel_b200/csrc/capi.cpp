@@ -1,0 +1,602 @@
+// C-ABI entry points (include/axhel_cuda.h): argument checking, the
+// device-resident NTT table cache, and pass sequencing for the transforms.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/axhel_cuda.h"
+#include "internal.h"
+#include "launch.h"
+
+using namespace axhel_impl;
+
+// ------------------------------------------------------------ bookkeeping
+
+namespace {
+
+thread_local std::string t_last_error;
+
+axhel_status_t fail(axhel_status_t st, const std::string& msg)
+{
+    t_last_error = msg;
+    return st;
+}
+
+axhel_status_t cuda_fail(cudaError_t e, const char* where)
+{
+    return fail(AXHEL_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+inline uint64_t bit_width(uint64_t x) { return x ? 64 - __builtin_clzll(x) : 0; }
+typedef unsigned __int128 u128;
+
+inline uint64_t shoup_quotient(uint64_t w, uint64_t q) { return (uint64_t)(((u128)w << 64) / q); }
+inline uint64_t shoup_lazy(uint64_t v, uint64_t w, uint64_t wq, uint64_t q)
+{
+    return v * w - (uint64_t)(((u128)v * wq) >> 64) * q;
+}
+inline uint64_t mulmod(uint64_t a, uint64_t b, uint64_t q) { return (uint64_t)(((u128)a * b) % q); }
+uint64_t powmod(uint64_t b, uint64_t e, uint64_t q)
+{
+    uint64_t r = 1;
+    b %= q;
+    while (e) {
+        if (e & 1) r = mulmod(r, b, q);
+        e >>= 1;
+        if (e) b = mulmod(b, b, q);
+    }
+    return r;
+}
+
+}  // namespace
+
+namespace axhel_impl {
+
+int sm_count()
+{
+    static int cache[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return 148;
+    if (!cache[dev]) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+        cache[dev] = n;
+    }
+    return cache[dev];
+}
+
+}  // namespace axhel_impl
+
+// -------------------------------------------------------- table contexts
+
+struct axhel_ntt_ctx {
+    std::atomic<int> refs{1};
+    uint64_t n = 0, q = 0, root = 0;
+    uint32_t logn = 0;
+    int device = 0;
+    bool cached = false;
+    void* mem = nullptr;          // device allocation: ModCtx | fwd[N] | inv[N]
+    const ModCtx* dctx = nullptr;  // device address of the ModCtx header
+};
+
+namespace {
+
+std::mutex g_cache_mu;
+std::map<std::tuple<int, uint64_t, uint64_t, uint64_t>, axhel_ntt_ctx*> g_cache;
+
+constexpr size_t kHeader = 256;  // ModCtx padded so the tables start 256-byte aligned
+
+// Builds the forward / inverse tables exactly as GenerateNTTTables
+// (axhel/ntt/ntt-tables.cpp:81-140): fwd[i] = psi^bitrev(i); inv[0] = 0,
+// inv[i] = psi^-(bitrev(i-1)+1); each with its Shoup quotient.
+void generate_tables(uint64_t n, uint32_t logn, uint64_t q, uint64_t psi, uint64_t* fwd, uint64_t* inv,
+                     uint64_t* ninv)
+{
+    std::vector<uint64_t> pw(n);
+    auto bitrev = [logn](uint64_t i) {
+        uint64_t r = 0;
+        for (uint32_t b = 0; b < logn; ++b) r |= ((i >> b) & 1) << (logn - 1 - b);
+        return r;
+    };
+    pw[0] = 1;
+    for (uint64_t i = 1; i < n; ++i) pw[i] = mulmod(pw[i - 1], psi, q);
+    for (uint64_t i = 0; i < n; ++i) {
+        const uint64_t w = pw[bitrev(i)];
+        fwd[2 * i] = w;
+        fwd[2 * i + 1] = shoup_quotient(w, q);
+    }
+    const uint64_t psi_inv = powmod(psi, q - 2, q);
+    for (uint64_t i = 1; i < n; ++i) pw[i] = mulmod(pw[i - 1], psi_inv, q);
+    inv[0] = inv[1] = 0;
+    for (uint64_t i = 1; i < n; ++i) {
+        const uint64_t w = pw[bitrev(i - 1) + 1];
+        inv[2 * i] = w;
+        inv[2 * i + 1] = shoup_quotient(w, q);
+    }
+    const uint64_t d = powmod(n % q, q - 2, q);
+    ninv[0] = d;
+    ninv[1] = shoup_quotient(d, q);
+}
+
+axhel_status_t upload(axhel_ntt_ctx* c, const uint64_t* fwd, const uint64_t* inv, const uint64_t* ninv)
+{
+    const size_t tab = c->n * 16;
+    const size_t total = kHeader + 2 * tab;
+    std::vector<unsigned char> img(total, 0);
+    cudaError_t e = cudaMalloc(&c->mem, total);
+    if (e != cudaSuccess) return fail(AXHEL_ERR_NOMEM, std::string("cudaMalloc(tables): ") + cudaGetErrorString(e));
+    unsigned char* base = static_cast<unsigned char*>(c->mem);
+    ModCtx h{};
+    h.q = c->q;
+    h.q2 = c->q << 1;
+    h.ninv = ninv[0];
+    h.ninv_q = ninv[1];
+    // scaled root of the final inverse stage (ntt-native.cpp:101-113)
+    uint64_t sr = shoup_lazy(inv[2 * (c->n - 1)], ninv[0], ninv[1], c->q);
+    if (sr >= c->q) sr -= c->q;
+    h.sroot = sr;
+    h.sroot_q = shoup_quotient(sr, c->q);
+    barrett_params(c->q, &h.mu, &h.shift);
+    h.logn = c->logn;
+    h.fwd = reinterpret_cast<const ulonglong2*>(base + kHeader);
+    h.inv = reinterpret_cast<const ulonglong2*>(base + kHeader + tab);
+    std::memcpy(img.data(), &h, sizeof h);
+    std::memcpy(img.data() + kHeader, fwd, tab);
+    std::memcpy(img.data() + kHeader + tab, inv, tab);
+    e = cudaMemcpy(c->mem, img.data(), total, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(c->mem);
+        c->mem = nullptr;
+        return cuda_fail(e, "cudaMemcpy(tables)");
+    }
+    c->dctx = reinterpret_cast<const ModCtx*>(base);
+    return AXHEL_OK;
+}
+
+axhel_status_t check_modulus(uint64_t q, uint64_t limit_bits)
+{
+    if (q < 2 || bit_width(q) > limit_bits)
+        return fail(AXHEL_ERR_INVALID, "modulus out of range (need 2 <= q < 2^" + std::to_string(limit_bits) + ")");
+    return AXHEL_OK;
+}
+
+axhel_status_t check_degree(uint64_t n, uint32_t* logn)
+{
+    if (n < AXHEL_MIN_DEGREE || n > AXHEL_MAX_DEGREE || (n & (n - 1)))
+        return fail(AXHEL_ERR_UNSUPPORTED, "degree must be a power of two in [2, 131072]");
+    uint32_t l = 0;
+    while ((1ull << l) < n) ++l;
+    *logn = l;
+    return AXHEL_OK;
+}
+
+inline cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
+
+}  // namespace
+
+extern "C" {
+
+const char* axhel_status_string(axhel_status_t st)
+{
+    switch (st) {
+    case AXHEL_OK: return "ok";
+    case AXHEL_ERR_INVALID: return "invalid argument";
+    case AXHEL_ERR_CUDA: return "CUDA error";
+    case AXHEL_ERR_NOMEM: return "out of memory";
+    case AXHEL_ERR_UNSUPPORTED: return "unsupported configuration";
+    case AXHEL_ERR_BUSY: return "busy";
+    case AXHEL_ERR_TIMEOUT: return "timeout";
+    case AXHEL_ERR_REJECTED: return "rejected";
+    case AXHEL_ERR_CANCELLED: return "cancelled";
+    default: return "unknown status";
+    }
+}
+
+const char* axhel_last_error(void) { return t_last_error.c_str(); }
+int axhel_version(void) { return 100; }
+
+int axhel_cuda_is_device_pointer(const void* p)
+{
+    if (!p) return 0;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+axhel_status_t axhel_cuda_ntt_create(uint64_t degree, uint64_t modulus, uint64_t root, axhel_ntt_t* out)
+{
+    if (!out) return fail(AXHEL_ERR_INVALID, "null output handle");
+    *out = nullptr;
+    uint32_t logn;
+    axhel_status_t st = check_degree(degree, &logn);
+    if (st) return st;
+    if ((st = check_modulus(modulus, 62))) return st;
+    if (root == 0 || root >= modulus) return fail(AXHEL_ERR_INVALID, "root of unity must be in [1, q)");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    auto key = std::make_tuple(dev, degree, modulus, root);
+    auto it = g_cache.find(key);
+    if (it != g_cache.end()) {
+        it->second->refs.fetch_add(1);
+        *out = it->second;
+        return AXHEL_OK;
+    }
+    auto c = std::make_unique<axhel_ntt_ctx>();
+    c->n = degree;
+    c->q = modulus;
+    c->root = root;
+    c->logn = logn;
+    c->device = dev;
+    c->cached = true;
+    std::vector<uint64_t> fwd(2 * degree), inv(2 * degree);
+    uint64_t ninv[2];
+    generate_tables(degree, logn, modulus, root, fwd.data(), inv.data(), ninv);
+    if ((st = upload(c.get(), fwd.data(), inv.data(), ninv))) return st;
+    c->refs.store(2);  // the cache keeps one reference: tables stay resident for the process
+    g_cache[key] = c.get();
+    *out = c.release();
+    return AXHEL_OK;
+}
+
+axhel_status_t axhel_cuda_ntt_create_external(uint64_t degree, uint64_t modulus, const uint64_t* fwd,
+                                              const uint64_t* inv, const uint64_t* ninv, axhel_ntt_t* out)
+{
+    if (!out) return fail(AXHEL_ERR_INVALID, "null output handle");
+    *out = nullptr;
+    uint32_t logn;
+    axhel_status_t st = check_degree(degree, &logn);
+    if (st) return st;
+    if ((st = check_modulus(modulus, 62))) return st;
+    if (!fwd || !inv || !ninv) return fail(AXHEL_ERR_INVALID, "null table pointer");
+    auto c = std::make_unique<axhel_ntt_ctx>();
+    c->n = degree;
+    c->q = modulus;
+    c->logn = logn;
+    cudaGetDevice(&c->device);
+    if ((st = upload(c.get(), fwd, inv, ninv))) return st;
+    *out = c.release();
+    return AXHEL_OK;
+}
+
+axhel_status_t axhel_cuda_ntt_retain(axhel_ntt_t h)
+{
+    if (!h) return fail(AXHEL_ERR_INVALID, "null handle");
+    h->refs.fetch_add(1);
+    return AXHEL_OK;
+}
+
+axhel_status_t axhel_cuda_ntt_release(axhel_ntt_t h)
+{
+    if (!h) return AXHEL_OK;
+    if (h->refs.fetch_sub(1) == 1) {
+        if (h->mem) cudaFree(h->mem);
+        delete h;
+    }
+    return AXHEL_OK;
+}
+
+uint64_t axhel_cuda_ntt_degree(axhel_ntt_t h) { return h ? h->n : 0; }
+uint64_t axhel_cuda_ntt_modulus(axhel_ntt_t h) { return h ? h->q : 0; }
+
+axhel_status_t axhel_cuda_ntt_read_tables(axhel_ntt_t h, uint64_t* fwd, uint64_t* inv, uint64_t* ninv)
+{
+    if (!h || !fwd || !inv || !ninv) return fail(AXHEL_ERR_INVALID, "null argument");
+    const unsigned char* base = static_cast<const unsigned char*>(h->mem);
+    cudaError_t e = cudaMemcpy(fwd, base + kHeader, h->n * 16, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(inv, base + kHeader + h->n * 16, h->n * 16, cudaMemcpyDeviceToHost);
+    ModCtx m;
+    if (e == cudaSuccess) e = cudaMemcpy(&m, base, sizeof m, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy(read tables)");
+    ninv[0] = m.ninv;
+    ninv[1] = m.ninv_q;
+    return AXHEL_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ transforms
+
+namespace {
+
+axhel_status_t collect(const axhel_ntt_t* ntts, uint64_t n_ntts, PassArgs& a, uint64_t* n_out)
+{
+    if (!ntts || n_ntts == 0) return fail(AXHEL_ERR_INVALID, "no NTT handles");
+    if (n_ntts > (uint64_t)kMaxInlineMods) return fail(AXHEL_ERR_UNSUPPORTED, "at most 64 moduli per batch");
+    const uint64_t n = ntts[0] ? ntts[0]->n : 0;
+    for (uint64_t i = 0; i < n_ntts; ++i) {
+        if (!ntts[i]) return fail(AXHEL_ERR_INVALID, "null NTT handle");
+        if (ntts[i]->n != n) return fail(AXHEL_ERR_INVALID, "all limbs of a batch need one degree");
+        a.ctx[i] = ntts[i]->dctx;
+    }
+    a.nctx = (uint32_t)n_ntts;
+    a.logn = ntts[0]->logn;
+    *n_out = n;
+    return AXHEL_OK;
+}
+
+// Runs the passes of `plan` in order; pass i reads `src` (first pass) or
+// `dst`, writes `dst`.
+axhel_status_t run_plan(bool inverse, const NttPlan& plan, PassArgs a, const uint64_t* src, uint64_t* dst,
+                        uint32_t first_flags, uint32_t last_flags, cudaStream_t s)
+{
+    uint32_t s0 = 0;
+    for (int i = 0; i < plan.npass; ++i) {
+        const PassCfg& c = plan.pass[i];
+        a.src = i == 0 ? src : dst;
+        a.dst = dst;
+        a.s0 = s0;
+        a.tg = (uint32_t)c.tg;
+        a.flags = (i == 0 ? first_flags : 0) | (i == plan.npass - 1 ? (last_flags | kLastPass) : 0);
+        cudaError_t e = launch_ntt_pass(inverse, c, a, s);
+        if (e != cudaSuccess) return cuda_fail(e, inverse ? "inverse NTT pass" : "forward NTT pass");
+        s0 += (uint32_t)c.lg;
+    }
+    return AXHEL_OK;
+}
+
+axhel_status_t transform(bool inverse, const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* result,
+                         const uint64_t* operand, uint64_t count, uint64_t in_f, uint64_t out_f, bool batch_api,
+                         void* stream)
+{
+    PassArgs a{};
+    uint64_t n;
+    axhel_status_t st = collect(ntts, n_ntts, a, &n);
+    if (st) return st;
+    if (count == 0) return AXHEL_OK;
+    if (!result || !operand) return fail(AXHEL_ERR_INVALID, "null data pointer");
+    a.count = count;
+    const NttPlan plan = plan_for(inverse, a.logn, count);
+    uint32_t first = 0, last = 0;
+    if (inverse) {
+        if (batch_api && in_f == 4) first |= kPreCsub2q;
+        if (out_f != 2) last |= kPostNorm;  // ntt.cpp:198-203
+    } else {
+        if (out_f != 4) last |= kPostNorm;  // ntt.cpp:180-185
+    }
+    return run_plan(inverse, plan, a, operand, result, first, last, S(stream));
+}
+
+axhel_status_t chain(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* result, const uint64_t* operand,
+                     const uint64_t* vec, const uint64_t* scalars, uint32_t op, uint64_t count, uint64_t in_f,
+                     uint64_t out_f, void* stream)
+{
+    ChainArgs c{};
+    uint64_t n;
+    axhel_status_t st = collect(ntts, n_ntts, c.pass, &n);
+    if (st) return st;
+    if (count == 0) return AXHEL_OK;
+    if (!result || !operand) return fail(AXHEL_ERR_INVALID, "null data pointer");
+    if (op == kChainMul && !vec) return fail(AXHEL_ERR_INVALID, "null multiplicand");
+    if (op == kChainFma && !scalars) return fail(AXHEL_ERR_INVALID, "null scalars");
+    c.pass.count = count;
+    const uint32_t logn = c.pass.logn;
+    const NttPlan inv = plan_for(true, logn, count);
+    // forward passes after the fused one: the inverse's earlier passes, reversed
+    NttPlan fwd{};
+    fwd.npass = inv.npass;
+    for (int i = 0; i < inv.npass; ++i) fwd.pass[i] = inv.pass[inv.npass - 1 - i];
+    cudaStream_t s = S(stream);
+    // inverse passes before the fused column pass
+    uint32_t s0 = 0;
+    const uint64_t* src = operand;
+    for (int i = 0; i + 1 < inv.npass; ++i) {
+        PassArgs a = c.pass;
+        a.src = src;
+        a.dst = result;
+        a.s0 = s0;
+        a.tg = (uint32_t)inv.pass[i].tg;
+        a.flags = (i == 0 && in_f == 4) ? kPreCsub2q : 0;
+        cudaError_t e = launch_ntt_pass(true, inv.pass[i], a, s);
+        if (e != cudaSuccess) return cuda_fail(e, "chain inverse pass");
+        s0 += (uint32_t)inv.pass[i].lg;
+        src = result;
+    }
+    // fused: inverse last pass -> op -> forward first pass
+    const PassCfg& fc = inv.pass[inv.npass - 1];
+    c.pass.src = src;
+    c.pass.dst = result;
+    c.pass.s0 = s0;
+    c.pass.tg = (uint32_t)fc.tg;
+    c.pass.flags = (inv.npass == 1 && in_f == 4 ? kPreCsub2q : 0) | (fwd.npass == 1 && out_f != 4 ? kPostNorm : 0);
+    c.operand = vec;
+    c.op = op;
+    c.op_factor = 2;
+    if (op == kChainFma)
+        for (uint64_t i = 0; i < n_ntts; ++i) c.scalar[i] = scalars[i];
+    cudaError_t e = launch_chain_pass(fc, c, s);
+    if (e != cudaSuccess) return cuda_fail(e, "chain fused pass");
+    // remaining forward passes
+    uint32_t f0 = (uint32_t)fc.lg;
+    for (int i = 1; i < fwd.npass; ++i) {
+        PassArgs a = c.pass;
+        a.src = result;
+        a.dst = result;
+        a.s0 = f0;
+        a.tg = (uint32_t)fwd.pass[i].tg;
+        a.flags = (i == fwd.npass - 1) ? (kLastPass | (out_f != 4 ? kPostNorm : 0)) : 0;
+        e = launch_ntt_pass(false, fwd.pass[i], a, s);
+        if (e != cudaSuccess) return cuda_fail(e, "chain forward pass");
+        f0 += (uint32_t)fwd.pass[i].lg;
+    }
+    return AXHEL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+axhel_status_t axhel_cuda_ntt_forward(axhel_ntt_t h, uint64_t* r, const uint64_t* x, uint64_t in_f, uint64_t out_f,
+                                      void* stream)
+{
+    return transform(false, &h, 1, r, x, 1, in_f, out_f, false, stream);
+}
+
+axhel_status_t axhel_cuda_ntt_inverse(axhel_ntt_t h, uint64_t* r, const uint64_t* x, uint64_t in_f, uint64_t out_f,
+                                      void* stream)
+{
+    return transform(true, &h, 1, r, x, 1, in_f, out_f, false, stream);
+}
+
+axhel_status_t axhel_cuda_ntt_forward_batch(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* r, const uint64_t* x,
+                                            uint64_t count, uint64_t in_f, uint64_t out_f, void* stream)
+{
+    return transform(false, ntts, n_ntts, r, x, count, in_f, out_f, true, stream);
+}
+
+axhel_status_t axhel_cuda_ntt_inverse_batch(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* r, const uint64_t* x,
+                                            uint64_t count, uint64_t in_f, uint64_t out_f, void* stream)
+{
+    return transform(true, ntts, n_ntts, r, x, count, in_f, out_f, true, stream);
+}
+
+axhel_status_t axhel_cuda_ntt_chain_mul_batch(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* r,
+                                              const uint64_t* x, const uint64_t* m, uint64_t count, uint64_t in_f,
+                                              uint64_t out_f, void* stream)
+{
+    return chain(ntts, n_ntts, r, x, m, nullptr, kChainMul, count, in_f, out_f, stream);
+}
+
+axhel_status_t axhel_cuda_ntt_chain_fma_batch(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* r,
+                                              const uint64_t* x, const uint64_t* scalars, const uint64_t* addend,
+                                              uint64_t count, uint64_t in_f, uint64_t out_f, void* stream)
+{
+    return chain(ntts, n_ntts, r, x, addend, scalars, kChainFma, count, in_f, out_f, stream);
+}
+
+// ------------------------------------------------------------- eltwise
+
+#define AXHEL_CHECK_PTRS(cond)                                                      \
+    do {                                                                             \
+        if (n == 0) return AXHEL_OK;                                                 \
+        if (!(cond)) return fail(AXHEL_ERR_INVALID, "null data pointer");            \
+    } while (0)
+
+#define AXHEL_RET(expr, what)                                 \
+    do {                                                      \
+        cudaError_t e_ = (expr);                              \
+        return e_ == cudaSuccess ? AXHEL_OK : cuda_fail(e_, what); \
+    } while (0)
+
+axhel_status_t axhel_cuda_eltwise_add_vv(uint64_t* r, const uint64_t* a, const uint64_t* b, uint64_t n, uint64_t q,
+                                         void* s)
+{
+    AXHEL_CHECK_PTRS(r && a && b);
+    if (axhel_status_t st = check_modulus(q, 63)) return st;
+    AXHEL_RET(eltwise_add(r, a, b, n, q, S(s)), "EltwiseAddMod");
+}
+axhel_status_t axhel_cuda_eltwise_add_vs(uint64_t* r, const uint64_t* a, uint64_t b, uint64_t n, uint64_t q, void* s)
+{
+    AXHEL_CHECK_PTRS(r && a);
+    if (axhel_status_t st = check_modulus(q, 63)) return st;
+    AXHEL_RET(eltwise_add_scalar(r, a, b, n, q, S(s)), "EltwiseAddMod");
+}
+axhel_status_t axhel_cuda_eltwise_sub_vv(uint64_t* r, const uint64_t* a, const uint64_t* b, uint64_t n, uint64_t q,
+                                         void* s)
+{
+    AXHEL_CHECK_PTRS(r && a && b);
+    if (axhel_status_t st = check_modulus(q, 63)) return st;
+    AXHEL_RET(eltwise_sub(r, a, b, n, q, S(s)), "EltwiseSubMod");
+}
+axhel_status_t axhel_cuda_eltwise_sub_vs(uint64_t* r, const uint64_t* a, uint64_t b, uint64_t n, uint64_t q, void* s)
+{
+    AXHEL_CHECK_PTRS(r && a);
+    if (axhel_status_t st = check_modulus(q, 63)) return st;
+    AXHEL_RET(eltwise_sub_scalar(r, a, b, n, q, S(s)), "EltwiseSubMod");
+}
+axhel_status_t axhel_cuda_eltwise_mul(uint64_t* r, const uint64_t* a, const uint64_t* b, uint64_t n, uint64_t q,
+                                      uint64_t f, void* s)
+{
+    AXHEL_CHECK_PTRS(r && a && b);
+    if (axhel_status_t st = check_modulus(q, 62)) return st;
+    AXHEL_RET(eltwise_mul(r, a, b, n, q, f, S(s)), "EltwiseMulMod");
+}
+axhel_status_t axhel_cuda_eltwise_fma(uint64_t* r, const uint64_t* a, uint64_t sc, const uint64_t* c, uint64_t n,
+                                      uint64_t q, uint64_t f, void* s)
+{
+    AXHEL_CHECK_PTRS(r && a);
+    if (axhel_status_t st = check_modulus(q, 62)) return st;
+    AXHEL_RET(eltwise_fma(r, a, sc, c, n, q, f, S(s)), "EltwiseFMAMod");
+}
+axhel_status_t axhel_cuda_eltwise_reduce(uint64_t* r, const uint64_t* a, uint64_t n, uint64_t q, uint64_t in_f,
+                                         uint64_t out_f, void* s)
+{
+    AXHEL_CHECK_PTRS(r && a);
+    if (axhel_status_t st = check_modulus(q, 62)) return st;
+    AXHEL_RET(eltwise_reduce(r, a, n, q, in_f, out_f, S(s)), "EltwiseReduceMod");
+}
+
+axhel_status_t axhel_cuda_tensor_product(uint64_t* r0, uint64_t* r1, uint64_t* r2, const uint64_t* c0,
+                                         const uint64_t* c1, const uint64_t* d0, const uint64_t* d1, uint64_t n,
+                                         uint64_t count, const uint64_t* moduli, uint64_t n_moduli,
+                                         uint64_t mod_factor, void* s)
+{
+    if (n == 0 || count == 0) return AXHEL_OK;
+    if (!r0 || !r1 || !r2 || !c0 || !c1 || !d0 || !d1 || !moduli) return fail(AXHEL_ERR_INVALID, "null pointer");
+    if (n_moduli == 0 || n_moduli > (uint64_t)kMaxInlineMods) return fail(AXHEL_ERR_UNSUPPORTED, "1..64 moduli");
+    if (n & 1) return fail(AXHEL_ERR_UNSUPPORTED, "limb length must be even");
+    if (mod_factor != 1 && mod_factor != 2 && mod_factor != 4) return fail(AXHEL_ERR_INVALID, "mod_factor 1, 2 or 4");
+    const uintptr_t al = (uintptr_t)r0 | (uintptr_t)r1 | (uintptr_t)r2 | (uintptr_t)c0 | (uintptr_t)c1 |
+                         (uintptr_t)d0 | (uintptr_t)d1;
+    if (al & 15) return fail(AXHEL_ERR_INVALID, "tensor product buffers must be 16-byte aligned");
+    if (count > 65535) return fail(AXHEL_ERR_UNSUPPORTED, "at most 65535 limbs per call");
+    for (uint64_t i = 0; i < n_moduli; ++i)
+        if (axhel_status_t st = check_modulus(moduli[i], 62)) return st;
+    AXHEL_RET(tensor_product(r0, r1, r2, c0, c1, d0, d1, n, count, moduli, n_moduli, mod_factor, S(s)),
+              "tensor product");
+}
+
+// --------------------------------------------------------------- plans
+
+axhel_status_t axhel_cuda_plan_set(int inverse, uint32_t logn, uint32_t npass, const uint32_t* lg, const uint32_t* lr,
+                                   const uint32_t* tg)
+{
+    if (npass == 0) {
+        plan_override(inverse != 0, logn, nullptr);
+        return AXHEL_OK;
+    }
+    if (npass > 3 || !lg || !lr || !tg) return fail(AXHEL_ERR_INVALID, "bad plan");
+    NttPlan p{};
+    p.npass = (int)npass;
+    for (uint32_t i = 0; i < npass; ++i) p.pass[i] = PassCfg{(int)lg[i], (int)lr[i], (int)tg[i]};
+    if (!plan_valid(p, logn, inverse != 0)) return fail(AXHEL_ERR_UNSUPPORTED, "plan not valid for this degree");
+    plan_override(inverse != 0, logn, &p);
+    return AXHEL_OK;
+}
+
+axhel_status_t axhel_cuda_plan_get(int inverse, uint32_t logn, uint64_t count, uint32_t* npass, uint32_t* lg,
+                                   uint32_t* lr, uint32_t* tg)
+{
+    if (!npass || !lg || !lr || !tg) return fail(AXHEL_ERR_INVALID, "null output");
+    if (logn < 1 || logn > 17) return fail(AXHEL_ERR_UNSUPPORTED, "log degree out of range");
+    const NttPlan p = plan_for(inverse != 0, logn, count);
+    *npass = (uint32_t)p.npass;
+    for (int i = 0; i < p.npass; ++i) {
+        lg[i] = (uint32_t)p.pass[i].lg;
+        lr[i] = (uint32_t)p.pass[i].lr;
+        tg[i] = (uint32_t)p.pass[i].tg;
+    }
+    return AXHEL_OK;
+}
+
+axhel_status_t axhel_cuda_plan_load(const char* path, uint32_t* loaded)
+{
+    const int n = plan_load(path);
+    if (loaded) *loaded = n < 0 ? 0 : (uint32_t)n;
+    if (n < 0) return fail(AXHEL_ERR_INVALID, "cannot open plan table");
+    return AXHEL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,236 @@
+// The unipi::axhel C++ drop-in (include/axhel/*.hpp), implemented on the
+// C-ABI (include/axhel_cuda.h).
+//
+// Same signatures and semantics as the reference public API: calls are
+// synchronous (results are visible on return), result may alias the
+// operands, n == 0 is a no-op, and unsupported mod-factors leave the result
+// untouched.  Pointers may be host memory (the reference's and SEAL's usage:
+// operands are staged through per-thread device buffers) or device memory
+// (used in place, no copies).  Each host thread issues its work on its own
+// per-thread default stream, so const NTT objects shared between threads (as
+// SEAL's process-wide cache does) are safe to use concurrently.
+// CUDA failures throw std::runtime_error: there is no CPU fallback.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/axhel/axhel.hpp"
+#include "../../include/axhel_cuda.h"
+
+namespace unipi {
+namespace axhel {
+
+namespace {
+
+void check(axhel_status_t st, const char* what)
+{
+    if (st != AXHEL_OK) throw std::runtime_error(std::string("AXHEL ") + what + ": " + axhel_last_error());
+}
+
+void check_cuda(cudaError_t e, const char* what)
+{
+    if (e != cudaSuccess) throw std::runtime_error(std::string("AXHEL ") + what + ": " + cudaGetErrorString(e));
+}
+
+inline cudaStream_t stream() { return cudaStreamPerThread; }
+
+// Growable per-thread device staging buffers (one per operand slot).
+struct Staging {
+    uint64_t* buf[4] = {nullptr, nullptr, nullptr, nullptr};
+    size_t cap[4] = {0, 0, 0, 0};
+    ~Staging()
+    {
+        for (auto* p : buf)
+            if (p) cudaFree(p);
+    }
+    uint64_t* get(int slot, size_t words)
+    {
+        if (cap[slot] < words) {
+            if (buf[slot]) cudaFree(buf[slot]);
+            buf[slot] = nullptr;
+            cap[slot] = 0;
+            check_cuda(cudaMalloc(&buf[slot], words * sizeof(uint64_t)), "staging allocation");
+            cap[slot] = words;
+        }
+        return buf[slot];
+    }
+};
+thread_local Staging t_staging;
+
+// Device view of an input operand: the pointer itself if it is device
+// memory, else a staged copy.
+const uint64_t* input(const uint64_t* p, uint64_t n, int slot)
+{
+    if (!p || axhel_cuda_is_device_pointer(p)) return p;
+    uint64_t* d = t_staging.get(slot, n);
+    check_cuda(cudaMemcpyAsync(d, p, n * sizeof(uint64_t), cudaMemcpyHostToDevice, stream()), "host to device copy");
+    return d;
+}
+
+// Device destination for `result` (itself, or staging slot 3).
+struct Output {
+    uint64_t* host = nullptr;
+    uint64_t* dev = nullptr;
+    uint64_t n = 0;
+    Output(uint64_t* r, uint64_t count) : n(count)
+    {
+        if (axhel_cuda_is_device_pointer(r)) {
+            dev = r;
+        } else {
+            host = r;
+            dev = t_staging.get(3, count);
+        }
+    }
+    void finish()
+    {
+        if (host)
+            check_cuda(cudaMemcpyAsync(host, dev, n * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream()),
+                       "device to host copy");
+        check_cuda(cudaStreamSynchronize(stream()), "stream synchronize");
+    }
+};
+
+}  // namespace
+
+// --------------------------------------------------------------- eltwise
+
+void EltwiseAddMod(uint64_t* result, const uint64_t* operand1, const uint64_t* operand2, uint64_t n, uint64_t modulus)
+{
+    if (n == 0) return;
+    Output out(result, n);
+    const uint64_t* a = input(operand1, n, 0);
+    const uint64_t* b = input(operand2, n, 1);
+    check(axhel_cuda_eltwise_add_vv(out.dev, a, b, n, modulus, stream()), "EltwiseAddMod");
+    out.finish();
+}
+
+void EltwiseAddMod(uint64_t* result, const uint64_t* operand1, uint64_t operand2, uint64_t n, uint64_t modulus)
+{
+    if (n == 0) return;
+    Output out(result, n);
+    const uint64_t* a = input(operand1, n, 0);
+    check(axhel_cuda_eltwise_add_vs(out.dev, a, operand2, n, modulus, stream()), "EltwiseAddMod");
+    out.finish();
+}
+
+void EltwiseSubMod(uint64_t* result, const uint64_t* operand1, const uint64_t* operand2, uint64_t n, uint64_t modulus)
+{
+    if (n == 0) return;
+    Output out(result, n);
+    const uint64_t* a = input(operand1, n, 0);
+    const uint64_t* b = input(operand2, n, 1);
+    check(axhel_cuda_eltwise_sub_vv(out.dev, a, b, n, modulus, stream()), "EltwiseSubMod");
+    out.finish();
+}
+
+void EltwiseSubMod(uint64_t* result, const uint64_t* operand1, uint64_t operand2, uint64_t n, uint64_t modulus)
+{
+    if (n == 0) return;
+    Output out(result, n);
+    const uint64_t* a = input(operand1, n, 0);
+    check(axhel_cuda_eltwise_sub_vs(out.dev, a, operand2, n, modulus, stream()), "EltwiseSubMod");
+    out.finish();
+}
+
+void EltwiseMulMod(uint64_t* result, const uint64_t* operand1, const uint64_t* operand2, uint64_t n, uint64_t modulus,
+                   uint64_t mod_factor)
+{
+    if (n == 0 || (mod_factor != 1 && mod_factor != 2 && mod_factor != 4)) return;  // eltwise-mul-mod.cpp:83-93
+    Output out(result, n);
+    const uint64_t* a = input(operand1, n, 0);
+    const uint64_t* b = input(operand2, n, 1);
+    check(axhel_cuda_eltwise_mul(out.dev, a, b, n, modulus, mod_factor, stream()), "EltwiseMulMod");
+    out.finish();
+}
+
+void EltwiseFMAMod(uint64_t* res, const uint64_t* op1, uint64_t op2, const uint64_t* op3, uint64_t n, uint64_t mod,
+                   uint64_t mod_factor)
+{
+    if (n == 0 || (mod_factor != 1 && mod_factor != 2 && mod_factor != 4 && mod_factor != 8)) return;
+    Output out(res, n);
+    const uint64_t* a = input(op1, n, 0);
+    const uint64_t* c = input(op3, n, 1);
+    check(axhel_cuda_eltwise_fma(out.dev, a, op2, c, n, mod, mod_factor, stream()), "EltwiseFMAMod");
+    out.finish();
+}
+
+void EltwiseReduceMod(uint64_t* res, const uint64_t* op, uint64_t n, uint64_t mod, uint64_t in_mod_factor,
+                      uint64_t out_mod_factor)
+{
+    if (n == 0) return;
+    Output out(res, n);
+    const bool matched = in_mod_factor == 1 || (out_mod_factor == 2 && in_mod_factor <= 2) ||
+                         (in_mod_factor == 2 && out_mod_factor == 1) ||
+                         (in_mod_factor == 4 && (out_mod_factor == 1 || out_mod_factor == 2)) ||
+                         in_mod_factor == mod;
+    if (!matched) return;  // eltwise-reduce-mod.cpp:32-128: an unmatched pair writes nothing
+    const uint64_t* a = input(op, n, 0);
+    check(axhel_cuda_eltwise_reduce(out.dev, a, n, mod, in_mod_factor, out_mod_factor, stream()), "EltwiseReduceMod");
+    out.finish();
+}
+
+// ------------------------------------------------------------------ NTT
+
+class NTT::Impl {
+public:
+    uint64_t degree{0};
+    uint64_t modulus{0};
+    axhel_ntt_t handle{nullptr};
+    ~Impl() { axhel_cuda_ntt_release(handle); }
+};
+
+NTT::NTT(uint64_t degree, uint64_t modulus, uint64_t root_of_unity) : impl_(std::make_shared<Impl>())
+{
+    impl_->degree = degree;
+    impl_->modulus = modulus;
+    check(axhel_cuda_ntt_create(degree, modulus, root_of_unity, &impl_->handle), "NTT tables");
+}
+
+NTT::NTT(uint64_t degree, uint64_t modulus, const NTTMultiplyOperand* root_powers,
+         const NTTMultiplyOperand* inv_root_powers, NTTMultiplyOperand inv_degree_modulo)
+    : impl_(std::make_shared<Impl>())
+{
+    static_assert(sizeof(NTTMultiplyOperand) == 16, "NTTMultiplyOperand layout");
+    impl_->degree = degree;
+    impl_->modulus = modulus;
+    const uint64_t ninv[2] = {inv_degree_modulo.operand, inv_degree_modulo.quotient};
+    check(axhel_cuda_ntt_create_external(degree, modulus, reinterpret_cast<const uint64_t*>(root_powers),
+                                         reinterpret_cast<const uint64_t*>(inv_root_powers), ninv, &impl_->handle),
+          "NTT external tables");
+}
+
+NTT::~NTT() = default;
+NTT::NTT(const NTT&) noexcept = default;
+NTT& NTT::operator=(const NTT&) noexcept = default;
+NTT::NTT(NTT&&) noexcept = default;
+NTT& NTT::operator=(NTT&&) noexcept = default;
+
+void NTT::ComputeForward(uint64_t* result, const uint64_t* operand, uint64_t input_mod_factor,
+                         uint64_t output_mod_factor) const
+{
+    const uint64_t n = impl_->degree;
+    Output out(result, n);
+    const uint64_t* a = input(operand, n, 0);
+    check(axhel_cuda_ntt_forward(impl_->handle, out.dev, a, input_mod_factor, output_mod_factor, stream()),
+          "ComputeForward");
+    out.finish();
+}
+
+void NTT::ComputeInverse(uint64_t* result, const uint64_t* operand, uint64_t input_mod_factor,
+                         uint64_t output_mod_factor) const
+{
+    const uint64_t n = impl_->degree;
+    Output out(result, n);
+    const uint64_t* a = input(operand, n, 0);
+    check(axhel_cuda_ntt_inverse(impl_->handle, out.dev, a, input_mod_factor, output_mod_factor, stream()),
+          "ComputeInverse");
+    out.finish();
+}
+
+uint64_t NTT::Degree() const noexcept { return impl_ ? impl_->degree : 0; }
+uint64_t NTT::Modulus() const noexcept { return impl_ ? impl_->modulus : 0; }
+
+}  // namespace axhel
+}  // namespace unipi

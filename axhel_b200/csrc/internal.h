@@ -1,0 +1,84 @@
+// Internal declarations shared by the CUDA kernels, the C-ABI layer and the
+// C++ drop-in.  Nothing here is part of the public interface.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include "../../include/axhel_cuda.h"
+
+namespace axhel_impl {
+
+// Device-resident constants of one (N, q) transform context; the twiddle
+// tables follow it in the same allocation.  One per distinct (N, q, tables).
+struct ModCtx {
+    uint64_t q, q2;
+    uint64_t ninv, ninv_q;    // N^-1 mod q and its Shoup quotient
+    uint64_t sroot, sroot_q;  // reduce2->1(Shoup(inv[N-1], N^-1)) and quotient (ntt-native.cpp:109-113)
+    uint64_t mu;              // Barrett factor floor(2^(k+62)/q), k = BitWidth(q)
+    uint32_t shift;           // k - 2
+    uint32_t logn;
+    const ulonglong2* fwd;    // N entries {w, floor(w 2^64 / q)}, bit-reversed (ntt-tables.cpp:96-106)
+    const ulonglong2* inv;    // N entries, inverse order (ntt-tables.cpp:113-129)
+};
+static_assert(sizeof(ModCtx) == 80, "ModCtx layout");
+
+constexpr int kMaxInlineMods = 64;
+
+// Pass-level flags, uniform per launch.
+enum PassFlags : uint32_t {
+    kPreCsub2q = 1u,     // x <- csub(x, 2q) on load (fuses EltwiseReduceMod 4->2 ahead of an inverse)
+    kPostNorm = 2u,      // forward: 4->1 after the last stage; inverse: 2->1 after the final stage
+    kLastPass = 4u,      // this pass holds global stage logN-1 (inverse: runs the N^-1 final stage)
+};
+
+// Geometry of one pass: stages [s0, s0 + lg) of an N = 2^logn transform, on
+// `count` limbs stored back to back (limb stride = N words).  Limb i uses
+// ctx[i % nctx].
+struct PassArgs {
+    const uint64_t* src;
+    uint64_t* dst;
+    uint64_t count;
+    uint32_t logn, s0, tg, flags;
+    uint32_t nctx;
+    const ModCtx* ctx[kMaxInlineMods];
+};
+
+// Chain operation applied between the inverse and the forward transform of a
+// fused INTT -> op -> NTT job (per element at natural-order position p).
+enum ChainOp : uint32_t { kChainNone = 0, kChainMul = 1, kChainFma = 2 };
+
+struct ChainArgs {
+    PassArgs pass;                // geometry of the shared column pass (inverse last pass == forward first pass)
+    const uint64_t* operand;      // MulMod operand / FMA addend, laid out like the data (count x N), may be null for FMA
+    const uint64_t* scalars;      // FMA scalar per modulus context (nctx entries, host-visible copy inlined below)
+    uint64_t scalar[kMaxInlineMods];
+    uint32_t op, op_factor;       // ChainOp and the MulMod/FMAMod input mod_factor
+};
+
+// One pass configuration chosen by the planner / autotuner.
+struct PassCfg {
+    int lg, lr, tg;
+};
+struct NttPlan {
+    int npass;
+    PassCfg pass[3];
+};
+
+// Kernel launchers (ntt.cu / eltwise.cu).  All return cudaError_t of launch.
+cudaError_t launch_ntt_pass(bool inverse, const PassCfg& cfg, const PassArgs& a, cudaStream_t s);
+cudaError_t launch_chain_pass(const PassCfg& inv_cfg, const ChainArgs& a, cudaStream_t s);
+bool pass_supported(const PassCfg& cfg);
+
+// Planner (plan.cpp): default plan for (dir, logN, limbs); autotuned table if loaded.
+NttPlan plan_for(bool inverse, uint32_t logn, uint64_t limbs);
+bool plan_valid(const NttPlan& p, uint32_t logn, bool inverse);
+int plan_load(const char* path);
+void plan_override(bool inverse, uint32_t logn, const NttPlan* p);  // nullptr clears
+
+// Host table generation (tables.cpp): restates axhel/ntt/ntt-tables.cpp:81-140.
+struct HostTables;
+}  // namespace axhel_impl

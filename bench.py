@@ -1,0 +1,411 @@
+#!/usr/bin/env python
+"""Benchmark: batched NTT+INTT limb-transforms/s at N = 2^16.
+
+Workload (one step, per GPU): 16 ciphertexts x 2 polynomials x 24 RNS limbs =
+768 limbs of N = 65536 residues (50..59-bit primes q = 1 mod 2N from a
+deterministic search; residues uniform in [0, q), seeded).  A step is the
+reference's lazy round trip on every limb,
+    ComputeForward(1, 4) -> EltwiseReduceMod(4, 2) -> ComputeInverse(2, 1),
+run as two batched C-ABI calls (forward_batch, inverse_batch with the 4->2
+reduce fused on load): 1536 limb-transforms.  Inputs (384 MiB) exceed the
+126 MB L2, so no flush is needed between steps.
+
+Prints one JSON line (rank 0).  `--impl reference` times the reference's own
+CPU implementation (oracle/_ref, compiled from the reference sources) on the
+same workload and metric.  Multi-GPU (torchrun): every rank runs its own 768
+limbs (weak scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 1 << 16
+LIMBS = 24
+CIPHERTEXTS = 16
+POLYS = 2
+COUNT = CIPHERTEXTS * POLYS * LIMBS  # 768 limbs per GPU
+SEED = 0x415848454C
+METRIC = "batched NTT+INTT limb-transforms/s at N=2^16"
+UNIT = "limb-transforms/s"
+HBM_FALLBACK = 6650.0
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK, "fallback"
+
+
+def workload_moduli():
+    from axhel_b200 import params
+
+    return params.rns_moduli(N, LIMBS, 50, 59)
+
+
+def make_inputs(mods, count=COUNT, seed=SEED):
+    rng = np.random.default_rng(seed)
+    qs = np.array([q for q, _ in mods], dtype=np.uint64)
+    out = np.empty((count, N), np.uint64)
+    for i in range(count):
+        out[i] = rng.integers(0, qs[i % len(qs)], N, dtype=np.uint64)
+    return out
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons on one GPU (NVML) while running."""
+
+    REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+               0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
+
+    def __init__(self, index, period=0.01):
+        self.index, self.period = index, period
+        self.samples, self.reasons = [], set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+
+            def run():
+                while not self._stop.is_set():
+                    try:
+                        self.samples.append(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                        r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        for bit, name in self.REASONS.items():
+                            if r & bit and bit != 0x1:
+                                self.reasons.add(name)
+                    except Exception:
+                        pass
+                    time.sleep(self.period)
+
+            self._t = threading.Thread(target=run, daemon=True)
+            self._t.start()
+        except Exception:
+            self._t = None
+        return self
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join()
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------------ distributed
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ------------------------------------------------------------------ CPU reference
+
+def reference_roundtrip_rate(mods, data, threads, target_s):
+    """Times the reference native backend (oracle/_ref) on a bounded sample of
+    the workload: the lazy round trip on S limbs over `threads` host threads.
+    Returns (limb-transforms/s, S, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from pyoracle import Reference
+
+    ref = Reference()
+    ntts = [ref.ntt(N, q, psi) for q, psi in mods]
+    # calibrate: one limb per thread
+    s0 = max(threads, 1)
+    buf = np.ascontiguousarray(data[:s0])
+    t = time.perf_counter()
+    ref.roundtrip_batch(ntts, buf, N, s0, threads)
+    dt = max(time.perf_counter() - t, 1e-4)
+    per_limb = dt / s0
+    S = int(min(len(data), max(threads, round(target_s / per_limb / threads) * threads)))
+    buf = np.ascontiguousarray(data[:S])
+    t = time.perf_counter()
+    ref.roundtrip_batch(ntts, buf, N, S, threads)
+    dt = time.perf_counter() - t
+    if not np.array_equal(buf, data[:S]):
+        raise RuntimeError("reference round trip did not reproduce its input")
+    return 2 * S / dt, S, dt
+
+
+def run_reference(args):
+    world, rank, local = dist_init()
+    if rank != 0:
+        return 0
+    mods = workload_moduli()
+    threads = len(os.sched_getaffinity(0))
+    data = make_inputs(mods, COUNT)
+    # size each step so the whole run stays within ~2 minutes
+    budget = min(10.0, 120.0 / max(1, args.steps + args.warmup))
+    _, S, _ = reference_roundtrip_rate(mods, data, threads, budget)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from pyoracle import Reference
+
+    ref = Reference()
+    ntts = [ref.ntt(N, q, psi) for q, psi in mods]
+    buf = np.ascontiguousarray(data[:S])
+    for _ in range(args.warmup):
+        ref.roundtrip_batch(ntts, buf, N, S, threads)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        ref.roundtrip_batch(ntts, buf, N, S, threads)
+    dt = time.perf_counter() - t
+    value = 2 * S * args.steps / dt
+    sample = f"{S} of the {COUNT} limbs per step (N=2^16, 24 primes), lazy round trip per limb"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": "batched RNS NTT+INTT round trip, N=2^16, 24 limbs x 16 ciphertexts x 2 polys",
+                   "limbs_per_step": S, "threads": threads},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ GPU arm
+
+def run_ours(args):
+    import torch
+
+    from axhel_b200 import capi
+
+    world, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        pg = dist
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+
+    mods = workload_moduli()
+    ntts = [capi.NTT(N, q, psi) for q, psi in mods]
+    data = make_inputs(mods, COUNT, SEED + rank)
+    x = torch.from_numpy(data.reshape(-1).view(np.int64)).to(dev)
+    y = torch.empty_like(x)
+    xp, yp = x.data_ptr(), y.data_ptr()
+
+    def step():
+        capi.forward_batch(ntts, yp, xp, COUNT, 1, 4, sh)
+        capi.inverse_batch(ntts, yp, yp, COUNT, 4, 1, sh)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    if not torch.equal(x, y):
+        raise RuntimeError("round trip mismatch before timing")
+
+    # ---- timed region (device time, CUDA events on the launching stream)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local).start()
+    l0 = capi.launch_count()
+    capi.profile_enable(True)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    capi.profile_enable(False)
+    launches = capi.launch_count() - l0
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    prof = capi.profile_report()
+    if pg:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+        pg.barrier()
+    if not torch.equal(x, y):
+        raise RuntimeError("round trip mismatch after timing")
+    value = world * 2 * COUNT * args.steps / (ms / 1e3)
+
+    # ---- dominant kernel roofline (algorithmic bytes: each pass reads and
+    # writes every limb once -> 16 * N * COUNT bytes per launch)
+    peak, peak_kind = peaks()
+    dom = max(prof.items(), key=lambda kv: kv[1][1]) if prof else None
+    roofline = None
+    if dom:
+        name, (cnt, tot) = dom
+        alg = 16 * N * COUNT
+        avg_s = tot / cnt / 1e3
+        achieved = alg / avg_s / 1e9
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+        if os.path.exists(tpath):
+            with open(tpath) as f:
+                traffic = json.load(f).get(name)
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": traffic, "kernel": name, "launches": cnt, "avg_launch_ms": tot / cnt,
+                    "alg_bytes_per_launch": alg, "peak_source": f"{peak_kind} hbm_gbs",
+                    "share": tot / sum(v[1] for v in prof.values())}
+
+    # ---- plain per-limb drop-in on the same device data (one call per limb
+    # per operation, as the reference API is used), for the batching speed-up
+    plain = plain_per_limb(capi, ntts, x, y, sh, limbs=min(COUNT, 768))
+
+    # ---- e2e through the C-ABI with pinned host buffers, copies inside the timed region
+    e2e = end_to_end(capi, ntts, data, dev, steps=max(1, min(args.steps, 10)))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            threads = len(os.sched_getaffinity(0))
+            rate, S, secs = reference_roundtrip_rate(mods, data, threads, args.cpu_seconds)
+            cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"{S} limbs of the N=2^16 workload, lazy round trip, {secs:.1f} s"}
+        except Exception as e:  # the reference build is test infrastructure; report its absence
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": "batched RNS NTT+INTT round trip, N=2^16, 24 limbs x 16 ciphertexts x 2 polys "
+                                   "(768 limbs per GPU, 1536 limb-transforms per step)",
+                       "limbs_per_gpu": COUNT, "degree": N, "moduli": "24 primes of 50-59 bits",
+                       "l2": "inputs 384 MiB > 126 MB L2, no flush",
+                       "parallelism": f"{world} independent GPU(s), no data-path collective"},
+            "gpu_launches": launches,
+            "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+            "roofline": roofline,
+            "plain_per_limb": plain,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
+def plain_per_limb(capi, ntts, x, y, sh, limbs):
+    """The reference's call pattern on the GPU drop-in: for each limb,
+    ComputeForward(1,4), EltwiseReduceMod(4,2), ComputeInverse(2,1) as three
+    separate C-ABI calls on device-resident data."""
+    import torch
+
+    L = len(ntts)
+
+    def run():
+        for i in range(limbs):
+            off = 8 * N * i
+            t = ntts[i % L]
+            t.forward(y.data_ptr() + off, x.data_ptr() + off, 1, 4, sh)
+            capi.reduce(y.data_ptr() + off, y.data_ptr() + off, N, t.modulus, 4, 2, sh)
+            t.inverse(y.data_ptr() + off, y.data_ptr() + off, 2, 1, sh)
+
+    run()
+    torch.cuda.synchronize()
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    run()
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    ok = torch.equal(x[: limbs * N], y[: limbs * N])
+    return {"value": 2 * limbs / (ms / 1e3), "unit": UNIT, "limbs": limbs, "ms": ms, "bitexact_roundtrip": ok,
+            "calls_per_limb": 3}
+
+
+def end_to_end(capi, ntts, data, dev, steps, chunks=8):
+    """Same metric through the C-ABI from pinned HOST memory: per step, every
+    chunk of limbs is copied host->device, transformed (forward, inverse) and
+    copied back, pipelined over 3 streams.  Timed with CUDA events."""
+    import torch
+
+    flat = data.reshape(-1)
+    hin = torch.from_numpy(flat.view(np.int64)).pin_memory()
+    hout = torch.empty_like(hin).pin_memory()
+    dbuf = torch.empty(hin.numel(), dtype=torch.int64, device=dev)
+    per = COUNT // chunks
+    assert per % LIMBS == 0
+    streams = [torch.cuda.Stream(dev) for _ in range(3)]
+    main = torch.cuda.current_stream(dev)
+
+    def one_step():
+        for c in range(chunks):
+            s = streams[c % len(streams)]
+            lo, hi = c * per * N, (c + 1) * per * N
+            with torch.cuda.stream(s):
+                dbuf[lo:hi].copy_(hin[lo:hi], non_blocking=True)
+                p = dbuf.data_ptr() + 8 * lo
+                capi.forward_batch(ntts, p, p, per, 1, 4, s.cuda_stream)
+                capi.inverse_batch(ntts, p, p, per, 4, 1, s.cuda_stream)
+                hout[lo:hi].copy_(dbuf[lo:hi], non_blocking=True)
+
+    for s in streams:
+        s.wait_stream(main)
+    one_step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(main)
+    for _ in range(steps):
+        for s in streams:
+            s.wait_stream(main)
+        one_step()
+        for s in streams:
+            main.wait_stream(s)
+    e1.record(main)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    ok = torch.equal(hin, hout)
+    nbytes = flat.nbytes
+    return {"value": 2 * COUNT * steps / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+            "d2h_bytes_per_step": nbytes, "ms_per_step": ms / steps, "bitexact_roundtrip": ok,
+            "pipeline": f"{chunks} chunks over 3 streams"}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU-baseline sample length")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,208 @@
+/*
+ * axhel_cuda.h — C-ABI of the B200 (sm_100a) implementation of AXHEL's hot
+ * path: the negacyclic Harvey NTT/INTT and the element-wise modular kernels.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, returns
+ * an axhel_status_t, and never allocates on behalf of the caller's data.
+ * Data pointers are DEVICE pointers unless stated otherwise; calls are
+ * asynchronous on the given CUDA stream (a cudaStream_t passed as void*,
+ * NULL = the legacy default stream).  Residues are uint64_t, moduli q < 2^62.
+ *
+ * Results are bit-identical to the reference native backend (AXHEL,
+ * axhel/ntt/ntt-native.cpp and axhel/eltwise/*.cpp), including the lazy
+ * representatives of forward output factor 4 ([0,4q)) and inverse output
+ * factor 2 ([0,2q)).  Each entry point names the reference interface it
+ * replaces (paths relative to the AXHEL project root).
+ *
+ * The C++ drop-in (include/axhel/axhel.hpp, namespace unipi::axhel) is built
+ * on these functions.
+ */
+#ifndef AXHEL_CUDA_H
+#define AXHEL_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t axhel_status_t;
+#define AXHEL_OK 0
+#define AXHEL_ERR_INVALID 1     /* bad argument (size, factor, pointer, modulus) */
+#define AXHEL_ERR_CUDA 2        /* a CUDA runtime call failed; see axhel_last_error() */
+#define AXHEL_ERR_NOMEM 3       /* device or pinned host allocation failed */
+#define AXHEL_ERR_UNSUPPORTED 4 /* degree / configuration outside the supported range */
+#define AXHEL_ERR_BUSY 5        /* serving queue full */
+#define AXHEL_ERR_TIMEOUT 6     /* a bounded wait expired */
+#define AXHEL_ERR_REJECTED 7    /* serving admission refused (over the HBM budget) */
+#define AXHEL_ERR_CANCELLED 8   /* serving request cancelled before it ran */
+
+/* Opaque handle to the device-resident tables of one (N, q) transform. */
+typedef struct axhel_ntt_ctx* axhel_ntt_t;
+
+/* Smallest and largest supported degree N (powers of two). */
+#define AXHEL_MIN_DEGREE 2u
+#define AXHEL_MAX_DEGREE 131072u
+
+const char* axhel_status_string(axhel_status_t status);
+/* Message of the last failure on the calling thread ("" if none). */
+const char* axhel_last_error(void);
+int axhel_version(void);
+
+/* ---------------------------------------------------------------------- */
+/* NTT tables                                                             */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces NTT::NTT(degree, modulus, root_of_unity)
+ * (axhel/include/axhel/ntt/ntt.hpp:32, axhel/ntt/ntt.cpp:136-152).
+ * Generates the forward/inverse Shoup tables once per (degree, modulus, root)
+ * (process-wide cache) and keeps them resident on the current device.  The
+ * returned handle holds one reference; release it with axhel_cuda_ntt_release. */
+axhel_status_t axhel_cuda_ntt_create(uint64_t degree, uint64_t modulus, uint64_t root_of_unity,
+                                     axhel_ntt_t* out);
+
+/* Replaces NTT::NTT(degree, modulus, root_powers, inv_root_powers, inv_degree_modulo)
+ * (ntt.hpp:37, ntt.cpp:124-133).  root_powers / inv_root_powers are HOST
+ * arrays of `degree` {operand, quotient} pairs (2*degree words, the layout of
+ * NTTMultiplyOperand, ntt.hpp:14-18); inv_degree is one pair.  They are
+ * copied to the device at creation (the reference borrows them instead). */
+axhel_status_t axhel_cuda_ntt_create_external(uint64_t degree, uint64_t modulus, const uint64_t* root_powers,
+                                              const uint64_t* inv_root_powers, const uint64_t* inv_degree,
+                                              axhel_ntt_t* out);
+
+axhel_status_t axhel_cuda_ntt_retain(axhel_ntt_t ntt);
+axhel_status_t axhel_cuda_ntt_release(axhel_ntt_t ntt);
+/* NTT::Degree / NTT::Modulus (ntt.hpp:56-59; 0 for a null handle, ntt.cpp:210-216). */
+uint64_t axhel_cuda_ntt_degree(axhel_ntt_t ntt);
+uint64_t axhel_cuda_ntt_modulus(axhel_ntt_t ntt);
+/* Copies the resident tables back to HOST arrays (2*N, 2*N and 2 words). */
+axhel_status_t axhel_cuda_ntt_read_tables(axhel_ntt_t ntt, uint64_t* root_powers, uint64_t* inv_root_powers,
+                                          uint64_t* inv_degree);
+
+/* ---------------------------------------------------------------------- */
+/* NTT transforms (device pointers)                                       */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces NTT::ComputeForward(result, operand, input_mod_factor, output_mod_factor)
+ * (ntt.hpp:49, ntt.cpp:173-186).  Input in [0, 4q) (the factor is accepted and
+ * ignored, as in the reference); output bit-reversed, in [0, 4q) when
+ * output_mod_factor == 4, else in [0, q).  result may equal operand. */
+axhel_status_t axhel_cuda_ntt_forward(axhel_ntt_t ntt, uint64_t* result, const uint64_t* operand,
+                                      uint64_t input_mod_factor, uint64_t output_mod_factor, void* stream);
+
+/* Replaces NTT::ComputeInverse (ntt.hpp:53, ntt.cpp:192-204).  Input in
+ * [0, 2q), bit-reversed; output natural order, in [0, 2q) when
+ * output_mod_factor == 2, else in [0, q).  input_mod_factor is ignored. */
+axhel_status_t axhel_cuda_ntt_inverse(axhel_ntt_t ntt, uint64_t* result, const uint64_t* operand,
+                                      uint64_t input_mod_factor, uint64_t output_mod_factor, void* stream);
+
+/* Batched forms (new; the reference has one call per limb).  `count` limbs of
+ * one degree N stored back to back (limb stride N words); limb i uses
+ * ntts[i % n_ntts] (n_ntts <= 64), e.g. the RNS limbs of many ciphertexts in
+ * [ciphertext][polynomial][limb][N] order.  Each limb's result equals the
+ * single-call result bit for bit.  One launch per pass covers all limbs. */
+axhel_status_t axhel_cuda_ntt_forward_batch(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* result,
+                                            const uint64_t* operand, uint64_t count, uint64_t input_mod_factor,
+                                            uint64_t output_mod_factor, void* stream);
+/* As above for the inverse.  input_mod_factor == 4 additionally fuses
+ * EltwiseReduceMod(4 -> 2) in front of the transform (the lazy round trip
+ * ComputeForward(1,4) -> EltwiseReduceMod(4,2) -> ComputeInverse(2,·));
+ * any other factor is ignored as in the reference. */
+axhel_status_t axhel_cuda_ntt_inverse_batch(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* result,
+                                            const uint64_t* operand, uint64_t count, uint64_t input_mod_factor,
+                                            uint64_t output_mod_factor, void* stream);
+
+/* Fused INTT -> MulMod -> NTT over a batch (new; one kernel chain replaces
+ *   ComputeInverse(x, x, in_f, 2); EltwiseMulMod(x, x, m, N, q, 2);
+ *   ComputeForward(x, x, 1, out_f)
+ * per limb).  `multiplicand` has the same layout as `operand`, values in
+ * [0, 2q).  in_f == 4 fuses EltwiseReduceMod(4,2) ahead of the inverse. */
+axhel_status_t axhel_cuda_ntt_chain_mul_batch(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* result,
+                                              const uint64_t* operand, const uint64_t* multiplicand, uint64_t count,
+                                              uint64_t input_mod_factor, uint64_t output_mod_factor, void* stream);
+
+/* Fused INTT -> FMAMod -> NTT (new):
+ *   ComputeInverse(x, x, in_f, 2); EltwiseFMAMod(x, x, scalars[i % n_ntts], addend_or_null, N, q, 2);
+ *   ComputeForward(x, x, 1, out_f)
+ * scalars is a HOST array of n_ntts values in [0, 2q); addend (device, same
+ * layout as operand, values in [0, 2q)) may be NULL. */
+axhel_status_t axhel_cuda_ntt_chain_fma_batch(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* result,
+                                              const uint64_t* operand, const uint64_t* scalars, const uint64_t* addend,
+                                              uint64_t count, uint64_t input_mod_factor, uint64_t output_mod_factor,
+                                              void* stream);
+
+/* ---------------------------------------------------------------------- */
+/* Element-wise (device pointers); result may alias any operand.           */
+/* ---------------------------------------------------------------------- */
+
+/* EltwiseAddMod vector-vector / vector-scalar (axhel/include/axhel/eltwise/eltwise-add-mod.hpp:13,17). */
+axhel_status_t axhel_cuda_eltwise_add_vv(uint64_t* result, const uint64_t* operand1, const uint64_t* operand2,
+                                         uint64_t n, uint64_t modulus, void* stream);
+axhel_status_t axhel_cuda_eltwise_add_vs(uint64_t* result, const uint64_t* operand1, uint64_t operand2, uint64_t n,
+                                         uint64_t modulus, void* stream);
+/* EltwiseSubMod (eltwise-sub-mod.hpp:13,17). */
+axhel_status_t axhel_cuda_eltwise_sub_vv(uint64_t* result, const uint64_t* operand1, const uint64_t* operand2,
+                                         uint64_t n, uint64_t modulus, void* stream);
+axhel_status_t axhel_cuda_eltwise_sub_vs(uint64_t* result, const uint64_t* operand1, uint64_t operand2, uint64_t n,
+                                         uint64_t modulus, void* stream);
+/* EltwiseMulMod (eltwise-mul-mod.hpp:14); mod_factor 1, 2 or 4, any other
+ * value writes nothing (eltwise-mul-mod.cpp:83-93) and returns AXHEL_OK. */
+axhel_status_t axhel_cuda_eltwise_mul(uint64_t* result, const uint64_t* operand1, const uint64_t* operand2,
+                                      uint64_t n, uint64_t modulus, uint64_t mod_factor, void* stream);
+/* EltwiseFMAMod (eltwise-fma-mod.hpp:15); op3 may be NULL; mod_factor 1, 2, 4 or 8. */
+axhel_status_t axhel_cuda_eltwise_fma(uint64_t* result, const uint64_t* operand1, uint64_t operand2,
+                                      const uint64_t* operand3, uint64_t n, uint64_t modulus, uint64_t mod_factor,
+                                      void* stream);
+/* EltwiseReduceMod (eltwise-reduce-mod.hpp:14); the (in, out) pairs of
+ * eltwise-reduce-mod.cpp:32-128, including the Barrett form in_factor == modulus;
+ * an unmatched pair writes nothing. */
+axhel_status_t axhel_cuda_eltwise_reduce(uint64_t* result, const uint64_t* operand, uint64_t n, uint64_t modulus,
+                                         uint64_t input_mod_factor, uint64_t output_mod_factor, void* stream);
+
+/* Fused tensor product of two ciphertexts (new; replaces the per-limb call
+ * sequence t0 = MulMod(c0,d0); t1 = MulMod(c0,d1); u = MulMod(c1,d0);
+ * t1 = AddMod(t1,u); t2 = MulMod(c1,d1) with factor `mod_factor`, then
+ * ReduceMod(·,4,1)).  Inputs: `count` limbs of n words each, stored back to back;
+ * limb i uses moduli[i % n_moduli] (HOST array, n_moduli <= 64). */
+axhel_status_t axhel_cuda_tensor_product(uint64_t* r0, uint64_t* r1, uint64_t* r2, const uint64_t* c0,
+                                         const uint64_t* c1, const uint64_t* d0, const uint64_t* d1, uint64_t n,
+                                         uint64_t count, const uint64_t* moduli, uint64_t n_moduli,
+                                         uint64_t mod_factor, void* stream);
+
+/* ---------------------------------------------------------------------- */
+/* Plans: autotuned pass configuration                                    */
+/* ---------------------------------------------------------------------- */
+
+/* Force the pass split for (inverse, log2 N): npass passes of lg[i] stages
+ * (sum == log2 N), lr[i] register stages and tg[i] groups per CTA.
+ * npass == 0 restores the default.  Used by the autotuner. */
+axhel_status_t axhel_cuda_plan_set(int inverse, uint32_t log_degree, uint32_t npass, const uint32_t* lg,
+                                   const uint32_t* lr, const uint32_t* tg);
+/* Reads the plan used for (inverse, log2 N, count limbs); arrays of >= 3. */
+axhel_status_t axhel_cuda_plan_get(int inverse, uint32_t log_degree, uint64_t count, uint32_t* npass, uint32_t* lg,
+                                   uint32_t* lr, uint32_t* tg);
+/* Loads an autotuner table (text, one plan per line); NULL = the table shipped
+ * beside the library.  Returns the number of plans loaded via *loaded. */
+axhel_status_t axhel_cuda_plan_load(const char* path, uint32_t* loaded);
+
+/* ---------------------------------------------------------------------- */
+/* Host-pointer helpers used by the C++ drop-in                           */
+/* ---------------------------------------------------------------------- */
+
+/* 1 if p is device (or managed) memory visible to the current device. */
+int axhel_cuda_is_device_pointer(const void* p);
+/* Number of kernel launches issued by this library since load (all threads). */
+uint64_t axhel_cuda_launch_count(void);
+
+/* Per-kernel device timing: while enabled, each launch of this library is
+ * bracketed by CUDA events on its own stream.  The report (one line per
+ * kernel configuration: "<name...> <launches> <total_ms>") drains the
+ * records; *needed receives the buffer size required. */
+axhel_status_t axhel_cuda_profile_enable(int on);
+axhel_status_t axhel_cuda_profile_report(char* buf, uint64_t len, uint64_t* needed);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AXHEL_CUDA_H */

@@ -1,0 +1,79 @@
+"""GPU parity of the fused forms against the reference's per-limb call
+sequences, run on the oracle: INTT -> MulMod/FMAMod -> NTT chains and the
+tensor-product eltwise chain."""
+import numpy as np
+import pytest
+
+from helpers import SEED, dev, dev_empty, host, ptr
+
+pytestmark = pytest.mark.gpu
+
+
+def moduli(oracle, n, L, bits0):
+    out = []
+    for i in range(L):
+        q = oracle.find_ntt_prime_near(n, bits0 + (i % 10), i + 1, L + 2)
+        psi = oracle.find_primitive_root(n, q)
+        out.append((q, psi))
+    return out
+
+
+@pytest.mark.parametrize("n", [8, 1024, 4096, 16384, 65536, 131072])
+@pytest.mark.parametrize("op", ["mul", "fma", "fma_noadd"])
+def test_chain_matches_call_sequence(cuda, oracle, n, op):
+    L, count = 3, 4
+    ms = moduli(oracle, n, L, 45)
+    ntts = [cuda.NTT(n, q, psi) for q, psi in ms]
+    tabs = [oracle.tables(n, q, psi) for q, psi in ms]
+    st = oracle.rng(SEED ^ 0xC4A1 ^ n)
+    x = np.concatenate([oracle.random_vector(st, n, 4 * ms[i % L][0]) for i in range(count)])
+    m = np.concatenate([oracle.random_vector(st, n, 2 * ms[i % L][0]) for i in range(count)])
+    scalars = [oracle.bounded(st, 2 * q) for q, _ in ms]
+    for in_f, out_f in ((4, 4), (2, 1)):
+        xin = x if in_f == 4 else np.concatenate(
+            [oracle.reduce(x[i * n:(i + 1) * n], ms[i % L][0], 4, 2) for i in range(count)])
+        d, o, dm = dev(xin), dev_empty(xin.size), dev(m)
+        if op == "mul":
+            cuda.chain_mul_batch(ntts, ptr(o), ptr(d), ptr(dm), count, in_f, out_f)
+        else:
+            cuda.chain_fma_batch(ntts, ptr(o), ptr(d), scalars, ptr(dm) if op == "fma" else 0, count, in_f, out_f)
+        got = host(o)
+        for i in range(count):
+            q = ms[i % L][0]
+            fwd, inv, ninv = tabs[i % L]
+            seg = xin[i * n:(i + 1) * n]
+            if in_f == 4:
+                seg = oracle.reduce(seg, q, 4, 2)
+            y = oracle.inverse(seg, q, inv, ninv, 2, 2)
+            mi = m[i * n:(i + 1) * n]
+            if op == "mul":
+                y = oracle.mul(y, mi, q, 2)
+            else:
+                y = oracle.fma(y, scalars[i % L], mi if op == "fma" else None, q, 2)
+            exp = oracle.forward(y, q, fwd, 1, out_f)
+            np.testing.assert_array_equal(got[i * n:(i + 1) * n], exp, err_msg=f"limb {i} in_f={in_f}")
+
+
+@pytest.mark.parametrize("factor", [1, 2, 4])
+def test_tensor_product_matches_call_sequence(cuda, oracle, factor):
+    n, L, pairs = 4096, 4, 3
+    qs = [q for q, _ in moduli(oracle, n, L, 40)]
+    count = pairs * L
+    st = oracle.rng(SEED ^ 0x7E45 ^ factor)
+    bound = lambda i: factor * qs[i % L]
+    c0, c1, d0, d1 = (np.concatenate([oracle.random_vector(st, n, bound(i)) for i in range(count)]) for _ in range(4))
+    bufs = [dev(v) for v in (c0, c1, d0, d1)]
+    outs = [dev_empty(n * count) for _ in range(3)]
+    cuda.tensor_product(*[ptr(t) for t in outs], *[ptr(t) for t in bufs], n, count, qs, factor)
+    r0, r1, r2 = (host(t) for t in outs)
+    for i in range(count):
+        q = qs[i % L]
+        s = slice(i * n, (i + 1) * n)
+        t0 = oracle.mul(c0[s], d0[s], q, factor)
+        t1 = oracle.mul(c0[s], d1[s], q, factor)
+        u = oracle.mul(c1[s], d0[s], q, factor)
+        t1 = oracle.add(t1, u, q)
+        t2 = oracle.mul(c1[s], d1[s], q, factor)
+        np.testing.assert_array_equal(r0[s], oracle.reduce(t0, q, 4, 1))
+        np.testing.assert_array_equal(r1[s], oracle.reduce(t1, q, 4, 1))
+        np.testing.assert_array_equal(r2[s], oracle.reduce(t2, q, 4, 1))

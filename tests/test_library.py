@@ -1,0 +1,120 @@
+"""CPU: the C-ABI library loads and exports every symbol the public headers
+declare (C-ABI and the unipi::axhel C++ drop-in); host-side planner logic and
+the workload parameter helpers.  No GPU calls."""
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB = os.path.join(ROOT, "axhel_b200", "libaxhel.so")
+
+
+def declared_c_functions():
+    names = []
+    for fn in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if fn.endswith(".h"):
+            text = open(os.path.join(ROOT, "include", fn)).read()
+            text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+            names += re.findall(r"^\s*[A-Za-z_][\w \*]*?\b(axhel_\w+)\s*\(", text, flags=re.M)
+    return sorted(set(names))
+
+
+def exported():
+    out = subprocess.run(["nm", "-D", "--defined-only", LIB], capture_output=True, text=True, check=True).stdout
+    return {line.split()[-1] for line in out.splitlines() if " T " in line}
+
+
+def test_library_built():
+    assert os.path.exists(LIB), "run python -m axhel_b200.build"
+
+
+def test_every_declared_c_symbol_is_exported():
+    names = declared_c_functions()
+    assert len(names) >= 30
+    missing = [n for n in names if n not in exported()]
+    assert not missing, missing
+
+
+def test_cpp_dropin_symbols_exported():
+    out = subprocess.run(["nm", "-DC", "--defined-only", LIB], capture_output=True, text=True, check=True).stdout
+    for sig in ("unipi::axhel::EltwiseAddMod(unsigned long*, unsigned long const*, unsigned long const*",
+                "unipi::axhel::EltwiseAddMod(unsigned long*, unsigned long const*, unsigned long,",
+                "unipi::axhel::EltwiseSubMod(unsigned long*, unsigned long const*, unsigned long const*",
+                "unipi::axhel::EltwiseSubMod(unsigned long*, unsigned long const*, unsigned long,",
+                "unipi::axhel::EltwiseMulMod(", "unipi::axhel::EltwiseFMAMod(", "unipi::axhel::EltwiseReduceMod(",
+                "unipi::axhel::NTT::NTT(unsigned long, unsigned long, unsigned long)",
+                "unipi::axhel::NTT::NTT(unsigned long, unsigned long, unipi::axhel::NTTMultiplyOperand const*",
+                "unipi::axhel::NTT::ComputeForward(", "unipi::axhel::NTT::ComputeInverse(",
+                "unipi::axhel::NTT::Degree() const", "unipi::axhel::NTT::Modulus() const"):
+        assert sig in out, sig
+
+
+def test_ctypes_load_and_cpu_side_calls():
+    from axhel_b200 import capi
+
+    L = capi.lib()
+    assert L.axhel_version() >= 100
+    assert L.axhel_status_string(4) == b"unsupported configuration"
+    # argument checks fail before touching a device
+    with pytest.raises(capi.AxhelError) as e:
+        capi.NTT(12, 97, 3)
+    assert e.value.status == 4
+    # n == 0 is a no-op with null pointers (reference loops run zero times)
+    capi.add(0, 0, 0, 0, 97)
+    capi.mul(0, 0, 0, 0, 97, 1)
+
+
+def test_default_plans_are_valid():
+    from axhel_b200 import capi
+
+    for logn in range(1, 18):
+        for inverse in (False, True):
+            for count in (1, 24, 768):
+                plan = capi.plan_get(inverse, logn, count)
+                assert sum(p[0] for p in plan) == logn
+                for lg, lr, tg in plan:
+                    assert 1 <= lr <= lg and tg >= 1 and (tg & (tg - 1)) == 0
+                    assert (tg << (lg - lr)) <= (256 if lr >= 5 else 512)
+                if logn >= 14:
+                    assert len(plan) == 2
+                    fwd = capi.plan_get(False, logn, count)
+                    inv = capi.plan_get(True, logn, count)
+                    assert fwd[0][0] == inv[-1][0], "chain fusion needs matching column passes"
+
+
+def test_plan_override_and_table(tmp_path):
+    from axhel_b200 import capi
+
+    capi.plan_set(False, 16, [(8, 4, 16), (8, 4, 4)])
+    assert capi.plan_get(False, 16, 768) == [(8, 4, 16), (8, 4, 4)]
+    with pytest.raises(capi.AxhelError):
+        capi.plan_set(False, 16, [(8, 4, 16), (7, 4, 4)])  # stages do not sum to 16
+    with pytest.raises(capi.AxhelError):
+        capi.plan_set(False, 16, [(8, 3, 64), (8, 4, 4)])  # 64 x 32 threads > 512
+    capi.plan_set(False, 16, [])
+    t = tmp_path / "plans.txt"
+    t.write_text("# inverse logn bucket npass lg lr tg ...\n0 15 3 2 8 4 8 7 4 16\n0 15 3 2 8 4 8 9 4 1\n")
+    assert capi.plan_load(str(t)) == 1  # the second line does not sum to 15
+    assert capi.plan_get(False, 15, 8) == [(8, 4, 8), (7, 4, 16)]
+
+
+def test_params_primes_match_reference_generator(oracle):
+    from axhel_b200 import params
+
+    for n in (1024, 1 << 16):
+        for bits in (30, 50, 59, 62):
+            for num, den in ((1, 4), (1, 2), (3, 4)):
+                assert params.ntt_prime_near(n, bits, num, den) == oracle.find_ntt_prime_near(n, bits, num, den)
+            q = params.ntt_prime_near(n, bits, 1, 2)
+            assert params.primitive_root(n, q) == oracle.find_primitive_root(n, q)
+    import random
+
+    r = random.Random(5)
+    for _ in range(2000):
+        x = r.getrandbits(62) | 1
+        assert params.is_prime(x) == bool(oracle.is_prime(x))
+    mods = params.rns_moduli(1 << 16, 24, 50, 59)
+    assert len({q for q, _ in mods}) == 24
+    assert all((q - 1) % (1 << 17) == 0 and 50 <= q.bit_length() <= 59 for q, _ in mods)
