@@ -1,0 +1,141 @@
+"""Autotuner for the NTT pass plans.
+
+For each direction, degree N = 2^logn and limb-count bucket, times every
+candidate split of the log2 N stages into passes (1 or 2 passes), register
+depth LR in {3, 4, 5} and tile width TG on the GPU (CUDA events, median of
+several launches of the batched C-ABI call) and writes the fastest to
+``axhel_b200/ntt_plans.txt``, which the library loads at first use:
+
+    <inverse> <logn> <limb-bucket> <npass> (<lg> <lr> <tg>)...
+
+limb-bucket = floor(log2(limbs)).  Every candidate computes the same bits
+(tests/test_ntt_gpu.py::test_every_plan_bitexact), so the choice only
+affects speed.
+
+    python -m axhel_b200.autotune [--logn 12-17] [--buckets 0,3,6,9]
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import statistics
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+TABLE = os.path.join(HERE, "ntt_plans.txt")
+
+
+def candidates(logn, inverse):
+    out = []
+    if logn <= 13:
+        for lr in (3, 4, 5):
+            if lr <= logn and (1 << (logn - lr)) <= (256 if lr >= 5 else 512):
+                out.append([(logn, lr, 1)])
+    if logn >= 6:
+        for a in range(3, min(13, logn - 3) + 1):  # a = strided column pass
+            b = logn - a
+            if b > 13 or b < 3:
+                continue
+            for lra in (3, 4, 5):
+                for lrb in (3, 4, 5):
+                    if lra > a or lrb > b:
+                        continue
+                    for tga in (4, 8, 16, 32):
+                        for tgb in (1, 2, 4, 8, 16, 32):
+                            col = (a, lra, tga)
+                            row = (b, lrb, tgb)
+                            if tga > (1 << b) or tgb > (1 << a):
+                                continue
+                            if (tga << (a - lra)) > (256 if lra >= 5 else 512):
+                                continue
+                            if (tgb << (b - lrb)) > (256 if lrb >= 5 else 512):
+                                continue
+                            if (tga << (a - lra)) < 64 or (tgb << (b - lrb)) < 64:
+                                continue
+                            out.append([row, col] if inverse else [col, row])
+    return out
+
+
+def time_plan(capi, torch, ntts, x, y, count, inverse, reps=5):
+    if inverse:
+        fn = lambda: capi.inverse_batch(ntts, y.data_ptr(), x.data_ptr(), count, 2, 2)
+    else:
+        fn = lambda: capi.forward_batch(ntts, y.data_ptr(), x.data_ptr(), count, 4, 4)
+    fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return statistics.median(ts)
+
+
+def tune(lognums, buckets, limbs_cap_bytes=1 << 30, verbose=True):
+    import torch
+
+    from axhel_b200 import capi, params
+
+    lines = []
+    for logn in lognums:
+        n = 1 << logn
+        mods = params.rns_moduli(n, 8, 50, 59)
+        ntts = [capi.NTT(n, q, psi) for q, psi in mods]
+        for bucket in buckets:
+            count = 1 << bucket
+            if count * n * 8 > limbs_cap_bytes:
+                count = max(1, limbs_cap_bytes // (n * 8))
+            rng = np.random.default_rng(logn * 100 + bucket)
+            data = np.concatenate([rng.integers(0, mods[i % 8][0], n, dtype=np.uint64) for i in range(count)])
+            x = torch.from_numpy(data.view(np.int64)).cuda()
+            y = torch.empty_like(x)
+            for inverse in (False, True):
+                best = None
+                for plan in candidates(logn, inverse):
+                    try:
+                        capi.plan_set(inverse, logn, plan)
+                    except capi.AxhelError:
+                        continue
+                    ms = time_plan(capi, torch, ntts, x, y, count, inverse)
+                    if best is None or ms < best[0]:
+                        best = (ms, plan)
+                capi.plan_set(inverse, logn, [])
+                if best is None:
+                    continue
+                ms, plan = best
+                flat = " ".join(f"{lg} {lr} {tg}" for lg, lr, tg in plan)
+                lines.append(f"{int(inverse)} {logn} {bucket} {len(plan)} {flat}")
+                if verbose:
+                    rate = count / (ms / 1e3)
+                    print(f"inv={int(inverse)} logn={logn} limbs={count}: {plan} {ms:.4f} ms "
+                          f"({rate:,.0f} limb-transforms/s)", flush=True)
+    return lines
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--logn", default="12-17")
+    ap.add_argument("--buckets", default="0,3,5,7,9")
+    ap.add_argument("--out", default=TABLE)
+    a = ap.parse_args()
+    lo, _, hi = a.logn.partition("-")
+    lognums = list(range(int(lo), int(hi or lo) + 1))
+    buckets = [int(b) for b in a.buckets.split(",")]
+    t = time.time()
+    lines = tune(lognums, buckets)
+    with open(a.out, "w") as f:
+        f.write("# NTT pass plans chosen by axhel_b200/autotune.py on one B200\n")
+        f.write("# inverse logn limb-bucket npass (lg lr tg)...\n")
+        f.write("\n".join(lines) + "\n")
+    print(f"wrote {a.out} ({len(lines)} plans, {time.time() - t:.0f} s)")
+
+
+if __name__ == "__main__":
+    sys.path.insert(0, os.path.dirname(HERE))
+    main()

@@ -81,6 +81,7 @@ def _declare(L):
     d("axhel_cuda_launch_count", u64)
     d("axhel_cuda_profile_enable", st_t, C.c_int)
     d("axhel_cuda_profile_report", st_t, C.c_char_p, u64, C.POINTER(u64))
+    d("axhel_cuda_butterfly_peak", st_t, vp, C.c_int, C.POINTER(C.c_double), vp)
 
 
 def check(status, where):
@@ -107,6 +108,13 @@ def profile_report():
         if len(parts) == 3:
             out[parts[0]] = (int(parts[1]), float(parts[2]))
     return out
+
+
+def butterfly_peak(ntt, inverse=False, stream=0):
+    """Measured butterflies/s of the reference butterfly on registers only."""
+    r = C.c_double()
+    check(lib().axhel_cuda_butterfly_peak(ntt.h, int(inverse), C.byref(r), stream), "butterfly_peak")
+    return r.value
 
 
 def _arr64(values):

@@ -77,22 +77,12 @@ int sm_count()
 
 // -------------------------------------------------------- table contexts
 
-struct axhel_ntt_ctx {
-    std::atomic<int> refs{1};
-    uint64_t n = 0, q = 0, root = 0;
-    uint32_t logn = 0;
-    int device = 0;
-    bool cached = false;
-    void* mem = nullptr;          // device allocation: ModCtx | fwd[N] | inv[N]
-    const ModCtx* dctx = nullptr;  // device address of the ModCtx header
-};
-
 namespace {
 
 std::mutex g_cache_mu;
 std::map<std::tuple<int, uint64_t, uint64_t, uint64_t>, axhel_ntt_ctx*> g_cache;
 
-constexpr size_t kHeader = 256;  // ModCtx padded so the tables start 256-byte aligned
+constexpr size_t kHeader = kCtxHeaderBytes;
 
 // Builds the forward / inverse tables exactly as GenerateNTTTables
 // (axhel/ntt/ntt-tables.cpp:81-140): fwd[i] = psi^bitrev(i); inv[0] = 0,

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
 #include <string>
@@ -79,6 +80,18 @@ bool plan_valid(const NttPlan& p, uint32_t logn, bool inverse);
 int plan_load(const char* path);
 void plan_override(bool inverse, uint32_t logn, const NttPlan* p);  // nullptr clears
 
-// Host table generation (tables.cpp): restates axhel/ntt/ntt-tables.cpp:81-140.
-struct HostTables;
+// Bytes reserved for the ModCtx header in front of the twiddle tables.
+constexpr size_t kCtxHeaderBytes = 256;
+
 }  // namespace axhel_impl
+
+// One (N, q) transform context: device allocation ModCtx | fwd[N] | inv[N].
+struct axhel_ntt_ctx {
+    std::atomic<int> refs{1};
+    uint64_t n = 0, q = 0, root = 0;
+    uint32_t logn = 0;
+    int device = 0;
+    bool cached = false;
+    void* mem = nullptr;                       // device allocation
+    const axhel_impl::ModCtx* dctx = nullptr;  // device address of the ModCtx header
+};

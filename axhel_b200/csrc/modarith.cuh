@@ -26,12 +26,71 @@ __device__ __forceinline__ uint64_t reduce_input(uint64_t x, uint64_t q)
     return x;
 }
 
+// Conditional subtract for the NTT's bounded ranges: the same function as
+// csub() whenever |x - bound| < 2^63, which holds for every value a transform
+// handles (x < 4q, bound <= 2q, q < 2^62).  Testing the sign of the
+// difference takes one compare on its high word instead of a 64-bit compare.
+__device__ __forceinline__ uint64_t csub_lazy(uint64_t x, uint64_t bound)
+{
+    const uint64_t d = x - bound;
+    return static_cast<int64_t>(d) < 0 ? x : d;
+}
+
+// floor(a * b / 2^64) through a 32-bit multiply-add carry chain (seven
+// integer multiply-adds and one add).
+__device__ __forceinline__ uint64_t mul_hi64(uint64_t a, uint64_t b)
+{
+    uint64_t r;
+    asm("{\n\t"
+        ".reg .u32 a0, a1, b0, b1, t0, t1, t2, r0, r1;\n\t"
+        "mov.b64 {a0, a1}, %1;\n\t"
+        "mov.b64 {b0, b1}, %2;\n\t"
+        "mul.hi.u32 t0, a0, b0;\n\t"
+        "mad.lo.cc.u32 t0, a0, b1, t0;\n\t"
+        "madc.hi.u32 t1, a0, b1, 0;\n\t"
+        "mad.lo.cc.u32 t0, a1, b0, t0;\n\t"
+        "madc.hi.cc.u32 t1, a1, b0, t1;\n\t"
+        "addc.u32 t2, 0, 0;\n\t"
+        "mad.lo.cc.u32 r0, a1, b1, t1;\n\t"
+        "madc.hi.u32 r1, a1, b1, t2;\n\t"
+        "mov.b64 %0, {r0, r1};\n\t"
+        "}"
+        : "=l"(r)
+        : "l"(a), "l"(b));
+    return r;
+}
+
+// (v * w + e * nq) mod 2^64 with 32-bit multiply-adds; nq = 2^64 - q turns
+// the Shoup subtraction v*w - e*q into one accumulation chain.
+__device__ __forceinline__ uint64_t mul_lo_acc(uint64_t v, uint64_t w, uint64_t e, uint64_t nq)
+{
+    uint64_t r;
+    asm("{\n\t"
+        ".reg .u32 v0, v1, w0, w1, e0, e1, n0, n1, r0, r1;\n\t"
+        "mov.b64 {v0, v1}, %1;\n\t"
+        "mov.b64 {w0, w1}, %2;\n\t"
+        "mov.b64 {e0, e1}, %3;\n\t"
+        "mov.b64 {n0, n1}, %4;\n\t"
+        "mul.lo.u32 r0, v0, w0;\n\t"
+        "mul.hi.u32 r1, v0, w0;\n\t"
+        "mad.lo.u32 r1, v0, w1, r1;\n\t"
+        "mad.lo.u32 r1, v1, w0, r1;\n\t"
+        "mad.lo.u32 r1, e0, n1, r1;\n\t"
+        "mad.lo.u32 r1, e1, n0, r1;\n\t"
+        "mad.lo.cc.u32 r0, e0, n0, r0;\n\t"
+        "madc.hi.u32 r1, e0, n0, r1;\n\t"
+        "mov.b64 %0, {r0, r1};\n\t"
+        "}"
+        : "=l"(r)
+        : "l"(v), "l"(w), "l"(e), "l"(nq));
+    return r;
+}
+
 // MultiplyUIntModLazy (axhel/include/axhel/number-theory/uint-arith.hpp:48-52):
 // value * w - floor(value * w' / 2^64) * q  (mod 2^64), in [0, 2q).
 __device__ __forceinline__ uint64_t shoup_lazy(uint64_t v, uint64_t w, uint64_t wq, uint64_t q)
 {
-    const uint64_t est = __umul64hi(v, wq);
-    return v * w - est * q;
+    return mul_lo_acc(v, w, mul_hi64(v, wq), 0 - q);
 }
 
 // Barrett product of EltwiseMulModNative (axhel/eltwise/eltwise-mul-mod.cpp:40-60),
@@ -58,7 +117,7 @@ __device__ __forceinline__ uint64_t barrett_reduce64(uint64_t x, uint64_t q, uin
 __device__ __forceinline__ void fwd_butterfly(uint64_t& x, uint64_t& y, uint64_t w, uint64_t wq, uint64_t q,
                                               uint64_t q2)
 {
-    const uint64_t gx = csub(x, q2);
+    const uint64_t gx = csub_lazy(x, q2);
     const uint64_t t = shoup_lazy(y, w, wq, q);
     x = gx + t;
     y = gx + q2 - t;
@@ -69,7 +128,7 @@ __device__ __forceinline__ void inv_butterfly(uint64_t& x, uint64_t& y, uint64_t
                                               uint64_t q2)
 {
     const uint64_t u = x, v = y;
-    x = csub(u + v, q2);
+    x = csub_lazy(u + v, q2);
     y = shoup_lazy(u + q2 - v, w, wq, q);
 }
 
@@ -78,7 +137,7 @@ __device__ __forceinline__ void inv_butterfly(uint64_t& x, uint64_t& y, uint64_t
 __device__ __forceinline__ void inv_final_butterfly(uint64_t& x, uint64_t& y, uint64_t ninv, uint64_t ninv_q,
                                                     uint64_t sr, uint64_t sr_q, uint64_t q, uint64_t q2)
 {
-    const uint64_t gx = csub(x, q2);
+    const uint64_t gx = csub_lazy(x, q2);
     const uint64_t v = y;
     x = shoup_lazy(gx + v, ninv, ninv_q, q);
     y = shoup_lazy(gx + q2 - v, sr, sr_q, q);

@@ -9,11 +9,16 @@
 // with stride S = 2^(logn - s0 - LG) for the forward (Cooley-Tukey, large gaps
 // first) and S = 2^s0 for the inverse (Gentleman-Sande, small gaps first).
 // A CTA takes TG consecutive groups (a "tile"): TG adjacent columns of one
-// block when S > 1 (coalesced rows of TG words), or TG adjacent contiguous
-// blocks when S == 1.  The tile is staged in shared memory (padded, XOR
-// swizzled), then processed in rounds: each thread holds R = 2^LR elements in
-// registers and applies LR consecutive stages to them before the next
-// shared-memory exchange.
+// block when S > 1, or TG adjacent contiguous blocks when S == 1.
+//
+// Each thread holds R = 2^LR elements of one group in registers and applies
+// LR consecutive stages to them per round.  The first round loads straight
+// from global memory and the last round stores straight back; shared memory
+// (padded, XOR-swizzled) is used only to exchange elements between rounds,
+// with one barrier per exchange.  Global accesses are coalesced: in strided
+// tiles consecutive lanes take consecutive columns; in contiguous tiles a
+// round whose register bits are the low bits reads R consecutive words per
+// thread as 16-byte vectors, and the other rounds read runs of 2^lo words.
 //
 // Every butterfly is exactly the reference's (ForwardButterflyNative /
 // InverseButterflyNative, axhel/ntt/ntt-internal.hpp:20-49, and the final
@@ -21,8 +26,8 @@
 // element pairs with the same twiddles in the same stage order, so outputs
 // are bit-identical, lazy ranges included.  Twiddle indices:
 //   forward stage t, position p : fwd[2^t + (p >> (logn - t))]      (ntt-native.cpp:39)
-//   inverse stage s, position p : inv[1 + N - N/2^s + (p >> (s+1))]  (ntt-native.cpp:84, sequential
-//                                 root_index over blocks i of each stage)
+//   inverse stage s, position p : inv[1 + N - N/2^s + (p >> (s+1))]  (ntt-native.cpp:84, the
+//                                 sequential root_index over the blocks of each stage)
 #pragma once
 
 #include <cuda_runtime.h>
@@ -37,42 +42,56 @@ namespace axhel_impl {
 
 using namespace axhel_dev;
 
+// Threads per CTA allowed for a register depth: 32 elements per thread need
+// more than the 128 registers a 512-thread launch bound leaves.
+constexpr int max_threads(int LR) { return LR >= 5 ? 256 : 512; }
+
+template <int LG, int LR>
+constexpr int num_rounds()
+{
+    return (LG + LR - 1) / LR;
+}
+
+// Lowest in-group bit held in registers during round RD.  Forward rounds walk
+// the bits from the top, inverse rounds from the bottom; a short final round
+// re-covers already processed bits so every round holds LR bits.
+template <bool INV, int LG, int LR, int RD>
+constexpr int round_lo()
+{
+    if constexpr (INV) {
+        return (RD * LR < LG - LR) ? RD * LR : LG - LR;
+    } else {
+        return (LG - (RD + 1) * LR > 0) ? LG - (RD + 1) * LR : 0;
+    }
+}
+
 // XOR swizzle of the in-group index: flips the low 4 bits by bits 4..7 so
 // that both unit-stride and stride-16 register fetches hit distinct banks.
 __device__ __forceinline__ uint32_t swz(uint32_t r) { return r ^ ((r >> 4) & 15u); }
 
-template <int LG>
-struct Geo {
-    static constexpr int G = 1 << LG;
-    static constexpr int GP = G + 1;  // padded group pitch in words
-};
-
-// Per-CTA tile geometry, shared by the plain and the fused chain kernels.
+// Per-CTA tile geometry.
 struct Tile {
-    uint64_t limb;       // limb index in the batch
-    uint64_t g0;         // first group of the tile within the limb
-    uint64_t base;       // word offset (in the limb) of element (gi = 0, r = 0)
-    uint64_t S;          // group stride in words
-    uint32_t lgS;
-    uint32_t lgtg;       // log2 groups per tile
-    bool strided;        // S > 1
+    uint64_t limb;  // limb index in the batch
+    uint64_t g0;    // first group of the tile within the limb
+    uint64_t base;  // word offset (in the limb) of element (gi = 0, r = 0)
+    uint32_t lgS;   // log2 group stride in words
+    uint32_t lgtg;  // log2 groups per tile
+    bool strided;   // S > 1
 };
 
 template <int LG>
 __device__ __forceinline__ Tile make_tile(uint32_t logn, uint32_t lgS, uint32_t lgtg)
 {
     Tile t;
-    const uint64_t groups_per_limb = 1ull << (logn - LG);
-    const uint64_t tiles_per_limb = groups_per_limb >> lgtg;
+    const uint32_t lg_tiles = logn - LG - lgtg;  // log2 tiles per limb
     const uint64_t tile = blockIdx.x;
-    t.limb = tile / tiles_per_limb;
-    t.g0 = (tile - t.limb * tiles_per_limb) << lgtg;
+    t.limb = tile >> lg_tiles;
+    t.g0 = (tile & ((1ull << lg_tiles) - 1)) << lgtg;
     t.lgS = lgS;
-    t.S = 1ull << lgS;
     t.lgtg = lgtg;
     t.strided = lgS != 0;
     if (t.strided) {
-        const uint64_t blk = t.g0 >> lgS, col = t.g0 & (t.S - 1);
+        const uint64_t blk = t.g0 >> lgS, col = t.g0 & ((1ull << lgS) - 1);
         t.base = (blk << (LG + lgS)) + col;
     } else {
         t.base = t.g0 << LG;
@@ -80,33 +99,14 @@ __device__ __forceinline__ Tile make_tile(uint32_t logn, uint32_t lgS, uint32_t 
     return t;
 }
 
-// Word offset in the limb of element (gi, r), and the group's block index.
-template <int LG>
-__device__ __forceinline__ uint64_t tile_addr(const Tile& t, uint32_t gi, uint32_t r)
-{
-    return t.strided ? t.base + ((uint64_t)r << t.lgS) + gi : t.base + ((uint64_t)gi << LG) + r;
-}
 template <int LG>
 __device__ __forceinline__ uint64_t tile_blk(const Tile& t, uint32_t gi)
 {
     return t.strided ? (t.g0 >> t.lgS) : (t.g0 + gi);
 }
 
-// Element e of the tile in memory order -> (gi, r).
-template <int LG>
-__device__ __forceinline__ void tile_elem(const Tile& t, uint32_t e, uint32_t& gi, uint32_t& r)
-{
-    if (t.strided) {
-        gi = e & ((1u << t.lgtg) - 1);
-        r = e >> t.lgtg;
-    } else {
-        gi = e >> LG;
-        r = e & ((1u << LG) - 1);
-    }
-}
-
 // Thread -> (group in tile, thread in group).  Column-fastest when strided so
-// a warp reads consecutive columns; thread-in-group-fastest otherwise.
+// a warp touches consecutive columns; thread-in-group-fastest otherwise.
 template <int LG, int LR>
 __device__ __forceinline__ void thread_role(const Tile& t, uint32_t& gi, uint32_t& k)
 {
@@ -121,22 +121,71 @@ __device__ __forceinline__ void thread_role(const Tile& t, uint32_t& gi, uint32_
     }
 }
 
-// ------------------------------------------------------------------ rounds
+// In-group index of register 0 for register bits [lo, lo + LR).
+template <int LR>
+__device__ __forceinline__ uint32_t round_base(uint32_t k, int lo)
+{
+    return ((k >> lo) << (lo + LR)) | (k & ((1u << lo) - 1));
+}
 
-// Forward round RD: stage bits hi-1 .. hi-nb of the in-group index (largest
-// gap first).  Registers hold bits [lo, lo + LR) of the index.
+// ------------------------------------------------------- global <-> registers
+
+template <int LG, int LR, int LO>
+__device__ __forceinline__ void load_global(uint64_t (&v)[1 << LR], const uint64_t* __restrict__ limb_src,
+                                            const Tile& t, uint32_t gi, uint32_t rb, bool vec_ok)
+{
+    constexpr int R = 1 << LR;
+    if (t.strided) {
+        const uint64_t* p = limb_src + t.base + gi + ((uint64_t)rb << t.lgS);
+#pragma unroll
+        for (int i = 0; i < R; ++i) v[i] = p[(uint64_t)i << (LO + t.lgS)];
+    } else if (LO == 0 && vec_ok) {
+        const ulonglong2* p = reinterpret_cast<const ulonglong2*>(limb_src + t.base + ((uint64_t)gi << LG) + rb);
+#pragma unroll
+        for (int i = 0; i < R / 2; ++i) {
+            const ulonglong2 w = p[i];
+            v[2 * i] = w.x;
+            v[2 * i + 1] = w.y;
+        }
+    } else {
+        const uint64_t* p = limb_src + t.base + ((uint64_t)gi << LG) + rb;
+#pragma unroll
+        for (int i = 0; i < R; ++i) v[i] = p[i << LO];
+    }
+}
+
+template <int LG, int LR, int LO>
+__device__ __forceinline__ void store_global(const uint64_t (&v)[1 << LR], uint64_t* __restrict__ limb_dst,
+                                             const Tile& t, uint32_t gi, uint32_t rb, bool vec_ok)
+{
+    constexpr int R = 1 << LR;
+    if (t.strided) {
+        uint64_t* p = limb_dst + t.base + gi + ((uint64_t)rb << t.lgS);
+#pragma unroll
+        for (int i = 0; i < R; ++i) p[(uint64_t)i << (LO + t.lgS)] = v[i];
+    } else if (LO == 0 && vec_ok) {
+        ulonglong2* p = reinterpret_cast<ulonglong2*>(limb_dst + t.base + ((uint64_t)gi << LG) + rb);
+#pragma unroll
+        for (int i = 0; i < R / 2; ++i) p[i] = make_ulonglong2(v[2 * i], v[2 * i + 1]);
+    } else {
+        uint64_t* p = limb_dst + t.base + ((uint64_t)gi << LG) + rb;
+#pragma unroll
+        for (int i = 0; i < R; ++i) p[i << LO] = v[i];
+    }
+}
+
+// ------------------------------------------------------------------ stages
+
+// Forward round RD on registers: stage bits hi-1 .. hi-nb of the in-group
+// index (largest gap first); registers hold bits [lo, lo + LR).
 template <int LG, int LR, int RD>
-__device__ __forceinline__ void fwd_round(uint64_t* smg, uint32_t k, uint64_t blk, uint32_t s0,
-                                          const ulonglong2* __restrict__ tw, uint64_t q, uint64_t q2)
+__device__ __forceinline__ void fwd_stages(uint64_t (&v)[1 << LR], uint32_t rbase, uint64_t blk, uint32_t s0,
+                                           const ulonglong2* __restrict__ tw, uint64_t q, uint64_t q2)
 {
     constexpr int R = 1 << LR;
     constexpr int hi = LG - RD * LR;
     constexpr int nb = hi < LR ? hi : LR;
-    constexpr int lo = hi - LR > 0 ? hi - LR : 0;
-    const uint32_t rbase = ((k >> lo) << (lo + LR)) | (k & ((1u << lo) - 1));
-    uint64_t v[R];
-#pragma unroll
-    for (int i = 0; i < R; ++i) v[i] = smg[swz(rbase | ((uint32_t)i << lo))];
+    constexpr int lo = round_lo<false, LG, LR, RD>();
 #pragma unroll
     for (int bb = 0; bb < nb; ++bb) {
         const int b = hi - 1 - bb;  // in-group bit = butterfly span
@@ -154,29 +203,24 @@ __device__ __forceinline__ void fwd_round(uint64_t* smg, uint32_t k, uint64_t bl
             }
         }
     }
-#pragma unroll
-    for (int i = 0; i < R; ++i) smg[swz(rbase | ((uint32_t)i << lo))] = v[i];
 }
 
-// Inverse round RD: stage bits b0 .. b1-1 (smallest gap first).  When `last`
-// is set the pass holds global stage logn-1, which runs the N^-1 final stage.
+// Inverse round RD on registers: stage bits b0 .. b1-1 (smallest gap first).
+// With `last` set the pass holds global stage logn-1, the N^-1 final stage.
 template <int LG, int LR, int RD>
-__device__ __forceinline__ void inv_round(uint64_t* smg, uint32_t k, uint64_t blk, uint32_t s0, uint64_t n,
-                                          const ulonglong2* __restrict__ tw, uint64_t q, uint64_t q2, bool last,
-                                          uint64_t ninv, uint64_t ninv_q, uint64_t sr, uint64_t sr_q)
+__device__ __forceinline__ void inv_stages(uint64_t (&v)[1 << LR], uint32_t rbase, uint64_t blk, uint32_t s0,
+                                           uint64_t n, const ulonglong2* __restrict__ tw, uint64_t q, uint64_t q2,
+                                           bool last, const ModCtx* cx)
 {
     constexpr int R = 1 << LR;
     constexpr int b0 = RD * LR;
     constexpr int b1 = (b0 + LR < LG) ? b0 + LR : LG;
-    constexpr int lo = (b0 < LG - LR) ? b0 : LG - LR;
-    const uint32_t rbase = ((k >> lo) << (lo + LR)) | (k & ((1u << lo) - 1));
-    uint64_t v[R];
-#pragma unroll
-    for (int i = 0; i < R; ++i) v[i] = smg[swz(rbase | ((uint32_t)i << lo))];
+    constexpr int lo = round_lo<true, LG, LR, RD>();
 #pragma unroll
     for (int b = b0; b < b1; ++b) {
         const int rb = b - lo;
         if (b == LG - 1 && last) {
+            const uint64_t ninv = cx->ninv, ninv_q = cx->ninv_q, sr = cx->sroot, sr_q = cx->sroot_q;
 #pragma unroll
             for (int j = 0; j < (R >> (rb + 1)); ++j)
 #pragma unroll
@@ -200,34 +244,61 @@ __device__ __forceinline__ void inv_round(uint64_t* smg, uint32_t k, uint64_t bl
             }
         }
     }
+}
+
+// Register exchange between rounds RD-1 and RD through shared memory.  Each
+// thread writes back the slots it held and reads its next slots; the slot
+// sets of one round are disjoint across threads, so one barrier suffices.
+template <bool INV, int LG, int LR, int RD>
+__device__ __forceinline__ void exchange(uint64_t (&v)[1 << LR], uint64_t* smg, uint32_t k)
+{
+    constexpr int R = 1 << LR;
+    constexpr int lp = round_lo<INV, LG, LR, RD - 1>();
+    constexpr int ln = round_lo<INV, LG, LR, RD>();
+    const uint32_t bp = round_base<LR>(k, lp), bn = round_base<LR>(k, ln);
 #pragma unroll
-    for (int i = 0; i < R; ++i) smg[swz(rbase | ((uint32_t)i << lo))] = v[i];
+    for (int i = 0; i < R; ++i) smg[swz(bp | ((uint32_t)i << lp))] = v[i];
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < R; ++i) v[i] = smg[swz(bn | ((uint32_t)i << ln))];
+}
+
+// Rounds 1 .. NR-1 (round 0 runs on the freshly loaded registers).
+template <int LG, int LR, int... RD>
+__device__ __forceinline__ void fwd_rest(std::integer_sequence<int, RD...>, uint64_t (&v)[1 << LR], uint64_t* smg,
+                                         uint32_t k, uint64_t blk, uint32_t s0, const ulonglong2* tw, uint64_t q,
+                                         uint64_t q2)
+{
+    ((exchange<false, LG, LR, RD + 1>(v, smg, k),
+      fwd_stages<LG, LR, RD + 1>(v, round_base<LR>(k, round_lo<false, LG, LR, RD + 1>()), blk, s0, tw, q, q2)),
+     ...);
 }
 
 template <int LG, int LR, int... RD>
-__device__ __forceinline__ void fwd_rounds(std::integer_sequence<int, RD...>, uint64_t* smg, uint32_t k,
-                                           uint64_t blk, uint32_t s0, const ulonglong2* tw, uint64_t q, uint64_t q2)
+__device__ __forceinline__ void inv_rest(std::integer_sequence<int, RD...>, uint64_t (&v)[1 << LR], uint64_t* smg,
+                                         uint32_t k, uint64_t blk, uint32_t s0, uint64_t n, const ulonglong2* tw,
+                                         uint64_t q, uint64_t q2, bool last, const ModCtx* cx)
 {
-    ((__syncthreads(), fwd_round<LG, LR, RD>(smg, k, blk, s0, tw, q, q2)), ...);
+    ((exchange<true, LG, LR, RD + 1>(v, smg, k),
+      inv_stages<LG, LR, RD + 1>(v, round_base<LR>(k, round_lo<true, LG, LR, RD + 1>()), blk, s0, n, tw, q, q2,
+                                 last, cx)),
+     ...);
 }
 
-template <int LG, int LR, int... RD>
-__device__ __forceinline__ void inv_rounds(std::integer_sequence<int, RD...>, uint64_t* smg, uint32_t k,
-                                           uint64_t blk, uint32_t s0, uint64_t n, const ulonglong2* tw, uint64_t q,
-                                           uint64_t q2, bool last, uint64_t ninv, uint64_t ninv_q, uint64_t sr,
-                                           uint64_t sr_q)
+template <bool INV, int LG, int LR>
+__device__ __forceinline__ void run_rounds(uint64_t (&v)[1 << LR], uint64_t* smg, uint32_t k, uint64_t blk,
+                                           uint32_t s0, uint64_t n, const ModCtx* cx, uint64_t q, uint64_t q2,
+                                           bool last)
 {
-    ((__syncthreads(), inv_round<LG, LR, RD>(smg, k, blk, s0, n, tw, q, q2, last, ninv, ninv_q, sr, sr_q)), ...);
-}
-
-// Threads per CTA allowed for a register depth: 32 elements per thread need
-// more than the 128 registers a 512-thread launch bound leaves.
-constexpr int max_threads(int LR) { return LR >= 5 ? 256 : 512; }
-
-template <int LG, int LR>
-constexpr int num_rounds()
-{
-    return (LG + LR - 1) / LR;
+    constexpr int NR = num_rounds<LG, LR>();
+    if constexpr (INV) {
+        inv_stages<LG, LR, 0>(v, round_base<LR>(k, round_lo<true, LG, LR, 0>()), blk, s0, n, cx->inv, q, q2, last,
+                              cx);
+        inv_rest<LG, LR>(std::make_integer_sequence<int, NR - 1>{}, v, smg, k, blk, s0, n, cx->inv, q, q2, last, cx);
+    } else {
+        fwd_stages<LG, LR, 0>(v, round_base<LR>(k, round_lo<false, LG, LR, 0>()), blk, s0, cx->fwd, q, q2);
+        fwd_rest<LG, LR>(std::make_integer_sequence<int, NR - 1>{}, v, smg, k, blk, s0, cx->fwd, q, q2);
+    }
 }
 
 // ------------------------------------------------------------------ kernels
@@ -236,127 +307,111 @@ template <bool INV, int LG, int LR>
 __global__ void __launch_bounds__(max_threads(LR)) ntt_pass_kernel(const __grid_constant__ PassArgs a)
 {
     extern __shared__ uint64_t sm[];
-    constexpr int GP = Geo<LG>::GP;
+    constexpr int R = 1 << LR;
+    constexpr int GP = (1 << LG) + 1;
+    constexpr int NR = num_rounds<LG, LR>();
+    constexpr int LO_FIRST = round_lo<INV, LG, LR, 0>();
+    constexpr int LO_LAST = round_lo<INV, LG, LR, NR - 1>();
     const uint32_t logn = a.logn;
     const uint32_t lgS = INV ? a.s0 : (logn - a.s0 - LG);
-    const uint32_t lgtg = __ffs(a.tg) - 1;
-    const Tile t = make_tile<LG>(logn, lgS, lgtg);
+    const Tile t = make_tile<LG>(logn, lgS, __ffs(a.tg) - 1);
     const ModCtx* cx = a.ctx[t.limb % a.nctx];
     const uint64_t q = cx->q, q2 = cx->q2;
     const uint64_t n = 1ull << logn;
-    const uint64_t* src = a.src + t.limb * n;
-    uint64_t* dst = a.dst + t.limb * n;
-    const uint32_t nel = a.tg << LG;
-    const bool pre = a.flags & kPreCsub2q;
-
-    for (uint32_t e = threadIdx.x; e < nel; e += blockDim.x) {
-        uint32_t gi, r;
-        tile_elem<LG>(t, e, gi, r);
-        uint64_t x = src[tile_addr<LG>(t, gi, r)];
-        if (pre) x = csub(x, q2);
-        sm[gi * GP + swz(r)] = x;
-    }
+    const uint64_t* src = a.src + (t.limb << logn);
+    uint64_t* dst = a.dst + (t.limb << logn);
+    const bool vec_ok = ((reinterpret_cast<uintptr_t>(a.src) | reinterpret_cast<uintptr_t>(a.dst)) & 15) == 0;
 
     uint32_t gi, k;
     thread_role<LG, LR>(t, gi, k);
-    uint64_t* smg = sm + gi * GP;
     const uint64_t blk = tile_blk<LG>(t, gi);
-    if constexpr (INV) {
-        const bool last = a.flags & kLastPass;
-        inv_rounds<LG, LR>(std::make_integer_sequence<int, num_rounds<LG, LR>()>{}, smg, k, blk, a.s0, n, cx->inv,
-                           q, q2, last, cx->ninv, cx->ninv_q, cx->sroot, cx->sroot_q);
-    } else {
-        fwd_rounds<LG, LR>(std::make_integer_sequence<int, num_rounds<LG, LR>()>{}, smg, k, blk, a.s0, cx->fwd, q,
-                           q2);
-    }
-    __syncthreads();
 
-    const bool norm = a.flags & kPostNorm;
-    for (uint32_t e = threadIdx.x; e < nel; e += blockDim.x) {
-        uint32_t g2, r;
-        tile_elem<LG>(t, e, g2, r);
-        uint64_t x = sm[g2 * GP + swz(r)];
-        if (norm) x = INV ? csub(x, q) : csub(csub(x, q2), q);
-        dst[tile_addr<LG>(t, g2, r)] = x;
+    uint64_t v[R];
+    load_global<LG, LR, LO_FIRST>(v, src, t, gi, round_base<LR>(k, LO_FIRST), vec_ok);
+    if (a.flags & kPreCsub2q) {
+#pragma unroll
+        for (int i = 0; i < R; ++i) v[i] = csub_lazy(v[i], q2);
     }
+    run_rounds<INV, LG, LR>(v, sm + gi * GP, k, blk, a.s0, n, cx, q, q2, (a.flags & kLastPass) != 0);
+    if (a.flags & kPostNorm) {
+#pragma unroll
+        for (int i = 0; i < R; ++i) v[i] = INV ? csub_lazy(v[i], q) : csub_lazy(csub_lazy(v[i], q2), q);
+    }
+    store_global<LG, LR, LO_LAST>(v, dst, t, gi, round_base<LR>(k, LO_LAST), vec_ok);
 }
 
 // Fused column pass of an INTT -> op -> NTT chain: the inverse's last pass
 // (stages logn-LG .. logn-1, incl. the N^-1 final stage) and the forward's
-// first pass (stages 0 .. LG-1) act on the same groups p = r*S + col, so the
-// element-wise op runs on the tile in shared memory between them.
+// first pass (stages 0 .. LG-1) act on the same groups p = r*S + col, and the
+// inverse's last round holds the same register bits as the forward's first
+// round, so the element-wise op runs in registers between them.
 template <int LG, int LR>
 __global__ void __launch_bounds__(max_threads(LR)) ntt_chain_kernel(const __grid_constant__ ChainArgs c)
 {
     extern __shared__ uint64_t sm[];
-    constexpr int GP = Geo<LG>::GP;
+    constexpr int R = 1 << LR;
+    constexpr int GP = (1 << LG) + 1;
+    constexpr int NR = num_rounds<LG, LR>();
+    constexpr int LO_FIRST = round_lo<true, LG, LR, 0>();
+    constexpr int LO_MID = round_lo<true, LG, LR, NR - 1>();
+    constexpr int LO_LAST = round_lo<false, LG, LR, NR - 1>();
+    static_assert(LO_MID == round_lo<false, LG, LR, 0>(), "inverse last round and forward first round differ");
     const PassArgs& a = c.pass;
     const uint32_t logn = a.logn;
-    const uint32_t lgS = logn - LG;
-    const uint32_t lgtg = __ffs(a.tg) - 1;
-    const Tile t = make_tile<LG>(logn, lgS, lgtg);
+    const Tile t = make_tile<LG>(logn, logn - LG, __ffs(a.tg) - 1);
     const uint32_t mi = t.limb % a.nctx;
     const ModCtx* cx = a.ctx[mi];
     const uint64_t q = cx->q, q2 = cx->q2;
     const uint64_t n = 1ull << logn;
-    const uint64_t* src = a.src + t.limb * n;
-    uint64_t* dst = a.dst + t.limb * n;
-    const uint32_t nel = a.tg << LG;
-    const bool pre = a.flags & kPreCsub2q;
+    const uint64_t* src = a.src + (t.limb << logn);
+    uint64_t* dst = a.dst + (t.limb << logn);
+    const bool vec_ok = ((reinterpret_cast<uintptr_t>(a.src) | reinterpret_cast<uintptr_t>(a.dst) |
+                          reinterpret_cast<uintptr_t>(c.operand)) & 15) == 0;
 
-    for (uint32_t e = threadIdx.x; e < nel; e += blockDim.x) {
-        uint32_t gi, r;
-        tile_elem<LG>(t, e, gi, r);
-        uint64_t x = src[tile_addr<LG>(t, gi, r)];
-        if (pre) x = csub(x, q2);
-        sm[gi * GP + swz(r)] = x;
-    }
     uint32_t gi, k;
     thread_role<LG, LR>(t, gi, k);
-    uint64_t* smg = sm + gi * GP;
     const uint64_t blk = tile_blk<LG>(t, gi);
-    inv_rounds<LG, LR>(std::make_integer_sequence<int, num_rounds<LG, LR>()>{}, smg, k, blk, logn - LG, n, cx->inv,
-                       q, q2, true, cx->ninv, cx->ninv_q, cx->sroot, cx->sroot_q);
-    __syncthreads();
+    uint64_t* smg = sm + gi * GP;
 
-    // Element-wise op on the inverse output (lazy [0, 2q)), factor-2 inputs.
-    const uint64_t* opnd = c.operand ? c.operand + t.limb * n : nullptr;
+    uint64_t v[R];
+    load_global<LG, LR, LO_FIRST>(v, src, t, gi, round_base<LR>(k, LO_FIRST), vec_ok);
+    if (a.flags & kPreCsub2q) {
+#pragma unroll
+        for (int i = 0; i < R; ++i) v[i] = csub_lazy(v[i], q2);
+    }
+    run_rounds<true, LG, LR>(v, smg, k, blk, logn - LG, n, cx, q, q2, true);
+
+    // Element-wise op on the inverse output (lazy [0, 2q)) with factor-2
+    // inputs: EltwiseMulMod<2> / EltwiseFMAMod<2> semantics.
     const uint64_t mu = cx->mu;
     const uint32_t shift = cx->shift;
+    const uint32_t rb = round_base<LR>(k, LO_MID);
     if (c.op == kChainMul) {
-        for (uint32_t e = threadIdx.x; e < nel; e += blockDim.x) {
-            uint32_t g2, r;
-            tile_elem<LG>(t, e, g2, r);
-            uint64_t* s = &sm[g2 * GP + swz(r)];
-            const uint64_t m = opnd[tile_addr<LG>(t, g2, r)];
-            *s = barrett_mul(reduce_input<2>(*s, q), reduce_input<2>(m, q), q, mu, shift);
-        }
+        uint64_t m[R];
+        load_global<LG, LR, LO_MID>(m, c.operand + (t.limb << logn), t, gi, rb, vec_ok);
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+            v[i] = barrett_mul(reduce_input<2>(v[i], q), reduce_input<2>(m[i], q), q, mu, shift);
     } else if (c.op == kChainFma) {
         const uint64_t sc = reduce_input<2>(c.scalar[mi], q);
-        for (uint32_t e = threadIdx.x; e < nel; e += blockDim.x) {
-            uint32_t g2, r;
-            tile_elem<LG>(t, e, g2, r);
-            uint64_t* s = &sm[g2 * GP + swz(r)];
-            uint64_t v = barrett_mul(reduce_input<2>(*s, q), sc, q, mu, shift);
-            if (opnd) {
-                v += reduce_input<2>(opnd[tile_addr<LG>(t, g2, r)], q);
-                v = csub(v, q);
-            }
-            *s = v;
+#pragma unroll
+        for (int i = 0; i < R; ++i) v[i] = barrett_mul(reduce_input<2>(v[i], q), sc, q, mu, shift);
+        if (c.operand) {
+            uint64_t m[R];
+            load_global<LG, LR, LO_MID>(m, c.operand + (t.limb << logn), t, gi, rb, vec_ok);
+#pragma unroll
+            for (int i = 0; i < R; ++i) v[i] = csub(v[i] + reduce_input<2>(m[i], q), q);
         }
     }
 
-    fwd_rounds<LG, LR>(std::make_integer_sequence<int, num_rounds<LG, LR>()>{}, smg, k, 0, 0, cx->fwd, q, q2);
-    __syncthreads();
-
-    const bool norm = a.flags & kPostNorm;
-    for (uint32_t e = threadIdx.x; e < nel; e += blockDim.x) {
-        uint32_t g2, r;
-        tile_elem<LG>(t, e, g2, r);
-        uint64_t x = sm[g2 * GP + swz(r)];
-        if (norm) x = csub(csub(x, q2), q);
-        dst[tile_addr<LG>(t, g2, r)] = x;
+    // The forward's first pass: stages 0 .. LG-1 of block 0.
+    fwd_stages<LG, LR, 0>(v, rb, 0, 0, cx->fwd, q, q2);
+    fwd_rest<LG, LR>(std::make_integer_sequence<int, NR - 1>{}, v, smg, k, 0, 0, cx->fwd, q, q2);
+    if (a.flags & kPostNorm) {
+#pragma unroll
+        for (int i = 0; i < R; ++i) v[i] = csub_lazy(csub_lazy(v[i], q2), q);
     }
+    store_global<LG, LR, LO_LAST>(v, dst, t, gi, round_base<LR>(k, LO_LAST), vec_ok);
 }
 
 }  // namespace axhel_impl

@@ -199,6 +199,12 @@ uint64_t axhel_cuda_launch_count(void);
  * kernel configuration: "<name...> <launches> <total_ms>") drains the
  * records; *needed receives the buffer size required. */
 axhel_status_t axhel_cuda_profile_enable(int on);
+
+/* Compute-roofline probe (new): the reference's forward (inverse = 0) or
+ * inverse butterfly, on values held in registers with the twiddles of `ntt`,
+ * over a full-device grid; returns the measured butterflies per second.  An
+ * N-point transform needs (N/2) log2 N butterflies. */
+axhel_status_t axhel_cuda_butterfly_peak(axhel_ntt_t ntt, int inverse, double* butterflies_per_s, void* stream);
 axhel_status_t axhel_cuda_profile_report(char* buf, uint64_t len, uint64_t* needed);
 
 #ifdef __cplusplus
