@@ -23,6 +23,18 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4
           6: "timeout", 7: "rejected", 8: "cancelled"}
 
 
+JOB_FORWARD, JOB_INVERSE, JOB_CHAIN_MUL, JOB_CHAIN_FMA = 1, 2, 3, 4
+
+
+class Job(C.Structure):
+    """axhel_job_t"""
+
+    _fields_ = [("kind", C.c_uint32), ("n_ntts", C.c_uint32), ("ntts", C.POINTER(C.c_void_p)),
+                ("count", C.c_uint64), ("result", C.c_void_p), ("operand", C.c_void_p), ("vector", C.c_void_p),
+                ("scalars", C.POINTER(C.c_uint64)), ("input_mod_factor", C.c_uint64),
+                ("output_mod_factor", C.c_uint64)]
+
+
 class AxhelError(RuntimeError):
     def __init__(self, status, where, msg):
         super().__init__(f"{where}: {STATUS.get(status, status)}: {msg}")
@@ -82,6 +94,15 @@ def _declare(L):
     d("axhel_cuda_profile_enable", st_t, C.c_int)
     d("axhel_cuda_profile_report", st_t, C.c_char_p, u64, C.POINTER(u64))
     d("axhel_cuda_butterfly_peak", st_t, vp, C.c_int, C.POINTER(C.c_double), vp)
+    d("axhel_cuda_batch_create", st_t, C.POINTER(Job), u64, C.POINTER(vp))
+    d("axhel_cuda_batch_launch", st_t, vp, vp)
+    d("axhel_cuda_batch_graph_launch", st_t, vp, vp)
+    d("axhel_cuda_batch_status", st_t, vp, vp)
+    d("axhel_cuda_batch_destroy", st_t, vp)
+    d("axhel_cuda_batch_run", st_t, C.POINTER(Job), u64, vp)
+    d("axhel_cuda_batch_last_error", C.c_char_p)
+    d("axhel_cuda_batch_set_wait_ns", st_t, vp, u64)
+    d("axhel_cuda_batch_debug_unreachable", st_t, vp, u64)
 
 
 def check(status, where):
@@ -115,6 +136,74 @@ def butterfly_peak(ntt, inverse=False, stream=0):
     r = C.c_double()
     check(lib().axhel_cuda_butterfly_peak(ntt.h, int(inverse), C.byref(r), stream), "butterfly_peak")
     return r.value
+
+
+def make_jobs(specs):
+    """specs: list of dicts {kind, ntts, count, result, operand, vector=0,
+    scalars=None, in_f, out_f}; returns (ctypes array of Job, keep-alive list)."""
+    arr = (Job * len(specs))()
+    keep = []
+    for i, sp in enumerate(specs):
+        hs = (C.c_void_p * len(sp["ntts"]))(*[t.h.value for t in sp["ntts"]])
+        keep.append(hs)
+        j = arr[i]
+        j.kind = sp["kind"]
+        j.n_ntts = len(sp["ntts"])
+        j.ntts = C.cast(hs, C.POINTER(C.c_void_p))
+        j.count = sp["count"]
+        j.result = sp["result"]
+        j.operand = sp["operand"]
+        j.vector = sp.get("vector") or None
+        if sp.get("scalars") is not None:
+            sc = (C.c_uint64 * len(sp["scalars"]))(*[int(v) for v in sp["scalars"]])
+            keep.append(sc)
+            j.scalars = C.cast(sc, C.POINTER(C.c_uint64))
+        j.input_mod_factor = sp.get("in_f", 1)
+        j.output_mod_factor = sp.get("out_f", 1)
+    return arr, keep
+
+
+def _bcheck(status, where):
+    if status != OK:
+        raise AxhelError(status, where, lib().axhel_cuda_batch_last_error().decode())
+
+
+class Batch:
+    """A batch of uneven jobs run by one persistent kernel launch."""
+
+    def __init__(self, specs):
+        self.jobs, self._keep = make_jobs(specs)
+        self.h = vp()
+        _bcheck(lib().axhel_cuda_batch_create(self.jobs, len(specs), C.byref(self.h)), "batch_create")
+
+    def launch(self, stream=0, graph=False):
+        f = lib().axhel_cuda_batch_graph_launch if graph else lib().axhel_cuda_batch_launch
+        _bcheck(f(self.h, stream), "batch_launch")
+
+    def status(self, stream=0):
+        return int(lib().axhel_cuda_batch_status(self.h, stream))
+
+    def set_wait_ns(self, ns):
+        _bcheck(lib().axhel_cuda_batch_set_wait_ns(self.h, ns), "batch_set_wait_ns")
+
+    def debug_unreachable(self, job):
+        _bcheck(lib().axhel_cuda_batch_debug_unreachable(self.h, job), "batch_debug_unreachable")
+
+    def close(self):
+        if self.h:
+            lib().axhel_cuda_batch_destroy(self.h)
+            self.h = vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_run(specs, stream=0):
+    jobs, keep = make_jobs(specs)
+    _bcheck(lib().axhel_cuda_batch_run(jobs, len(specs), stream), "batch_run")
 
 
 def _arr64(values):

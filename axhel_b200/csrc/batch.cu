@@ -1,0 +1,551 @@
+// Uneven batches in one persistent launch.
+//
+// A batch mixes jobs of different degree N (2^10 .. 2^17), limb count and
+// kind: forward NTT, inverse NTT, and the fused INTT -> MulMod/FMAMod -> NTT
+// chain.  Every job runs as two or three phases of tiles:
+//
+//   forward : column pass (stages 0..A-1)  -> row pass (stages A..n-1)
+//   inverse : row pass (stages 0..B-1)     -> column pass (stages B..n-1, N^-1)
+//   chain   : inverse row pass -> fused [inverse column pass, op, forward
+//             column pass] -> forward row pass
+//
+// with A = ceil(n/2), B = n - A.  The kernel is persistent (one wave of CTAs
+// sized to the device); CTAs take tiles from one atomic counter in
+// phase-major order (every phase-0 tile of every job before any phase-1
+// tile), so by the time a phase-p tile is taken, every tile it depends on is
+// already held by a running CTA.  A tile of phase p >= 1 of limb l waits for
+// the phase p-1 tiles of the same limb (per-limb completion counters,
+// release/acquire at device scope); the wait is bounded and, if it ever runs
+// out, the CTA records AXHEL's timeout status in the batch's error word and
+// stops.  Data written by other CTAs of the launch is read through L2
+// (ld.global.cg), never through a possibly stale L1 line.
+//
+// Each tile is 1024 residues handled by 128 threads x 8 registers
+// (LR = 3): 2^(10-LG) groups of 2^LG for the pass widths LG = 5..9 of the
+// degrees 2^10 .. 2^17 (a tile never spans two limbs or two blocks).
+// The same tile functions as the plain kernels run the butterflies
+// (ntt_kernels.cuh), so every job's result equals the per-limb calls bit for
+// bit.
+#include <cuda/atomic>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/axhel_cuda.h"
+#include "internal.h"
+#include "launch.h"
+#include "ntt_kernels.cuh"
+
+namespace axhel_impl {
+
+constexpr int kBatchThreads = 128;
+constexpr int kBatchLR = 3;
+constexpr int kBatchTileWords = kBatchThreads << kBatchLR;  // 1024 residues
+constexpr int kBatchMinLG = 5, kBatchMaxLG = 9;
+
+enum BatchKind : uint32_t { kJobForward = 1, kJobInverse = 2, kJobChainMul = 3, kJobChainFma = 4 };
+
+struct BatchJob {
+    const uint64_t* src;
+    uint64_t* dst;
+    const uint64_t* vec;              // chain multiplicand / addend (may be null for FMA)
+    const ModCtx* const* ctx;         // nmods device pointers
+    const uint64_t* scalars;          // chain FMA scalars (nmods), device
+    uint64_t count;                   // limbs
+    uint64_t done_off;                // first completion counter of this job (count per phase)
+    uint32_t kind, logn, nmods, nphase;
+    uint32_t lg_col, lg_row;          // pass widths A (strided) and B (contiguous)
+    uint32_t tiles_per_limb[3];
+    uint32_t pre, norm;               // fuse ReduceMod(4,2) on load / normalize the output
+    uint32_t wait_extra;              // added to every dependency target (0; a test sets 1 to force a timeout)
+    uint32_t pad;
+};
+
+struct BatchEntry {
+    uint64_t tile_begin;  // first global tile of (job, phase)
+    uint32_t job, phase;
+};
+
+struct BatchArgs {
+    const BatchJob* jobs;
+    const BatchEntry* entries;
+    uint32_t nentries;
+    uint64_t total_tiles;
+    unsigned int* done;                 // per (job, phase, limb) completed tiles
+    unsigned long long* next_tile;      // work counter
+    int* error;                         // AXHEL_OK or AXHEL_ERR_TIMEOUT
+    uint64_t wait_ns;                   // a dependency wait gives up after this long
+};
+
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Per-phase pass of a job: direction, width and first stage.
+struct PhaseCfg {
+    bool inv, chain;
+    uint32_t lg, s0;
+};
+
+__device__ __forceinline__ PhaseCfg phase_cfg(const BatchJob& j, uint32_t p)
+{
+    PhaseCfg c{false, false, 0, 0};
+    if (j.kind == kJobForward) {
+        c.lg = p == 0 ? j.lg_col : j.lg_row;
+        c.s0 = p == 0 ? 0 : j.lg_col;
+    } else if (j.kind == kJobInverse) {
+        c.inv = true;
+        c.lg = p == 0 ? j.lg_row : j.lg_col;
+        c.s0 = p == 0 ? 0 : j.lg_row;
+    } else {  // chain
+        if (p == 0) {
+            c.inv = true;
+            c.lg = j.lg_row;
+            c.s0 = 0;
+        } else if (p == 1) {
+            c.chain = true;
+            c.lg = j.lg_col;
+            c.s0 = j.lg_row;
+        } else {
+            c.lg = j.lg_row;
+            c.s0 = j.lg_col;
+        }
+    }
+    return c;
+}
+
+template <int LG>
+__device__ __forceinline__ void run_tile_lg(const BatchJob& j, const PhaseCfg& c, uint32_t p, uint64_t limb,
+                                            uint64_t tile_in_limb, uint64_t* sm)
+{
+    constexpr uint32_t lgtg = 10 - LG;  // 1024 / 2^LG groups per tile
+    const uint32_t mi = (uint32_t)(limb % j.nmods);
+    const ModCtx* cx = j.ctx[mi];
+    const bool first = p == 0, last = p + 1 == j.nphase;
+    const uint64_t* src = first ? j.src : j.dst;
+    uint32_t flags = (first && j.pre) ? kPreCsub2q : 0;
+    if (last) flags |= kLastPass | (j.norm ? kPostNorm : 0);
+    if (c.chain) {
+        const uint32_t op = j.kind == kJobChainMul ? kChainMul : kChainFma;
+        const uint64_t sc = j.kind == kJobChainFma ? j.scalars[mi] : 0;
+        chain_tile<LG, kBatchLR, true>(src, j.dst, j.vec, cx, op, sc, j.logn, lgtg, limb, tile_in_limb,
+                                        (first && j.pre ? kPreCsub2q : 0) | (last && j.norm ? kPostNorm : 0), sm);
+    } else if (c.inv) {
+        // the inverse's last pass holds the N^-1 stage even inside a chain
+        const uint32_t f = flags | (c.s0 + LG == j.logn ? kLastPass : 0);
+        pass_tile<true, LG, kBatchLR, true>(src, j.dst, cx, j.logn, c.s0, lgtg, limb, tile_in_limb, f, sm);
+    } else {
+        pass_tile<false, LG, kBatchLR, true>(src, j.dst, cx, j.logn, c.s0, lgtg, limb, tile_in_limb, flags, sm);
+    }
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batch_kernel(const __grid_constant__ BatchArgs a)
+{
+    __shared__ uint64_t sm[kBatchTileWords + 128];
+    __shared__ unsigned long long s_tile;
+    __shared__ int s_abort;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            s_tile = atomicAdd(a.next_tile, 1ull);
+            s_abort = 0;
+        }
+        __syncthreads();
+        const uint64_t tile = s_tile;
+        if (tile >= a.total_tiles) break;
+        // (job, phase) of this tile: last entry with tile_begin <= tile
+        uint32_t lo = 0, hi = a.nentries;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (a.entries[mid].tile_begin <= tile) lo = mid; else hi = mid;
+        }
+        const BatchEntry e = a.entries[lo];
+        const BatchJob& j = a.jobs[e.job];
+        const uint64_t lt = tile - e.tile_begin;
+        const uint32_t tpl = j.tiles_per_limb[e.phase];
+        const uint64_t limb = lt / tpl;
+        const uint64_t til = lt - limb * tpl;
+        if (e.phase > 0 && threadIdx.x == 0) {
+            cuda::atomic_ref<unsigned int, cuda::thread_scope_device> dep(
+                a.done[j.done_off + (uint64_t)(e.phase - 1) * j.count + limb]);
+            const unsigned need = j.tiles_per_limb[e.phase - 1] + j.wait_extra;
+            const uint64_t t0 = global_ns();
+            uint32_t polls = 0;
+            while (dep.load(cuda::memory_order_acquire) < need) {
+                // bounded in wall time and in polls
+                if (++polls > (1u << 24) || global_ns() - t0 > a.wait_ns) {
+                    atomicExch(a.error, AXHEL_ERR_TIMEOUT);
+                    s_abort = 1;
+                    break;
+                }
+                __nanosleep(100);
+            }
+        }
+        __syncthreads();
+        if (s_abort) break;
+        const PhaseCfg c = phase_cfg(j, e.phase);
+        switch (c.lg) {
+        case 5: run_tile_lg<5>(j, c, e.phase, limb, til, sm); break;
+        case 6: run_tile_lg<6>(j, c, e.phase, limb, til, sm); break;
+        case 7: run_tile_lg<7>(j, c, e.phase, limb, til, sm); break;
+        case 8: run_tile_lg<8>(j, c, e.phase, limb, til, sm); break;
+        case 9: run_tile_lg<9>(j, c, e.phase, limb, til, sm); break;
+        default: break;
+        }
+        __threadfence();  // this thread's stores, before the tile is published
+        __syncthreads();
+        if (threadIdx.x == 0 && e.phase + 1 < j.nphase) {
+            cuda::atomic_ref<unsigned int, cuda::thread_scope_device> done(
+                a.done[j.done_off + (uint64_t)e.phase * j.count + limb]);
+            done.fetch_add(1u, cuda::memory_order_release);
+        }
+    }
+}
+
+}  // namespace axhel_impl
+
+using namespace axhel_impl;
+
+// ------------------------------------------------------------------ host
+
+struct axhel_batch {
+    int device = 0;
+    void* mem = nullptr;  // descriptors | entries | ctx tables | scalars | done | counter | error
+    size_t bytes = 0;
+    size_t zero_off = 0, zero_bytes = 0;  // counters cleared before every launch
+    BatchArgs args{};
+    unsigned grid = 0;
+    std::vector<axhel_ntt_t> held;  // table contexts kept alive while the batch exists
+    cudaGraphExec_t graph = nullptr;
+    cudaStream_t graph_stream = nullptr;
+};
+
+namespace {
+
+thread_local std::string t_batch_error;
+
+axhel_status_t bfail(axhel_status_t st, const std::string& m)
+{
+    t_batch_error = m;
+    return st;
+}
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+int batch_grid()
+{
+    static int cached = 0;
+    if (!cached) {
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, kBatchThreads, 0);
+        if (per_sm < 1) per_sm = 1;
+        cached = per_sm * sm_count();
+    }
+    return cached;
+}
+
+}  // namespace
+
+namespace axhel_impl {
+
+// Host layout of a batch: fills `host` (to be copied to the device at `base`)
+// and the kernel arguments.  Shared by the allocating and the static-scratch
+// entry points.
+axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned char* base,
+                           std::vector<unsigned char>& host, size_t* zero_off, size_t* zero_bytes, BatchArgs* args,
+                           std::vector<axhel_ntt_t>* held, std::string* err)
+{
+    if (!jobs || n_jobs == 0) {
+        *err = "empty batch";
+        return AXHEL_ERR_INVALID;
+    }
+    std::vector<BatchJob> bj(n_jobs);
+    std::vector<std::vector<const ModCtx*>> ctxs(n_jobs);
+    std::vector<std::vector<uint64_t>> scal(n_jobs);
+    uint64_t done_total = 0;
+    for (uint64_t i = 0; i < n_jobs; ++i) {
+        const axhel_job_t& J = jobs[i];
+        BatchJob& b = bj[i];
+        std::memset(&b, 0, sizeof b);
+        if (J.kind < AXHEL_JOB_FORWARD || J.kind > AXHEL_JOB_CHAIN_FMA) {
+            *err = "job " + std::to_string(i) + ": unknown kind";
+            return AXHEL_ERR_INVALID;
+        }
+        if (!J.ntts || J.n_ntts == 0 || J.n_ntts > 1024) {
+            *err = "job " + std::to_string(i) + ": 1..1024 NTT handles needed";
+            return AXHEL_ERR_INVALID;
+        }
+        const uint64_t n = J.ntts[0] ? J.ntts[0]->n : 0;
+        for (uint32_t m = 0; m < J.n_ntts; ++m) {
+            if (!J.ntts[m] || J.ntts[m]->n != n) {
+                *err = "job " + std::to_string(i) + ": handles must share one degree";
+                return AXHEL_ERR_INVALID;
+            }
+            ctxs[i].push_back(J.ntts[m]->dctx);
+            if (held) held->push_back(J.ntts[m]);
+        }
+        const uint32_t logn = J.ntts[0]->logn;
+        if (logn < 10 || logn > 17) {
+            *err = "job " + std::to_string(i) + ": batched degree must be in [2^10, 2^17]";
+            return AXHEL_ERR_UNSUPPORTED;
+        }
+        if (J.count && (!J.result || !J.operand)) {
+            *err = "job " + std::to_string(i) + ": null data pointer";
+            return AXHEL_ERR_INVALID;
+        }
+        if (J.kind == AXHEL_JOB_CHAIN_MUL && J.count && !J.vector) {
+            *err = "job " + std::to_string(i) + ": chain multiplicand missing";
+            return AXHEL_ERR_INVALID;
+        }
+        if (J.kind == AXHEL_JOB_CHAIN_FMA) {
+            if (!J.scalars) {
+                *err = "job " + std::to_string(i) + ": chain scalars missing";
+                return AXHEL_ERR_INVALID;
+            }
+            scal[i].assign(J.scalars, J.scalars + J.n_ntts);
+        }
+        b.kind = J.kind;
+        b.logn = logn;
+        b.count = J.count;
+        b.nmods = J.n_ntts;
+        b.src = J.operand;
+        b.dst = J.result;
+        b.vec = J.vector;
+        b.lg_col = (logn + 1) / 2;
+        b.lg_row = logn - b.lg_col;
+        const bool inv_first = J.kind != AXHEL_JOB_FORWARD;
+        b.pre = inv_first && J.input_mod_factor == 4;
+        b.norm = (J.kind == AXHEL_JOB_INVERSE) ? (J.output_mod_factor != 2) : (J.output_mod_factor != 4);
+        b.nphase = (J.kind == AXHEL_JOB_CHAIN_MUL || J.kind == AXHEL_JOB_CHAIN_FMA) ? 3 : 2;
+        const uint32_t lgs_fwd[2] = {b.lg_col, b.lg_row};
+        for (uint32_t p = 0; p < b.nphase; ++p) {
+            uint32_t lg;
+            if (J.kind == AXHEL_JOB_FORWARD) lg = lgs_fwd[p];
+            else if (J.kind == AXHEL_JOB_INVERSE) lg = p == 0 ? b.lg_row : b.lg_col;
+            else lg = p == 1 ? b.lg_col : b.lg_row;
+            if (lg < (uint32_t)kBatchMinLG || lg > (uint32_t)kBatchMaxLG || (1ull << logn) % kBatchTileWords) {
+                *err = "job " + std::to_string(i) + ": degree outside the batched range";
+                return AXHEL_ERR_UNSUPPORTED;
+            }
+            b.tiles_per_limb[p] = (uint32_t)((1ull << logn) / kBatchTileWords);
+        }
+        b.done_off = done_total;
+        done_total += (uint64_t)(b.nphase - 1) * b.count;
+    }
+    // phase-major tile order
+    std::vector<BatchEntry> ent;
+    uint64_t tiles = 0;
+    for (uint32_t p = 0; p < 3; ++p)
+        for (uint64_t i = 0; i < n_jobs; ++i) {
+            if (p >= bj[i].nphase || bj[i].count == 0) continue;
+            ent.push_back(BatchEntry{tiles, (uint32_t)i, p});
+            tiles += bj[i].count * bj[i].tiles_per_limb[p];
+        }
+    if (ent.empty()) {
+        *err = "";
+        args->total_tiles = 0;
+        return AXHEL_OK;
+    }
+    // device image
+    size_t off = 0;
+    const size_t jobs_off = off;
+    off = align_up(off + n_jobs * sizeof(BatchJob), 256);
+    const size_t ent_off = off;
+    off = align_up(off + ent.size() * sizeof(BatchEntry), 256);
+    std::vector<size_t> ctx_off(n_jobs), sc_off(n_jobs, 0);
+    for (uint64_t i = 0; i < n_jobs; ++i) {
+        ctx_off[i] = off;
+        off = align_up(off + ctxs[i].size() * sizeof(void*), 16);
+        if (!scal[i].empty()) {
+            sc_off[i] = off;
+            off = align_up(off + scal[i].size() * 8, 16);
+        }
+    }
+    off = align_up(off, 256);
+    *zero_off = off;
+    const size_t done_off = off;
+    off = align_up(off + done_total * sizeof(unsigned), 16);
+    const size_t ctr_off = off;
+    off += 16;
+    const size_t err_off = off;
+    off = align_up(off + 16, 256);
+    *zero_bytes = off - *zero_off;
+    host.assign(off, 0);
+    for (uint64_t i = 0; i < n_jobs; ++i) {
+        bj[i].ctx = reinterpret_cast<const ModCtx* const*>(base + ctx_off[i]);
+        bj[i].scalars = scal[i].empty() ? nullptr : reinterpret_cast<const uint64_t*>(base + sc_off[i]);
+        std::memcpy(host.data() + ctx_off[i], ctxs[i].data(), ctxs[i].size() * sizeof(void*));
+        if (!scal[i].empty()) std::memcpy(host.data() + sc_off[i], scal[i].data(), scal[i].size() * 8);
+    }
+    std::memcpy(host.data() + jobs_off, bj.data(), n_jobs * sizeof(BatchJob));
+    std::memcpy(host.data() + ent_off, ent.data(), ent.size() * sizeof(BatchEntry));
+    args->jobs = reinterpret_cast<const BatchJob*>(base + jobs_off);
+    args->entries = reinterpret_cast<const BatchEntry*>(base + ent_off);
+    args->nentries = (uint32_t)ent.size();
+    args->total_tiles = tiles;
+    args->done = reinterpret_cast<unsigned*>(base + done_off);
+    args->next_tile = reinterpret_cast<unsigned long long*>(base + ctr_off);
+    args->error = reinterpret_cast<int*>(base + err_off);
+    args->wait_ns = 2000000000ull;  // 2 s
+    return AXHEL_OK;
+}
+
+cudaError_t batch_launch_args(const BatchArgs& a, cudaStream_t s)
+{
+    if (a.total_tiles == 0) return cudaSuccess;
+    uint64_t grid = (uint64_t)batch_grid();
+    if (grid > a.total_tiles) grid = a.total_tiles;
+    count_launch();
+    ProfScope prof(s, "batch_kernel");
+    batch_kernel<<<(unsigned)grid, kBatchThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace axhel_impl
+
+extern "C" {
+
+axhel_status_t axhel_cuda_batch_create(const axhel_job_t* jobs, uint64_t n_jobs, axhel_batch_t* out)
+{
+    if (!out) return bfail(AXHEL_ERR_INVALID, "null output");
+    *out = nullptr;
+    auto b = std::make_unique<axhel_batch>();
+    cudaGetDevice(&b->device);
+    // first pass for the size, then with the real base address
+    std::vector<unsigned char> img;
+    BatchArgs args{};
+    std::string err;
+    std::vector<axhel_ntt_t> held;
+    axhel_status_t st = batch_build(jobs, n_jobs, nullptr, img, &b->zero_off, &b->zero_bytes, &args, nullptr, &err);
+    if (st) return bfail(st, err);
+    b->bytes = img.size();
+    if (b->bytes) {
+        cudaError_t e = cudaMalloc(&b->mem, b->bytes);
+        if (e != cudaSuccess) return bfail(AXHEL_ERR_NOMEM, std::string("cudaMalloc(batch): ") + cudaGetErrorString(e));
+        st = batch_build(jobs, n_jobs, static_cast<unsigned char*>(b->mem), img, &b->zero_off, &b->zero_bytes,
+                         &b->args, &held, &err);
+        if (st) {
+            cudaFree(b->mem);
+            return bfail(st, err);
+        }
+        e = cudaMemcpy(b->mem, img.data(), img.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(b->mem);
+            return bfail(AXHEL_ERR_CUDA, std::string("cudaMemcpy(batch): ") + cudaGetErrorString(e));
+        }
+    } else {
+        b->args = args;
+    }
+    for (axhel_ntt_t h : held) axhel_cuda_ntt_retain(h);
+    b->held = std::move(held);
+    *out = b.release();
+    return AXHEL_OK;
+}
+
+axhel_status_t axhel_cuda_batch_launch(axhel_batch_t b, void* stream)
+{
+    if (!b) return bfail(AXHEL_ERR_INVALID, "null batch");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (b->args.total_tiles == 0) return AXHEL_OK;
+    cudaError_t e = cudaMemsetAsync(static_cast<unsigned char*>(b->mem) + b->zero_off, 0, b->zero_bytes, s);
+    if (e == cudaSuccess) e = batch_launch_args(b->args, s);
+    if (e != cudaSuccess) return bfail(AXHEL_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
+    return AXHEL_OK;
+}
+
+axhel_status_t axhel_cuda_batch_graph_launch(axhel_batch_t b, void* stream)
+{
+    if (!b) return bfail(AXHEL_ERR_INVALID, "null batch");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (b->args.total_tiles == 0) return AXHEL_OK;
+    if (!b->graph) {
+        cudaStream_t cap;
+        if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess)
+            return bfail(AXHEL_ERR_CUDA, "stream create");
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            cudaMemsetAsync(static_cast<unsigned char*>(b->mem) + b->zero_off, 0, b->zero_bytes, cap);
+            batch_launch_args(b->args, cap);
+            e = cudaStreamEndCapture(cap, &g);
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph, g, 0);
+        if (g) cudaGraphDestroy(g);
+        cudaStreamDestroy(cap);
+        if (e != cudaSuccess) return bfail(AXHEL_ERR_CUDA, std::string("batch graph: ") + cudaGetErrorString(e));
+    }
+    count_launch();
+    cudaError_t e = cudaGraphLaunch(b->graph, s);
+    if (e != cudaSuccess) return bfail(AXHEL_ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(e));
+    return AXHEL_OK;
+}
+
+axhel_status_t axhel_cuda_batch_status(axhel_batch_t b, void* stream)
+{
+    if (!b) return bfail(AXHEL_ERR_INVALID, "null batch");
+    if (b->args.total_tiles == 0) return AXHEL_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int err = 0;
+    cudaError_t e = cudaMemcpyAsync(&err, b->args.error, sizeof err, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return bfail(AXHEL_ERR_CUDA, std::string("batch status: ") + cudaGetErrorString(e));
+    if (err) return bfail(err, "a dependency wait in the batch kernel timed out");
+    return AXHEL_OK;
+}
+
+axhel_status_t axhel_cuda_batch_destroy(axhel_batch_t b)
+{
+    if (!b) return AXHEL_OK;
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    if (b->mem) cudaFree(b->mem);
+    for (axhel_ntt_t h : b->held) axhel_cuda_ntt_release(h);
+    delete b;
+    return AXHEL_OK;
+}
+
+axhel_status_t axhel_cuda_batch_run(const axhel_job_t* jobs, uint64_t n_jobs, void* stream)
+{
+    axhel_batch_t b = nullptr;
+    axhel_status_t st = axhel_cuda_batch_create(jobs, n_jobs, &b);
+    if (st) return st;
+    st = axhel_cuda_batch_launch(b, stream);
+    if (!st) st = axhel_cuda_batch_status(b, stream);
+    axhel_cuda_batch_destroy(b);
+    return st;
+}
+
+const char* axhel_cuda_batch_last_error(void) { return t_batch_error.c_str(); }
+
+axhel_status_t axhel_cuda_batch_set_wait_ns(axhel_batch_t b, uint64_t ns)
+{
+    if (!b) return bfail(AXHEL_ERR_INVALID, "null batch");
+    if (ns < 1000000ull || ns > 10000000000ull) return bfail(AXHEL_ERR_INVALID, "wait bound must be 1 ms .. 10 s");
+    b->args.wait_ns = ns;
+    if (b->graph) {  // the captured launch holds the old arguments
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return AXHEL_OK;
+}
+
+axhel_status_t axhel_cuda_batch_debug_unreachable(axhel_batch_t b, uint64_t job)
+{
+    if (!b || b->args.total_tiles == 0) return bfail(AXHEL_ERR_INVALID, "empty batch");
+    // the job descriptors sit at the start of the batch allocation
+    BatchJob* d = const_cast<BatchJob*>(b->args.jobs) + job;
+    BatchJob host;
+    cudaError_t e = cudaMemcpy(&host, d, sizeof host, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return bfail(AXHEL_ERR_CUDA, cudaGetErrorString(e));
+    host.wait_extra = 1;
+    e = cudaMemcpy(d, &host, sizeof host, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return bfail(AXHEL_ERR_CUDA, cudaGetErrorString(e));
+    return AXHEL_OK;
+}
+
+}  // extern "C"

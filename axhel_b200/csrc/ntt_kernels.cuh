@@ -79,14 +79,14 @@ struct Tile {
     bool strided;   // S > 1
 };
 
+// Tile `tile_in_limb` of limb `limb` for a pass with group stride 2^lgS and
+// 2^lgtg groups per tile.
 template <int LG>
-__device__ __forceinline__ Tile make_tile(uint32_t logn, uint32_t lgS, uint32_t lgtg)
+__device__ __forceinline__ Tile make_tile(uint32_t lgS, uint32_t lgtg, uint64_t limb, uint64_t tile_in_limb)
 {
     Tile t;
-    const uint32_t lg_tiles = logn - LG - lgtg;  // log2 tiles per limb
-    const uint64_t tile = blockIdx.x;
-    t.limb = tile >> lg_tiles;
-    t.g0 = (tile & ((1ull << lg_tiles) - 1)) << lgtg;
+    t.limb = limb;
+    t.g0 = tile_in_limb << lgtg;
     t.lgS = lgS;
     t.lgtg = lgtg;
     t.strided = lgS != 0;
@@ -130,7 +130,22 @@ __device__ __forceinline__ uint32_t round_base(uint32_t k, int lo)
 
 // ------------------------------------------------------- global <-> registers
 
-template <int LG, int LR, int LO>
+// Loads with CG = true bypass L1 (ld.global.cg): used when the data was
+// written by other CTAs of the same launch (the persistent batch kernel).
+template <bool CG>
+__device__ __forceinline__ uint64_t ld64(const uint64_t* p)
+{
+    if constexpr (CG) return __ldcg(reinterpret_cast<const unsigned long long*>(p));
+    return *p;
+}
+template <bool CG>
+__device__ __forceinline__ ulonglong2 ld128(const ulonglong2* p)
+{
+    if constexpr (CG) return __ldcg(p);
+    return *p;
+}
+
+template <int LG, int LR, int LO, bool CG = false>
 __device__ __forceinline__ void load_global(uint64_t (&v)[1 << LR], const uint64_t* __restrict__ limb_src,
                                             const Tile& t, uint32_t gi, uint32_t rb, bool vec_ok)
 {
@@ -138,19 +153,19 @@ __device__ __forceinline__ void load_global(uint64_t (&v)[1 << LR], const uint64
     if (t.strided) {
         const uint64_t* p = limb_src + t.base + gi + ((uint64_t)rb << t.lgS);
 #pragma unroll
-        for (int i = 0; i < R; ++i) v[i] = p[(uint64_t)i << (LO + t.lgS)];
+        for (int i = 0; i < R; ++i) v[i] = ld64<CG>(p + ((uint64_t)i << (LO + t.lgS)));
     } else if (LO == 0 && vec_ok) {
         const ulonglong2* p = reinterpret_cast<const ulonglong2*>(limb_src + t.base + ((uint64_t)gi << LG) + rb);
 #pragma unroll
         for (int i = 0; i < R / 2; ++i) {
-            const ulonglong2 w = p[i];
+            const ulonglong2 w = ld128<CG>(p + i);
             v[2 * i] = w.x;
             v[2 * i + 1] = w.y;
         }
     } else {
         const uint64_t* p = limb_src + t.base + ((uint64_t)gi << LG) + rb;
 #pragma unroll
-        for (int i = 0; i < R; ++i) v[i] = p[i << LO];
+        for (int i = 0; i < R; ++i) v[i] = ld64<CG>(p + (i << LO));
     }
 }
 
@@ -303,41 +318,126 @@ __device__ __forceinline__ void run_rounds(uint64_t (&v)[1 << LR], uint64_t* smg
 
 // ------------------------------------------------------------------ kernels
 
-template <bool INV, int LG, int LR>
-__global__ void __launch_bounds__(max_threads(LR)) ntt_pass_kernel(const __grid_constant__ PassArgs a)
+// One tile of a pass: stages [s0, s0 + LG) of limb `limb`.  `sm` holds
+// 2^lgtg groups of 2^LG + 1 words; all threads of the CTA take part.
+template <bool INV, int LG, int LR, bool CG>
+__device__ __forceinline__ void pass_tile(const uint64_t* src, uint64_t* dst, const ModCtx* cx, uint32_t logn,
+                                          uint32_t s0, uint32_t lgtg, uint64_t limb, uint64_t tile_in_limb,
+                                          uint32_t flags, uint64_t* sm)
 {
-    extern __shared__ uint64_t sm[];
     constexpr int R = 1 << LR;
     constexpr int GP = (1 << LG) + 1;
     constexpr int NR = num_rounds<LG, LR>();
     constexpr int LO_FIRST = round_lo<INV, LG, LR, 0>();
     constexpr int LO_LAST = round_lo<INV, LG, LR, NR - 1>();
-    const uint32_t logn = a.logn;
-    const uint32_t lgS = INV ? a.s0 : (logn - a.s0 - LG);
-    const Tile t = make_tile<LG>(logn, lgS, __ffs(a.tg) - 1);
-    const ModCtx* cx = a.ctx[t.limb % a.nctx];
+    const uint32_t lgS = INV ? s0 : (logn - s0 - LG);
+    const Tile t = make_tile<LG>(lgS, lgtg, limb, tile_in_limb);
     const uint64_t q = cx->q, q2 = cx->q2;
     const uint64_t n = 1ull << logn;
-    const uint64_t* src = a.src + (t.limb << logn);
-    uint64_t* dst = a.dst + (t.limb << logn);
-    const bool vec_ok = ((reinterpret_cast<uintptr_t>(a.src) | reinterpret_cast<uintptr_t>(a.dst)) & 15) == 0;
+    const uint64_t* lsrc = src + (limb << logn);
+    uint64_t* ldst = dst + (limb << logn);
+    const bool vec_ok = ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0;
 
     uint32_t gi, k;
     thread_role<LG, LR>(t, gi, k);
     const uint64_t blk = tile_blk<LG>(t, gi);
 
     uint64_t v[R];
-    load_global<LG, LR, LO_FIRST>(v, src, t, gi, round_base<LR>(k, LO_FIRST), vec_ok);
-    if (a.flags & kPreCsub2q) {
+    load_global<LG, LR, LO_FIRST, CG>(v, lsrc, t, gi, round_base<LR>(k, LO_FIRST), vec_ok);
+    if (flags & kPreCsub2q) {
 #pragma unroll
         for (int i = 0; i < R; ++i) v[i] = csub_lazy(v[i], q2);
     }
-    run_rounds<INV, LG, LR>(v, sm + gi * GP, k, blk, a.s0, n, cx, q, q2, (a.flags & kLastPass) != 0);
-    if (a.flags & kPostNorm) {
+    run_rounds<INV, LG, LR>(v, sm + gi * GP, k, blk, s0, n, cx, q, q2, (flags & kLastPass) != 0);
+    if (flags & kPostNorm) {
 #pragma unroll
         for (int i = 0; i < R; ++i) v[i] = INV ? csub_lazy(v[i], q) : csub_lazy(csub_lazy(v[i], q2), q);
     }
-    store_global<LG, LR, LO_LAST>(v, dst, t, gi, round_base<LR>(k, LO_LAST), vec_ok);
+    store_global<LG, LR, LO_LAST>(v, ldst, t, gi, round_base<LR>(k, LO_LAST), vec_ok);
+}
+
+template <bool INV, int LG, int LR>
+__global__ void __launch_bounds__(max_threads(LR)) ntt_pass_kernel(const __grid_constant__ PassArgs a)
+{
+    extern __shared__ uint64_t sm[];
+    const uint32_t lgtg = __ffs(a.tg) - 1;
+    const uint32_t lg_tiles = a.logn - LG - lgtg;  // log2 tiles per limb
+    const uint64_t tile = blockIdx.x;
+    const uint64_t limb = tile >> lg_tiles;
+    pass_tile<INV, LG, LR, false>(a.src, a.dst, a.ctx[limb % a.nctx], a.logn, a.s0, lgtg, limb,
+                                  tile & ((1ull << lg_tiles) - 1), a.flags, sm);
+}
+
+// Fused column pass of an INTT -> op -> NTT chain: the inverse's last pass
+// (stages logn-LG .. logn-1, incl. the N^-1 final stage) and the forward's
+// first pass (stages 0 .. LG-1) act on the same groups p = r*S + col, and the
+// inverse's last round holds the same register bits as the forward's first
+// round, so the element-wise op runs in registers between them.
+template <int LG, int LR, bool CG>
+__device__ __forceinline__ void chain_tile(const uint64_t* src, uint64_t* dst, const uint64_t* operand,
+                                           const ModCtx* cx, uint32_t op, uint64_t scalar, uint32_t logn,
+                                           uint32_t lgtg, uint64_t limb, uint64_t tile_in_limb, uint32_t flags,
+                                           uint64_t* sm)
+{
+    constexpr int R = 1 << LR;
+    constexpr int GP = (1 << LG) + 1;
+    constexpr int NR = num_rounds<LG, LR>();
+    constexpr int LO_FIRST = round_lo<true, LG, LR, 0>();
+    constexpr int LO_MID = round_lo<true, LG, LR, NR - 1>();
+    constexpr int LO_LAST = round_lo<false, LG, LR, NR - 1>();
+    static_assert(LO_MID == round_lo<false, LG, LR, 0>(), "inverse last round and forward first round differ");
+    const Tile t = make_tile<LG>(logn - LG, lgtg, limb, tile_in_limb);
+    const uint64_t q = cx->q, q2 = cx->q2;
+    const uint64_t n = 1ull << logn;
+    const uint64_t* lsrc = src + (limb << logn);
+    uint64_t* ldst = dst + (limb << logn);
+    const bool vec_ok = ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst) |
+                          reinterpret_cast<uintptr_t>(operand)) & 15) == 0;
+
+    uint32_t gi, k;
+    thread_role<LG, LR>(t, gi, k);
+    const uint64_t blk = tile_blk<LG>(t, gi);
+    uint64_t* smg = sm + gi * GP;
+
+    uint64_t v[R];
+    load_global<LG, LR, LO_FIRST, CG>(v, lsrc, t, gi, round_base<LR>(k, LO_FIRST), vec_ok);
+    if (flags & kPreCsub2q) {
+#pragma unroll
+        for (int i = 0; i < R; ++i) v[i] = csub_lazy(v[i], q2);
+    }
+    run_rounds<true, LG, LR>(v, smg, k, blk, logn - LG, n, cx, q, q2, true);
+
+    // Element-wise op on the inverse output (lazy [0, 2q)) with factor-2
+    // inputs: EltwiseMulModNative<2> / EltwiseFMAModNative<2> formulas.
+    const uint64_t mu = cx->mu;
+    const uint32_t shift = cx->shift;
+    const uint32_t rb = round_base<LR>(k, LO_MID);
+    if (op == kChainMul) {
+        uint64_t m[R];
+        load_global<LG, LR, LO_MID, false>(m, operand + (limb << logn), t, gi, rb, vec_ok);
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+            v[i] = barrett_mul(reduce_input<2>(v[i], q), reduce_input<2>(m[i], q), q, mu, shift);
+    } else if (op == kChainFma) {
+        const uint64_t sc = reduce_input<2>(scalar, q);
+#pragma unroll
+        for (int i = 0; i < R; ++i) v[i] = barrett_mul(reduce_input<2>(v[i], q), sc, q, mu, shift);
+        if (operand) {
+            uint64_t m[R];
+            load_global<LG, LR, LO_MID, false>(m, operand + (limb << logn), t, gi, rb, vec_ok);
+#pragma unroll
+            for (int i = 0; i < R; ++i) v[i] = csub(v[i] + reduce_input<2>(m[i], q), q);
+        }
+    }
+
+    // The forward's first pass: stages 0 .. LG-1 of block 0.
+    fwd_stages<LG, LR, 0>(v, rb, 0, 0, cx->fwd, q, q2);
+    fwd_rest<LG, LR>(std::make_integer_sequence<int, NR - 1>{}, v, smg, k, 0, 0, cx->fwd, q, q2);
+    if (flags & kPostNorm) {
+#pragma unroll
+        for (int i = 0; i < R; ++i) v[i] = csub_lazy(csub_lazy(v[i], q2), q);
+    }
+    store_global<LG, LR, LO_LAST>(v, ldst, t, gi, round_base<LR>(k, LO_LAST), vec_ok);
 }
 
 // Fused column pass of an INTT -> op -> NTT chain: the inverse's last pass
@@ -349,69 +449,14 @@ template <int LG, int LR>
 __global__ void __launch_bounds__(max_threads(LR)) ntt_chain_kernel(const __grid_constant__ ChainArgs c)
 {
     extern __shared__ uint64_t sm[];
-    constexpr int R = 1 << LR;
-    constexpr int GP = (1 << LG) + 1;
-    constexpr int NR = num_rounds<LG, LR>();
-    constexpr int LO_FIRST = round_lo<true, LG, LR, 0>();
-    constexpr int LO_MID = round_lo<true, LG, LR, NR - 1>();
-    constexpr int LO_LAST = round_lo<false, LG, LR, NR - 1>();
-    static_assert(LO_MID == round_lo<false, LG, LR, 0>(), "inverse last round and forward first round differ");
     const PassArgs& a = c.pass;
-    const uint32_t logn = a.logn;
-    const Tile t = make_tile<LG>(logn, logn - LG, __ffs(a.tg) - 1);
-    const uint32_t mi = t.limb % a.nctx;
-    const ModCtx* cx = a.ctx[mi];
-    const uint64_t q = cx->q, q2 = cx->q2;
-    const uint64_t n = 1ull << logn;
-    const uint64_t* src = a.src + (t.limb << logn);
-    uint64_t* dst = a.dst + (t.limb << logn);
-    const bool vec_ok = ((reinterpret_cast<uintptr_t>(a.src) | reinterpret_cast<uintptr_t>(a.dst) |
-                          reinterpret_cast<uintptr_t>(c.operand)) & 15) == 0;
-
-    uint32_t gi, k;
-    thread_role<LG, LR>(t, gi, k);
-    const uint64_t blk = tile_blk<LG>(t, gi);
-    uint64_t* smg = sm + gi * GP;
-
-    uint64_t v[R];
-    load_global<LG, LR, LO_FIRST>(v, src, t, gi, round_base<LR>(k, LO_FIRST), vec_ok);
-    if (a.flags & kPreCsub2q) {
-#pragma unroll
-        for (int i = 0; i < R; ++i) v[i] = csub_lazy(v[i], q2);
-    }
-    run_rounds<true, LG, LR>(v, smg, k, blk, logn - LG, n, cx, q, q2, true);
-
-    // Element-wise op on the inverse output (lazy [0, 2q)) with factor-2
-    // inputs: EltwiseMulMod<2> / EltwiseFMAMod<2> semantics.
-    const uint64_t mu = cx->mu;
-    const uint32_t shift = cx->shift;
-    const uint32_t rb = round_base<LR>(k, LO_MID);
-    if (c.op == kChainMul) {
-        uint64_t m[R];
-        load_global<LG, LR, LO_MID>(m, c.operand + (t.limb << logn), t, gi, rb, vec_ok);
-#pragma unroll
-        for (int i = 0; i < R; ++i)
-            v[i] = barrett_mul(reduce_input<2>(v[i], q), reduce_input<2>(m[i], q), q, mu, shift);
-    } else if (c.op == kChainFma) {
-        const uint64_t sc = reduce_input<2>(c.scalar[mi], q);
-#pragma unroll
-        for (int i = 0; i < R; ++i) v[i] = barrett_mul(reduce_input<2>(v[i], q), sc, q, mu, shift);
-        if (c.operand) {
-            uint64_t m[R];
-            load_global<LG, LR, LO_MID>(m, c.operand + (t.limb << logn), t, gi, rb, vec_ok);
-#pragma unroll
-            for (int i = 0; i < R; ++i) v[i] = csub(v[i] + reduce_input<2>(m[i], q), q);
-        }
-    }
-
-    // The forward's first pass: stages 0 .. LG-1 of block 0.
-    fwd_stages<LG, LR, 0>(v, rb, 0, 0, cx->fwd, q, q2);
-    fwd_rest<LG, LR>(std::make_integer_sequence<int, NR - 1>{}, v, smg, k, 0, 0, cx->fwd, q, q2);
-    if (a.flags & kPostNorm) {
-#pragma unroll
-        for (int i = 0; i < R; ++i) v[i] = csub_lazy(csub_lazy(v[i], q2), q);
-    }
-    store_global<LG, LR, LO_LAST>(v, dst, t, gi, round_base<LR>(k, LO_LAST), vec_ok);
+    const uint32_t lgtg = __ffs(a.tg) - 1;
+    const uint32_t lg_tiles = a.logn - LG - lgtg;
+    const uint64_t tile = blockIdx.x;
+    const uint64_t limb = tile >> lg_tiles;
+    const uint32_t mi = limb % a.nctx;
+    chain_tile<LG, LR, false>(a.src, a.dst, c.operand, a.ctx[mi], c.op, c.scalar[mi], a.logn, lgtg, limb,
+                              tile & ((1ull << lg_tiles) - 1), a.flags, sm);
 }
 
 }  // namespace axhel_impl

@@ -169,7 +169,7 @@ void plan_override(bool inverse, uint32_t logn, const NttPlan* p)
 int plan_load(const char* path)
 {
     std::lock_guard<std::mutex> lk(g_mu);
-    g_table_tried = true;
+    ensure_table_locked();  // the shipped table first; `path` entries override it
     if (!path) {
         const std::string def = lib_dir() + "/ntt_plans.txt";
         return load_table_locked(def.c_str());

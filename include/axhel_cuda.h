@@ -132,6 +132,59 @@ axhel_status_t axhel_cuda_ntt_chain_fma_batch(const axhel_ntt_t* ntts, uint64_t 
                                               void* stream);
 
 /* ---------------------------------------------------------------------- */
+/* Uneven batches in one persistent launch (new)                          */
+/* ---------------------------------------------------------------------- */
+
+#define AXHEL_JOB_FORWARD 1u   /* ComputeForward(in_f, out_f) on every limb */
+#define AXHEL_JOB_INVERSE 2u   /* ComputeInverse; in_f == 4 fuses ReduceMod(4,2) on load */
+#define AXHEL_JOB_CHAIN_MUL 3u /* ComputeInverse(in_f,2) -> MulMod(., vector, 2) -> ComputeForward(1,out_f) */
+#define AXHEL_JOB_CHAIN_FMA 4u /* ComputeInverse(in_f,2) -> FMAMod(., scalars[m], vector|NULL, 2) -> ComputeForward */
+
+/* One job of a batch: `count` limbs of one degree N (2^10 <= N <= 2^17)
+ * stored back to back, limb i using ntts[i % n_ntts]; result/operand/vector
+ * are DEVICE pointers (result may equal operand), scalars a HOST array of
+ * n_ntts values (chain FMA only). */
+typedef struct axhel_job {
+    uint32_t kind;
+    uint32_t n_ntts;
+    const axhel_ntt_t* ntts;
+    uint64_t count;
+    uint64_t* result;
+    const uint64_t* operand;
+    const uint64_t* vector;
+    const uint64_t* scalars;
+    uint64_t input_mod_factor;
+    uint64_t output_mod_factor;
+} axhel_job_t;
+
+typedef struct axhel_batch* axhel_batch_t;
+
+/* Builds the device descriptors of a batch of jobs of mixed degree, limb
+ * count and kind (owned by the batch; the NTT handles are retained).  Each
+ * job's result equals the per-limb reference call sequence bit for bit. */
+axhel_status_t axhel_cuda_batch_create(const axhel_job_t* jobs, uint64_t n_jobs, axhel_batch_t* out);
+/* Runs the whole batch as ONE persistent kernel launch on `stream` (after
+ * clearing its counters); may be captured into a CUDA graph. */
+axhel_status_t axhel_cuda_batch_launch(axhel_batch_t batch, void* stream);
+/* Same, through a CUDA graph instantiated on first use and replayed after. */
+axhel_status_t axhel_cuda_batch_graph_launch(axhel_batch_t batch, void* stream);
+/* Waits for `stream` and returns AXHEL_ERR_TIMEOUT if a dependency wait
+ * inside the kernel gave up (bounded at 2 s), else AXHEL_OK. */
+axhel_status_t axhel_cuda_batch_status(axhel_batch_t batch, void* stream);
+axhel_status_t axhel_cuda_batch_destroy(axhel_batch_t batch);
+/* create + launch + status + destroy (synchronous). */
+axhel_status_t axhel_cuda_batch_run(const axhel_job_t* jobs, uint64_t n_jobs, void* stream);
+/* Message of the last batch failure on the calling thread. */
+const char* axhel_cuda_batch_last_error(void);
+/* Bound of every dependency wait inside the batch kernel (1 ms .. 10 s;
+ * default 2 s). */
+axhel_status_t axhel_cuda_batch_set_wait_ns(axhel_batch_t batch, uint64_t ns);
+/* Failure-detection hook: makes every dependency of job `job` unreachable
+ * (its waits run out), so the launch ends with AXHEL_ERR_TIMEOUT while the
+ * device stays usable.  For tests. */
+axhel_status_t axhel_cuda_batch_debug_unreachable(axhel_batch_t batch, uint64_t job);
+
+/* ---------------------------------------------------------------------- */
 /* Element-wise (device pointers); result may alias any operand.           */
 /* ---------------------------------------------------------------------- */
 
