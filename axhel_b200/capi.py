@@ -102,6 +102,7 @@ def _declare(L):
     d("axhel_cuda_batch_run", st_t, C.POINTER(Job), u64, vp)
     d("axhel_cuda_batch_last_error", C.c_char_p)
     d("axhel_cuda_batch_set_wait_ns", st_t, vp, u64)
+    d("axhel_cuda_batch_run_static", st_t, C.POINTER(Job), u64, vp)
     d("axhel_cuda_batch_debug_unreachable", st_t, vp, u64)
 
 
@@ -204,6 +205,13 @@ class Batch:
 def batch_run(specs, stream=0):
     jobs, keep = make_jobs(specs)
     _bcheck(lib().axhel_cuda_batch_run(jobs, len(specs), stream), "batch_run")
+
+
+def batch_run_static(specs, stream=0):
+    """axhel_cuda_batch_run_static: the batch with its scratch in the library's
+    static device array (no device allocation)."""
+    jobs, keep = make_jobs(specs)
+    _bcheck(lib().axhel_cuda_batch_run_static(jobs, len(specs), stream), "batch_run_static")
 
 
 def _arr64(values):

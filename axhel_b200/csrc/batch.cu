@@ -38,48 +38,10 @@
 #include "../../include/axhel_cuda.h"
 #include "internal.h"
 #include "launch.h"
+#include "batch.h"
 #include "ntt_kernels.cuh"
 
 namespace axhel_impl {
-
-constexpr int kBatchThreads = 128;
-constexpr int kBatchLR = 3;
-constexpr int kBatchTileWords = kBatchThreads << kBatchLR;  // 1024 residues
-constexpr int kBatchMinLG = 5, kBatchMaxLG = 9;
-
-enum BatchKind : uint32_t { kJobForward = 1, kJobInverse = 2, kJobChainMul = 3, kJobChainFma = 4 };
-
-struct BatchJob {
-    const uint64_t* src;
-    uint64_t* dst;
-    const uint64_t* vec;              // chain multiplicand / addend (may be null for FMA)
-    const ModCtx* const* ctx;         // nmods device pointers
-    const uint64_t* scalars;          // chain FMA scalars (nmods), device
-    uint64_t count;                   // limbs
-    uint64_t done_off;                // first completion counter of this job (count per phase)
-    uint32_t kind, logn, nmods, nphase;
-    uint32_t lg_col, lg_row;          // pass widths A (strided) and B (contiguous)
-    uint32_t tiles_per_limb[3];
-    uint32_t pre, norm;               // fuse ReduceMod(4,2) on load / normalize the output
-    uint32_t wait_extra;              // added to every dependency target (0; a test sets 1 to force a timeout)
-    uint32_t pad;
-};
-
-struct BatchEntry {
-    uint64_t tile_begin;  // first global tile of (job, phase)
-    uint32_t job, phase;
-};
-
-struct BatchArgs {
-    const BatchJob* jobs;
-    const BatchEntry* entries;
-    uint32_t nentries;
-    uint64_t total_tiles;
-    unsigned int* done;                 // per (job, phase, limb) completed tiles
-    unsigned long long* next_tile;      // work counter
-    int* error;                         // AXHEL_OK or AXHEL_ERR_TIMEOUT
-    uint64_t wait_ns;                   // a dependency wait gives up after this long
-};
 
 __device__ __forceinline__ uint64_t global_ns()
 {
@@ -235,6 +197,12 @@ axhel_status_t bfail(axhel_status_t st, const std::string& m)
     t_batch_error = m;
     return st;
 }
+
+}  // namespace
+
+void axhel_impl::batch_set_error(const std::string& msg) { t_batch_error = msg; }
+
+namespace {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 

@@ -1,0 +1,69 @@
+// Descriptors of the uneven-batch engine (batch.cu), shared with the
+// static-scratch entry point (batch_static.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/axhel_cuda.h"
+#include "internal.h"
+
+namespace axhel_impl {
+
+constexpr int kBatchThreads = 128;
+constexpr int kBatchLR = 3;
+constexpr int kBatchTileWords = kBatchThreads << kBatchLR;  // 1024 residues
+constexpr int kBatchMinLG = 5, kBatchMaxLG = 9;
+
+enum BatchKind : uint32_t { kJobForward = 1, kJobInverse = 2, kJobChainMul = 3, kJobChainFma = 4 };
+
+struct BatchJob {
+    const uint64_t* src;
+    uint64_t* dst;
+    const uint64_t* vec;              // chain multiplicand / addend (may be null for FMA)
+    const ModCtx* const* ctx;         // nmods device pointers
+    const uint64_t* scalars;          // chain FMA scalars (nmods), device
+    uint64_t count;                   // limbs
+    uint64_t done_off;                // first completion counter of this job (count per phase)
+    uint32_t kind, logn, nmods, nphase;
+    uint32_t lg_col, lg_row;          // pass widths A (strided) and B (contiguous)
+    uint32_t tiles_per_limb[3];
+    uint32_t pre, norm;               // fuse ReduceMod(4,2) on load / normalize the output
+    uint32_t wait_extra;              // added to every dependency target (0; a test sets 1 to force a timeout)
+    uint32_t pad;
+};
+
+struct BatchEntry {
+    uint64_t tile_begin;  // first global tile of (job, phase)
+    uint32_t job, phase;
+};
+
+struct BatchArgs {
+    const BatchJob* jobs;
+    const BatchEntry* entries;
+    uint32_t nentries;
+    uint64_t total_tiles;
+    unsigned int* done;                 // per (job, phase, limb) completed tiles
+    unsigned long long* next_tile;      // work counter
+    int* error;                         // AXHEL_OK or AXHEL_ERR_TIMEOUT
+    uint64_t wait_ns;                   // a dependency wait gives up after this long
+};
+
+// Lays out the device image of a batch for the device address `base`:
+// fills `host` (to be copied to `base`), the range of counters that must be
+// zero before a launch, and the kernel arguments.  NTT handles referenced by
+// the jobs are appended to `held` when it is not null.
+axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned char* base,
+                           std::vector<unsigned char>& host, size_t* zero_off, size_t* zero_bytes, BatchArgs* args,
+                           std::vector<axhel_ntt_t>* held, std::string* err);
+
+// Launches the persistent batch kernel for prepared arguments.
+cudaError_t batch_launch_args(const BatchArgs& a, cudaStream_t s);
+
+// Records the message returned by axhel_cuda_batch_last_error on this thread.
+void batch_set_error(const std::string& msg);
+
+}  // namespace axhel_impl

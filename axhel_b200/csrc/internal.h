@@ -80,9 +80,6 @@ bool plan_valid(const NttPlan& p, uint32_t logn, bool inverse);
 int plan_load(const char* path);
 void plan_override(bool inverse, uint32_t logn, const NttPlan* p);  // nullptr clears
 
-// Kernel launchers of the uneven-batch engine (batch.cu).
-struct BatchArgs;
-
 // Bytes reserved for the ModCtx header in front of the twiddle tables.
 constexpr size_t kCtxHeaderBytes = 256;
 

@@ -179,6 +179,17 @@ const char* axhel_cuda_batch_last_error(void);
 /* Bound of every dependency wait inside the batch kernel (1 ms .. 10 s;
  * default 2 s). */
 axhel_status_t axhel_cuda_batch_set_wait_ns(axhel_batch_t batch, uint64_t ns);
+/* No counterpart in the reference.  axhel_cuda_batch_run without any device
+ * allocation, for callers that cannot call cudaMalloc while they run (a
+ * process whose HBM is reserved up front by its own allocator or a fixed
+ * budget; a latency-critical loop where cudaMalloc/cudaFree would
+ * synchronize the device).  The batch's descriptors and counters live in a
+ * static 1 MiB device array per device; a batch that needs more returns
+ * AXHEL_ERR_UNSUPPORTED.  The first call on a device resolves that array's
+ * address (make it before any stream capture).  All calls share the array:
+ * calls that overlap on the GPU race and must not be issued.  Synchronous;
+ * results equal axhel_cuda_batch_run's bit for bit. */
+axhel_status_t axhel_cuda_batch_run_static(const axhel_job_t* jobs, uint64_t n_jobs, void* stream);
 /* Failure-detection hook: makes every dependency of job `job` unreachable
  * (its waits run out), so the launch ends with AXHEL_ERR_TIMEOUT while the
  * device stays usable.  For tests. */
