@@ -35,6 +35,30 @@ class Job(C.Structure):
                 ("output_mod_factor", C.c_uint64)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_inflight", C.c_uint32), ("max_batch_requests", C.c_uint32)]
+
+
+class Request(C.Structure):
+    """axhel_request_t"""
+
+    _fields_ = [("kind", C.c_uint32), ("n_ntts", C.c_uint32), ("ntts", C.POINTER(C.c_void_p)),
+                ("count", C.c_uint64), ("input", C.c_void_p), ("output", C.c_void_p), ("vector", C.c_void_p),
+                ("scalars", C.POINTER(C.c_uint64)), ("input_mod_factor", C.c_uint64),
+                ("output_mod_factor", C.c_uint64)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("batch_size", C.c_uint32), ("batch_id", C.c_uint64),
+                ("queue_ms", C.c_double), ("latency_ms", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_uint64), ("batches", C.c_uint64), ("max_batch_requests", C.c_uint64),
+                ("pending", C.c_uint64), ("in_use_bytes", C.c_uint64), ("peak_in_use_bytes", C.c_uint64),
+                ("samples", C.c_uint64), ("p50_ms", C.c_double), ("p99_ms", C.c_double)]
+
+
 class AxhelError(RuntimeError):
     def __init__(self, status, where, msg):
         super().__init__(f"{where}: {STATUS.get(status, status)}: {msg}")
@@ -103,6 +127,14 @@ def _declare(L):
     d("axhel_cuda_batch_last_error", C.c_char_p)
     d("axhel_cuda_batch_set_wait_ns", st_t, vp, u64)
     d("axhel_cuda_batch_run_static", st_t, C.POINTER(Job), u64, vp)
+    d("axhel_server_create", st_t, C.POINTER(ServerConfig), C.POINTER(vp))
+    d("axhel_server_submit", st_t, vp, C.POINTER(Request), C.POINTER(u64))
+    d("axhel_server_wait", st_t, vp, u64, u64, C.POINTER(RequestInfo))
+    d("axhel_server_cancel", st_t, vp, u64)
+    d("axhel_server_pause", st_t, vp, C.c_int)
+    d("axhel_server_stats", st_t, vp, C.POINTER(ServerStats), C.c_int)
+    d("axhel_server_destroy", st_t, vp)
+    d("axhel_server_last_error", C.c_char_p)
     d("axhel_cuda_batch_debug_unreachable", st_t, vp, u64)
 
 
@@ -212,6 +244,65 @@ def batch_run_static(specs, stream=0):
     static device array (no device allocation)."""
     jobs, keep = make_jobs(specs)
     _bcheck(lib().axhel_cuda_batch_run_static(jobs, len(specs), stream), "batch_run_static")
+
+
+def _scheck(status, where):
+    if status != OK:
+        raise AxhelError(status, where, lib().axhel_server_last_error().decode())
+
+
+class Server:
+    """The continuous-batching serving loop (axhel_server_*)."""
+
+    def __init__(self, budget_bytes, max_inflight=2, max_batch_requests=256):
+        cfg = ServerConfig(budget_bytes, max_inflight, max_batch_requests)
+        self.h = vp()
+        _scheck(lib().axhel_server_create(C.byref(cfg), C.byref(self.h)), "server_create")
+        self._keep = {}
+
+    def submit(self, kind, ntts, count, input, output, vector=0, scalars=None, in_f=1, out_f=1):
+        hs = (C.c_void_p * len(ntts))(*[t.h.value for t in ntts])
+        r = Request(kind, len(ntts), C.cast(hs, C.POINTER(C.c_void_p)), count, input, output, vector or None,
+                    None, in_f, out_f)
+        keep = [hs]
+        if scalars is not None:
+            sc = (C.c_uint64 * len(scalars))(*[int(v) for v in scalars])
+            r.scalars = C.cast(sc, C.POINTER(C.c_uint64))
+            keep.append(sc)
+        rid = u64()
+        _scheck(lib().axhel_server_submit(self.h, C.byref(r), C.byref(rid)), "server_submit")
+        self._keep[rid.value] = keep
+        return rid.value
+
+    def wait(self, rid, timeout_s=60.0):
+        """Returns (status, RequestInfo); status AXHEL_ERR_TIMEOUT (6) leaves the request queued."""
+        info = RequestInfo()
+        st = int(lib().axhel_server_wait(self.h, rid, int(timeout_s * 1e6), C.byref(info)))
+        if st != 6:
+            self._keep.pop(rid, None)
+        return st, info
+
+    def cancel(self, rid):
+        return int(lib().axhel_server_cancel(self.h, rid))
+
+    def pause(self, paused=True):
+        _scheck(lib().axhel_server_pause(self.h, 1 if paused else 0), "server_pause")
+
+    def stats(self, reset=False):
+        s = ServerStats()
+        _scheck(lib().axhel_server_stats(self.h, C.byref(s), 1 if reset else 0), "server_stats")
+        return {k: getattr(s, k) for k, _ in ServerStats._fields_}
+
+    def close(self):
+        if self.h:
+            lib().axhel_server_destroy(self.h)
+            self.h = vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _arr64(values):

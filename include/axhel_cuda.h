@@ -196,6 +196,65 @@ axhel_status_t axhel_cuda_batch_run_static(const axhel_job_t* jobs, uint64_t n_j
 axhel_status_t axhel_cuda_batch_debug_unreachable(axhel_batch_t batch, uint64_t job);
 
 /* ---------------------------------------------------------------------- */
+/* Serving loop: continuous batching on one GPU (new)                      */
+/* ---------------------------------------------------------------------- */
+
+typedef struct axhel_server* axhel_server_t;
+
+typedef struct axhel_server_config {
+    uint64_t hbm_budget_bytes;   /* device bytes the server may hold for staged operands */
+    uint32_t max_inflight;       /* batches concurrently on the GPU (1..16 streams) */
+    uint32_t max_batch_requests; /* requests admitted into one batch launch */
+} axhel_server_config_t;
+
+/* One request: a job of the batch engine (AXHEL_JOB_*).  input / output /
+ * vector may be HOST memory (staged by the server; pinned memory keeps the
+ * copies asynchronous) or DEVICE memory (used in place).  Buffers must stay
+ * valid until axhel_server_wait returns for the request. */
+typedef struct axhel_request {
+    uint32_t kind;
+    uint32_t n_ntts;
+    const axhel_ntt_t* ntts;
+    uint64_t count;
+    const uint64_t* input;
+    uint64_t* output;
+    const uint64_t* vector;
+    const uint64_t* scalars;
+    uint64_t input_mod_factor;
+    uint64_t output_mod_factor;
+} axhel_request_t;
+
+typedef struct axhel_request_info {
+    int32_t status;       /* AXHEL_OK, AXHEL_ERR_CANCELLED, AXHEL_ERR_TIMEOUT, ... */
+    uint32_t batch_size;  /* requests in the launch that ran it */
+    uint64_t batch_id;
+    double queue_ms;      /* submit -> admitted */
+    double latency_ms;    /* submit -> result available */
+} axhel_request_info_t;
+
+typedef struct axhel_server_stats {
+    uint64_t completed, batches, max_batch_requests, pending, in_use_bytes, peak_in_use_bytes, samples;
+    double p50_ms, p99_ms; /* submit -> done latency over completed requests */
+} axhel_server_stats_t;
+
+/* Starts the scheduler and completion threads on the current device. */
+axhel_status_t axhel_server_create(const axhel_server_config_t* config, axhel_server_t* out);
+/* Queues a request; returns at once with its id.  AXHEL_ERR_REJECTED if the
+ * request alone needs more device memory than the budget. */
+axhel_status_t axhel_server_submit(axhel_server_t server, const axhel_request_t* request, uint64_t* id);
+/* Waits (at most timeout_us) for a request; on completion returns its status
+ * and forgets it.  AXHEL_ERR_TIMEOUT if still pending or running. */
+axhel_status_t axhel_server_wait(axhel_server_t server, uint64_t id, uint64_t timeout_us, axhel_request_info_t* info);
+/* Cancels a request that has not been admitted yet (AXHEL_ERR_BUSY otherwise). */
+axhel_status_t axhel_server_cancel(axhel_server_t server, uint64_t id);
+/* Holds (1) or resumes (0) admission; running batches are unaffected. */
+axhel_status_t axhel_server_pause(axhel_server_t server, int paused);
+axhel_status_t axhel_server_stats(axhel_server_t server, axhel_server_stats_t* out, int reset_latencies);
+/* Stops admission, drains the batches in flight, frees everything. */
+axhel_status_t axhel_server_destroy(axhel_server_t server);
+const char* axhel_server_last_error(void);
+
+/* ---------------------------------------------------------------------- */
 /* Element-wise (device pointers); result may alias any operand.           */
 /* ---------------------------------------------------------------------- */
 

@@ -1,0 +1,137 @@
+"""GPU: the serving loop.  Requests of mixed degree and limb count, from host
+(pinned) and device memory, give the same bits alone and in a concurrent mix
+(and match the reference call sequence on the oracle); admission respects the
+HBM budget; host-side failure cases (rejection, cancellation, a held queue
+and a bounded wait) leave the server healthy."""
+import numpy as np
+import pytest
+
+from helpers import SEED, dev, dev_empty, host, ptr
+
+pytestmark = pytest.mark.gpu
+
+
+def pinned(arr):
+    import torch
+
+    t = torch.empty(max(arr.size, 1), dtype=torch.int64).pin_memory()
+    t.numpy().view(np.uint64)[: arr.size] = arr
+    return t
+
+
+def make_requests(cuda, oracle, seed, specs):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for j, (logn, L, count, kind) in enumerate(specs):
+        n = 1 << logn
+        mods = []
+        for i in range(L):
+            q = oracle.find_ntt_prime_near(n, int(rng.integers(40, 60)), int(rng.integers(1, 4)), 4)
+            mods.append((q, oracle.find_primitive_root(n, q)))
+        st = oracle.rng(SEED ^ (seed * 1000 + j))
+        x = np.concatenate([oracle.random_vector(st, n, 2 * mods[i % L][0]) for i in range(count)])
+        v = np.concatenate([oracle.random_vector(st, n, 2 * mods[i % L][0]) for i in range(count)])
+        sc = [oracle.bounded(st, 2 * q) for q, _ in mods]
+        reqs.append(dict(n=n, L=L, count=count, kind=kind, mods=mods, x=x, v=v, sc=sc,
+                         ntts=[cuda.NTT(n, q, psi) for q, psi in mods]))
+    return reqs
+
+
+def expected(oracle, r):
+    n, out = r["n"], []
+    for i in range(r["count"]):
+        q, psi = r["mods"][i % r["L"]]
+        fwd, inv, ninv = oracle.tables(n, q, psi)
+        s = slice(i * n, (i + 1) * n)
+        y = oracle.inverse(r["x"][s], q, inv, ninv, 2, 2)
+        y = oracle.mul(y, r["v"][s], q, 2) if r["kind"] == 3 else oracle.fma(y, r["sc"][i % r["L"]], r["v"][s], q, 2)
+        out.append(oracle.forward(y, q, fwd, 1, 4))
+    return np.concatenate(out)
+
+
+def submit(srv, r, on_device):
+    if on_device:
+        bi, bo, bv = dev(r["x"]), dev_empty(r["x"].size), dev(r["v"])
+        pi, po, pv = ptr(bi), ptr(bo), ptr(bv)
+    else:
+        bi, bo, bv = pinned(r["x"]), pinned(np.zeros(r["x"].size, np.uint64)), pinned(r["v"])
+        pi, po, pv = bi.data_ptr(), bo.data_ptr(), bv.data_ptr()
+    rid = srv.submit(r["kind"], r["ntts"], r["count"], pi, po, vector=pv,
+                     scalars=r["sc"] if r["kind"] == 4 else None, in_f=2, out_f=4)
+    return rid, (bi, bo, bv)
+
+
+def result(bufs, size, on_device):
+    if on_device:
+        return host(bufs[1], size)
+    return bufs[1].numpy().view(np.uint64)[:size].copy()
+
+
+SPECS = [(13, 4, 4, 3), (14, 2, 2, 4), (15, 6, 6, 3), (16, 3, 3, 4), (17, 2, 2, 3), (13, 8, 8, 4), (16, 5, 5, 3),
+         (12, 3, 3, 4)]
+
+
+def test_same_bits_alone_and_in_a_mix(cuda, oracle):
+    reqs = make_requests(cuda, oracle, 5, SPECS)
+    srv = cuda.Server(budget_bytes=8 << 30, max_inflight=2, max_batch_requests=64)
+    alone = []
+    for k, r in enumerate(reqs):  # one at a time on an idle server
+        rid, bufs = submit(srv, r, on_device=k % 2 == 0)
+        st, info = srv.wait(rid)
+        assert st == 0 and info.batch_size == 1
+        alone.append(result(bufs, r["x"].size, k % 2 == 0))
+        np.testing.assert_array_equal(alone[-1], expected(oracle, r), err_msg=f"request {k}")
+    # everything at once, twice over: batches mix requests and overlap
+    handles = []
+    for rep in range(2):
+        for k, r in enumerate(reqs):
+            rid, bufs = submit(srv, r, on_device=(k + rep) % 2 == 0)
+            handles.append((k, rid, bufs, (k + rep) % 2 == 0))
+    sizes = []
+    for k, rid, bufs, on_dev in handles:
+        st, info = srv.wait(rid)
+        assert st == 0
+        sizes.append(info.batch_size)
+        np.testing.assert_array_equal(result(bufs, reqs[k]["x"].size, on_dev), alone[k], err_msg=f"mix {k}")
+    assert max(sizes) > 1, "concurrent requests were batched together"
+    stats = srv.stats()
+    assert stats["completed"] == 3 * len(reqs) and stats["p99_ms"] >= stats["p50_ms"] > 0
+    srv.close()
+
+
+def test_admission_respects_the_budget(cuda, oracle):
+    reqs = make_requests(cuda, oracle, 6, [(16, 4, 4, 3)] * 6)
+    one = 3 * reqs[0]["x"].nbytes  # input, output and vector staged per request
+    srv = cuda.Server(budget_bytes=2 * one, max_inflight=4, max_batch_requests=16)
+    hs = [submit(srv, r, on_device=False) for r in reqs]
+    for (rid, bufs), r in zip(hs, reqs):
+        st, _ = srv.wait(rid)
+        assert st == 0
+        np.testing.assert_array_equal(result(bufs, r["x"].size, False), expected(oracle, r))
+    assert srv.stats()["peak_in_use_bytes"] <= 2 * one
+    srv.close()
+
+
+def test_rejection_cancel_and_bounded_wait(cuda, oracle):
+    reqs = make_requests(cuda, oracle, 7, [(13, 2, 2, 3), (13, 2, 2, 4), (13, 2, 2, 3)])
+    one = 3 * reqs[0]["x"].nbytes
+    srv = cuda.Server(budget_bytes=one, max_inflight=1, max_batch_requests=4)
+    big = make_requests(cuda, oracle, 8, [(14, 2, 4, 3)])[0]
+    with pytest.raises(cuda.AxhelError) as e:  # alone over the budget
+        submit(srv, big, on_device=False)
+    assert e.value.status == 7
+    srv.pause(True)  # a held queue: nothing is admitted
+    a, abufs = submit(srv, reqs[0], on_device=False)
+    b, bbufs = submit(srv, reqs[1], on_device=False)
+    c, cbufs = submit(srv, reqs[2], on_device=False)
+    st, _ = srv.wait(a, timeout_s=0.02)
+    assert st == 6  # bounded wait: still queued
+    assert srv.cancel(b) == 0
+    srv.pause(False)
+    st, info = srv.wait(b)
+    assert st == 8  # cancelled, never ran
+    for rid, bufs, r in ((a, abufs, reqs[0]), (c, cbufs, reqs[2])):
+        st, _ = srv.wait(rid)
+        assert st == 0
+        np.testing.assert_array_equal(result(bufs, r["x"].size, False), expected(oracle, r))
+    srv.close()
