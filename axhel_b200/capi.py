@@ -35,8 +35,13 @@ class Job(C.Structure):
                 ("output_mod_factor", C.c_uint64)]
 
 
+SERVER_PERSISTENT = 1
+
+
 class ServerConfig(C.Structure):
-    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_inflight", C.c_uint32), ("max_batch_requests", C.c_uint32)]
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_batch_words", C.c_uint64),
+                ("small_request_words", C.c_uint64), ("max_inflight", C.c_uint32),
+                ("max_batch_requests", C.c_uint32), ("flags", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class Request(C.Structure):
@@ -57,6 +62,13 @@ class ServerStats(C.Structure):
     _fields_ = [("completed", C.c_uint64), ("batches", C.c_uint64), ("max_batch_requests", C.c_uint64),
                 ("pending", C.c_uint64), ("in_use_bytes", C.c_uint64), ("peak_in_use_bytes", C.c_uint64),
                 ("samples", C.c_uint64), ("p50_ms", C.c_double), ("p99_ms", C.c_double)]
+
+
+class DriveResult(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("skipped", C.c_uint64),
+                ("failed", C.c_uint64), ("wall_s", C.c_double), ("jobs_per_s", C.c_double),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("p50_slowdown", C.c_double),
+                ("p99_slowdown", C.c_double), ("isolated_p99_ms", C.c_double)]
 
 
 class AxhelError(RuntimeError):
@@ -135,6 +147,8 @@ def _declare(L):
     d("axhel_server_stats", st_t, vp, C.POINTER(ServerStats), C.c_int)
     d("axhel_server_destroy", st_t, vp)
     d("axhel_server_last_error", C.c_char_p)
+    d("axhel_server_drive", st_t, vp, C.POINTER(Request), C.c_uint32, C.POINTER(C.c_void_p), C.c_uint32,
+      C.POINTER(C.c_double), C.c_double, C.c_double, u64, C.POINTER(DriveResult))
     d("axhel_cuda_batch_debug_unreachable", st_t, vp, u64)
 
 
@@ -254,8 +268,10 @@ def _scheck(status, where):
 class Server:
     """The continuous-batching serving loop (axhel_server_*)."""
 
-    def __init__(self, budget_bytes, max_inflight=2, max_batch_requests=256):
-        cfg = ServerConfig(budget_bytes, max_inflight, max_batch_requests)
+    def __init__(self, budget_bytes, max_inflight=2, max_batch_requests=256, max_batch_words=0, persistent=False,
+                 small_request_words=0):
+        cfg = ServerConfig(budget_bytes, max_batch_words, small_request_words, max_inflight, max_batch_requests,
+                           SERVER_PERSISTENT if persistent else 0, 0)
         self.h = vp()
         _scheck(lib().axhel_server_create(C.byref(cfg), C.byref(self.h)), "server_create")
         self._keep = {}
@@ -292,6 +308,32 @@ class Server:
         s = ServerStats()
         _scheck(lib().axhel_server_stats(self.h, C.byref(s), 1 if reset else 0), "server_stats")
         return {k: getattr(s, k) for k, _ in ServerStats._fields_}
+
+    def drive(self, templates, outputs, isolated_ms, rate, seconds, seed=1):
+        """axhel_server_drive: Poisson load from a C++ thread.  templates: list
+        of dicts as submit() takes (output ignored); outputs: per template a
+        list of `copies` output addresses."""
+        n = len(templates)
+        copies = len(outputs[0])
+        arr = (Request * n)()
+        keep = []
+        for i, t in enumerate(templates):
+            hs = (C.c_void_p * len(t["ntts"]))(*[h.h.value for h in t["ntts"]])
+            keep.append(hs)
+            r = arr[i]
+            r.kind, r.n_ntts, r.ntts, r.count = t["kind"], len(t["ntts"]), C.cast(hs, C.POINTER(C.c_void_p)), t["count"]
+            r.input, r.output, r.vector = t["input"], outputs[i][0], t.get("vector") or None
+            if t.get("scalars") is not None:
+                sc = (C.c_uint64 * len(t["scalars"]))(*[int(v) for v in t["scalars"]])
+                keep.append(sc)
+                r.scalars = C.cast(sc, C.POINTER(C.c_uint64))
+            r.input_mod_factor, r.output_mod_factor = t.get("in_f", 1), t.get("out_f", 1)
+        outs = (C.c_void_p * (n * copies))(*[o for row in outputs for o in row])
+        iso = (C.c_double * n)(*isolated_ms) if isolated_ms is not None else None
+        res = DriveResult()
+        _scheck(lib().axhel_server_drive(self.h, arr, n, outs, copies, iso, rate, seconds, seed, C.byref(res)),
+                "server_drive")
+        return {k: getattr(res, k) for k, _ in DriveResult._fields_}
 
     def close(self):
         if self.h:

@@ -170,6 +170,35 @@ __global__ void __launch_bounds__(kBatchThreads) batch_kernel(const __grid_const
     }
 }
 
+// One phase of a batch as an ordinary launch: CTA b runs global tile
+// first + b.  Tiles of earlier phases were finished by earlier launches.
+__global__ void __launch_bounds__(kBatchThreads) batch_phase_kernel(const __grid_constant__ BatchArgs a,
+                                                                    uint64_t first)
+{
+    __shared__ uint64_t sm[kBatchTileWords + 128];
+    const uint64_t tile = first + blockIdx.x;
+    uint32_t lo = 0, hi = a.nentries;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (a.entries[mid].tile_begin <= tile) lo = mid; else hi = mid;
+    }
+    const BatchEntry e = a.entries[lo];
+    const BatchJob& j = a.jobs[e.job];
+    const uint64_t lt = tile - e.tile_begin;
+    const uint32_t tpl = j.tiles_per_limb[e.phase];
+    const uint64_t limb = lt / tpl;
+    const uint64_t til = lt - limb * tpl;
+    const PhaseCfg c = phase_cfg(j, e.phase);
+    switch (c.lg) {
+    case 5: run_tile_lg<5>(j, c, e.phase, limb, til, sm); break;
+    case 6: run_tile_lg<6>(j, c, e.phase, limb, til, sm); break;
+    case 7: run_tile_lg<7>(j, c, e.phase, limb, til, sm); break;
+    case 8: run_tile_lg<8>(j, c, e.phase, limb, til, sm); break;
+    case 9: run_tile_lg<9>(j, c, e.phase, limb, til, sm); break;
+    default: break;
+    }
+}
+
 }  // namespace axhel_impl
 
 using namespace axhel_impl;
@@ -227,7 +256,7 @@ namespace axhel_impl {
 // entry points.
 axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned char* base,
                            std::vector<unsigned char>& host, size_t* zero_off, size_t* zero_bytes, BatchArgs* args,
-                           std::vector<axhel_ntt_t>* held, std::string* err)
+                           std::vector<axhel_ntt_t>* held, std::string* err, uint64_t* phase_begin)
 {
     if (!jobs || n_jobs == 0) {
         *err = "empty batch";
@@ -309,12 +338,15 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
     // phase-major tile order
     std::vector<BatchEntry> ent;
     uint64_t tiles = 0;
-    for (uint32_t p = 0; p < 3; ++p)
+    for (uint32_t p = 0; p < 3; ++p) {
+        if (phase_begin) phase_begin[p] = tiles;
         for (uint64_t i = 0; i < n_jobs; ++i) {
             if (p >= bj[i].nphase || bj[i].count == 0) continue;
             ent.push_back(BatchEntry{tiles, (uint32_t)i, p});
             tiles += bj[i].count * bj[i].tiles_per_limb[p];
         }
+    }
+    if (phase_begin) phase_begin[3] = tiles;
     if (ent.empty()) {
         *err = "";
         args->total_tiles = 0;
@@ -362,6 +394,21 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
     args->error = reinterpret_cast<int*>(base + err_off);
     args->wait_ns = 2000000000ull;  // 2 s
     return AXHEL_OK;
+}
+
+cudaError_t batch_launch_phases(const BatchArgs& a, const uint64_t* phase_begin, cudaStream_t s)
+{
+    for (int p = 0; p < 3; ++p) {
+        const uint64_t n = phase_begin[p + 1] - phase_begin[p];
+        if (n == 0) continue;
+        if (n > 0x7fffffffull) return cudaErrorInvalidValue;
+        count_launch();
+        ProfScope prof(s, "batch_phase_kernel");
+        batch_phase_kernel<<<(unsigned)n, kBatchThreads, 0, s>>>(a, phase_begin[p]);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t batch_launch_args(const BatchArgs& a, cudaStream_t s)

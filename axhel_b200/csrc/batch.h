@@ -56,12 +56,20 @@ struct BatchArgs {
 // fills `host` (to be copied to `base`), the range of counters that must be
 // zero before a launch, and the kernel arguments.  NTT handles referenced by
 // the jobs are appended to `held` when it is not null.
+// `phase_begin`, when not null, receives the first global tile of phases
+// 0, 1, 2 and the total (4 entries; tiles are numbered phase-major).
 axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned char* base,
                            std::vector<unsigned char>& host, size_t* zero_off, size_t* zero_bytes, BatchArgs* args,
-                           std::vector<axhel_ntt_t>* held, std::string* err);
+                           std::vector<axhel_ntt_t>* held, std::string* err, uint64_t* phase_begin = nullptr);
 
 // Launches the persistent batch kernel for prepared arguments.
 cudaError_t batch_launch_args(const BatchArgs& a, cudaStream_t s);
+
+// Runs a prepared batch as one ordinary (non-persistent) launch per phase,
+// one CTA per tile and no waits inside a launch: the phases are ordered by
+// the stream.  Concurrent batches on other streams share the SMs tile by
+// tile.  `phase_begin` as filled by batch_build.
+cudaError_t batch_launch_phases(const BatchArgs& a, const uint64_t* phase_begin, cudaStream_t s);
 
 // Records the message returned by axhel_cuda_batch_last_error on this thread.
 void batch_set_error(const std::string& msg);

@@ -3,6 +3,10 @@
 // Requests (any job kind of the batch engine: forward, inverse, or the fused
 // INTT -> MulMod/FMAMod -> NTT chain, each of any degree 2^10..2^17 and limb
 // count) are submitted from any host thread and return at once with an id.
+// (Batches run as one launch per phase by default, so batches on different
+// streams share the SMs tile by tile; AXHEL_SERVER_PERSISTENT selects the
+// single persistent launch instead.  max_batch_words caps a batch's size so
+// that one large request does not hold small ones back.)
 // A scheduler thread admits pending requests in arrival order while their
 // device bytes fit the HBM budget, stages host operands into stream-ordered
 // pool allocations, and launches every admitted request as ONE persistent
@@ -19,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -69,17 +74,21 @@ struct Req {
 };
 
 struct Slot {
+    int lane = 0;  // 0: small requests (high-priority stream), 1: the rest
     cudaStream_t stream = nullptr;
     void* scratch = nullptr;
     size_t cap = 0;
-    int* err_host = nullptr;  // pinned word the kernel's error status is copied into
+    int* err_host = nullptr;        // pinned word the kernel's error status is copied into
+    unsigned char* host_img = nullptr;  // pinned staging of the batch descriptors
+    size_t host_cap = 0;
     bool busy = false;
 };
 
+// A batch on the GPU: its requests in the order their results land, each
+// with the event recorded after its result copy.
 struct Inflight {
-    cudaEvent_t done = nullptr;
     std::vector<Req*> reqs;
-    size_t bytes = 0;
+    std::vector<cudaEvent_t> done;
     int slot = 0;
     uint64_t id = 0;
 };
@@ -92,16 +101,31 @@ struct axhel_server {
     cudaMemPool_t pool = nullptr;
     std::mutex mu;
     std::condition_variable cv_sched, cv_done, cv_wait;
-    std::deque<Req*> pending;
+    std::deque<Req*> pending[2];  // per lane, arrival order
     std::unordered_map<uint64_t, std::unique_ptr<Req>> reqs;
     std::deque<Inflight> inflight;
     std::vector<Slot> slots;
     size_t in_use = 0, peak_in_use = 0;
     uint64_t next_id = 1, batches = 0, completed = 0, max_batch = 0;
+    int lanes = 1;
     bool stop = false, paused = false;
     std::vector<double> lat_ms;  // submit -> done of every completed request
     std::thread sched, comp;
     std::string fatal;
+    std::vector<cudaEvent_t> event_pool;  // reused completion events
+
+    cudaEvent_t get_event()
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!event_pool.empty()) {
+            cudaEvent_t e = event_pool.back();
+            event_pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+        return e;
+    }
 
     void scheduler();
     void completer();
@@ -151,6 +175,7 @@ axhel_status_t axhel_server::launch(Slot& s, int slot_index, std::vector<Req*>& 
     size_t zo = 0, zb = 0;
     axhel_impl::BatchArgs args{};
     std::string err;
+    uint64_t phases[4] = {0, 0, 0, 0};
     axhel_status_t rc = axhel_impl::batch_build(jobs.data(), jobs.size(), nullptr, img, &zo, &zb, &args, nullptr, &err);
     if (rc) return sfail(rc, err);
     if (img.size() > s.cap) {
@@ -163,21 +188,40 @@ axhel_status_t axhel_server::launch(Slot& s, int slot_index, std::vector<Req*>& 
         s.cap = cap;
     }
     rc = axhel_impl::batch_build(jobs.data(), jobs.size(), static_cast<unsigned char*>(s.scratch), img, &zo, &zb,
-                                 &args, nullptr, &err);
+                                 &args, nullptr, &err, phases);
     if (rc) return sfail(rc, err);
-    cudaError_t e = cudaMemcpyAsync(s.scratch, img.data(), img.size(), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = axhel_impl::batch_launch_args(args, st);
+    if (img.size() > s.host_cap) {
+        if (s.host_img) cudaFreeHost(s.host_img);
+        s.host_img = nullptr;
+        s.host_cap = 0;
+        const size_t cap = std::max<size_t>(img.size() * 2, 1 << 20);
+        if (cudaMallocHost(reinterpret_cast<void**>(&s.host_img), cap) != cudaSuccess)
+            return sfail(AXHEL_ERR_NOMEM, "pinned descriptor staging");
+        s.host_cap = cap;
+    }
+    // the slot's previous batch has completed, so its staging copy is done
+    std::memcpy(s.host_img, img.data(), img.size());
+    cudaError_t e = cudaMemcpyAsync(s.scratch, s.host_img, img.size(), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = (cfg.flags & AXHEL_SERVER_PERSISTENT) ? axhel_impl::batch_launch_args(args, st)
+                                                   : axhel_impl::batch_launch_phases(args, phases, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(s.err_host, args.error, sizeof(int), cudaMemcpyDeviceToHost, st);
-    for (Req* q : take) {
+    // results back smallest first; each request completes at its own event
+    std::vector<Req*> order(take);
+    std::stable_sort(order.begin(), order.end(), [](const Req* a, const Req* b) { return a->words < b->words; });
+    for (Req* q : order) {
         if (e != cudaSuccess) break;
         if (!q->out_dev) e = cudaMemcpyAsync(q->r.output, q->d_out, q->words * 8, cudaMemcpyDeviceToHost, st);
+        cudaEvent_t ev = get_event();
+        if (!ev) e = cudaErrorMemoryAllocation;
+        if (e == cudaSuccess) e = cudaEventRecord(ev, st);
+        if (ev) f.done.push_back(ev);
         if (!q->in_dev) cudaFreeAsync(q->d_in, st);
         if (!q->out_dev && q->d_out != q->d_in) cudaFreeAsync(q->d_out, st);
         if (q->r.vector && !q->vec_dev) cudaFreeAsync(q->d_vec, st);
     }
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventRecord(f.done, st);
     if (e != cudaSuccess) return sfail(AXHEL_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
+    f.reqs = order;
     f.slot = slot_index;
     return AXHEL_OK;
 }
@@ -186,25 +230,33 @@ void axhel_server::scheduler()
 {
     cudaSetDevice(device);
     std::unique_lock<std::mutex> lk(mu);
+    auto free_slot = [&](int lane) {
+        for (size_t i = 0; i < slots.size(); ++i)
+            if (slots[i].lane == lane && !slots[i].busy) return (int)i;
+        return -1;
+    };
+    auto runnable = [&](int lane) { return !pending[lane].empty() && free_slot(lane) >= 0; };
     for (;;) {
-        cv_sched.wait(lk, [&] {
-            if (stop) return true;
-            if (paused || pending.empty()) return false;
-            return std::any_of(slots.begin(), slots.end(), [](const Slot& s) { return !s.busy; });
-        });
+        cv_sched.wait(lk, [&] { return stop || (!paused && (runnable(0) || runnable(1))); });
         if (stop) break;
+        // the small-request lane first, then the other
+        const int lane = runnable(0) ? 0 : 1;
+        std::deque<Req*>& queue = pending[lane];
         // admit in arrival order while the budget allows
         std::vector<Req*> take;
         size_t bytes = 0;
-        while (!pending.empty() && take.size() < cfg.max_batch_requests) {
-            Req* q = pending.front();
+        uint64_t words = 0;
+        while (!queue.empty() && take.size() < cfg.max_batch_requests) {
+            Req* q = queue.front();
             if (q->status != kPending) {  // cancelled
-                pending.pop_front();
+                queue.pop_front();
                 continue;
             }
             if (in_use + bytes + q->need > cfg.hbm_budget_bytes) break;
+            if (cfg.max_batch_words && !take.empty() && words + q->words > cfg.max_batch_words) break;
             bytes += q->need;
-            pending.pop_front();
+            words += q->words;
+            queue.pop_front();
             take.push_back(q);
         }
         if (take.empty()) {
@@ -213,12 +265,11 @@ void axhel_server::scheduler()
             // budget: larger ones are refused at submit), or it is cancelled.
             const size_t held = in_use;
             cv_sched.wait(lk, [&] {
-                return stop || paused || in_use < held || pending.empty() || pending.front()->status != kPending;
+                return stop || paused || in_use < held || queue.empty() || queue.front()->status != kPending;
             });
             continue;
         }
-        int si = 0;
-        while (slots[si].busy) ++si;
+        const int si = free_slot(lane);
         slots[si].busy = true;
         in_use += bytes;
         peak_in_use = std::max(peak_in_use, in_use);
@@ -233,8 +284,6 @@ void axhel_server::scheduler()
         max_batch = std::max<uint64_t>(max_batch, take.size());
         lk.unlock();
         Inflight f;
-        f.reqs = take;
-        f.bytes = bytes;
         f.id = bid;
         const axhel_status_t rc = launch(slots[si], si, take, f);
         lk.lock();
@@ -243,8 +292,8 @@ void axhel_server::scheduler()
                 q->status = rc;
                 q->t_done = Clock::now();
             }
-            if (f.done) cudaEventDestroy(f.done);
             cudaStreamSynchronize(slots[si].stream);
+            for (cudaEvent_t ev : f.done) event_pool.push_back(ev);
             slots[si].busy = false;
             in_use -= bytes;
             cv_wait.notify_all();
@@ -265,28 +314,44 @@ void axhel_server::completer()
             if (stop) break;
             continue;
         }
-        cudaEvent_t ev = inflight.front().done;
-        lk.unlock();
-        const cudaError_t e = cudaEventSynchronize(ev);
-        lk.lock();
-        Inflight f = std::move(inflight.front());
-        inflight.pop_front();
-        Slot& s = slots[f.slot];
-        const int kernel_status = (e == cudaSuccess) ? *s.err_host : AXHEL_ERR_CUDA;
-        const auto now = Clock::now();
-        for (Req* q : f.reqs) {
-            q->status = kernel_status;
-            q->t_done = now;
-            lat_ms.push_back(std::chrono::duration<double, std::milli>(now - q->t_submit).count());
-            for (axhel_ntt_t h : q->ntts) axhel_cuda_ntt_release(h);
-            q->ntts.clear();
-            ++completed;
+        // Poll every request of every batch in flight: batches of the two
+        // lanes finish out of launch order, and a request completes as soon
+        // as its own result has landed.
+        bool progress = false;
+        for (auto it = inflight.begin(); it != inflight.end();) {
+            Inflight& f = *it;
+            Slot& sl = slots[f.slot];
+            while (!f.reqs.empty()) {
+                cudaEvent_t ev = f.done.empty() ? nullptr : f.done.front();
+                const cudaError_t e = ev ? cudaEventQuery(ev) : cudaErrorNotReady;
+                if (e == cudaErrorNotReady) break;
+                Req* q = f.reqs.front();
+                q->status = (e == cudaSuccess) ? *sl.err_host : AXHEL_ERR_CUDA;
+                q->t_done = Clock::now();
+                lat_ms.push_back(std::chrono::duration<double, std::milli>(q->t_done - q->t_submit).count());
+                for (axhel_ntt_t h : q->ntts) axhel_cuda_ntt_release(h);
+                q->ntts.clear();
+                ++completed;
+                in_use -= q->need;
+                event_pool.push_back(ev);
+                f.done.erase(f.done.begin());
+                f.reqs.erase(f.reqs.begin());
+                progress = true;
+            }
+            if (f.reqs.empty()) {
+                for (cudaEvent_t ev : f.done) event_pool.push_back(ev);
+                sl.busy = false;
+                it = inflight.erase(it);
+            } else {
+                ++it;
+            }
         }
-        cudaEventDestroy(f.done);
-        s.busy = false;
-        in_use -= f.bytes;
-        cv_sched.notify_all();
-        cv_wait.notify_all();
+        if (progress) {
+            cv_wait.notify_all();
+            cv_sched.notify_all();
+        } else {
+            cv_done.wait_for(lk, std::chrono::microseconds(20));
+        }
     }
 }
 
@@ -311,9 +376,17 @@ axhel_status_t axhel_server_create(const axhel_server_config_t* cfg, axhel_serve
         uint64_t keep = cfg->hbm_budget_bytes;  // keep freed blocks for reuse up to the budget
         e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
-    s->slots.resize(cfg->max_inflight);
-    for (Slot& sl : s->slots) {
-        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
+    s->lanes = cfg->small_request_words ? 2 : 1;
+    int prio_low = 0, prio_high = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+    s->slots.resize((size_t)cfg->max_inflight * s->lanes);
+    for (size_t i = 0; i < s->slots.size(); ++i) {
+        Slot& sl = s->slots[i];
+        // with two lanes, lane 0 (small requests) gets the highest priority:
+        // its CTAs are dispatched ahead of the large lane's as SMs free up
+        sl.lane = s->lanes == 2 ? (int)(i / cfg->max_inflight) : 1;
+        const int prio = sl.lane == 0 ? prio_high : prio_low;
+        if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&sl.stream, cudaStreamNonBlocking, prio);
         if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&sl.err_host), sizeof(int));
     }
     if (e != cudaSuccess) {
@@ -367,7 +440,8 @@ axhel_status_t axhel_server_submit(axhel_server_t s, const axhel_request_t* r, u
     q->id = s->next_id++;
     q->t_submit = Clock::now();
     *id = q->id;
-    s->pending.push_back(q.get());
+    const int lane = (s->lanes == 2 && q->words <= s->cfg.small_request_words) ? 0 : 1;
+    s->pending[lane].push_back(q.get());
     s->reqs.emplace(q->id, std::move(q));
     s->cv_sched.notify_one();
     return AXHEL_OK;
@@ -430,7 +504,7 @@ axhel_status_t axhel_server_stats(axhel_server_t s, axhel_server_stats_t* out, i
     out->completed = s->completed;
     out->batches = s->batches;
     out->max_batch_requests = s->max_batch;
-    out->pending = s->pending.size();
+    out->pending = s->pending[0].size() + s->pending[1].size();
     out->in_use_bytes = s->in_use;
     out->peak_in_use_bytes = s->peak_in_use;
     out->p50_ms = pct(0.50);
@@ -456,7 +530,9 @@ axhel_status_t axhel_server_destroy(axhel_server_t s)
         if (sl.scratch) cudaFree(sl.scratch);
         cudaStreamDestroy(sl.stream);
         cudaFreeHost(sl.err_host);
+        if (sl.host_img) cudaFreeHost(sl.host_img);
     }
+    for (cudaEvent_t ev : s->event_pool) cudaEventDestroy(ev);
     for (auto& kv : s->reqs)
         for (axhel_ntt_t h : kv.second->ntts) axhel_cuda_ntt_release(h);
     cudaMemPoolDestroy(s->pool);
@@ -465,5 +541,112 @@ axhel_status_t axhel_server_destroy(axhel_server_t s)
 }
 
 const char* axhel_server_last_error(void) { return t_serve_error.c_str(); }
+
+axhel_status_t axhel_server_drive(axhel_server_t server, const axhel_request_t* templates, uint32_t n_templates,
+                                  uint64_t* const* outputs, uint32_t copies, const double* isolated_ms,
+                                  double rate_per_s, double seconds, uint64_t seed, axhel_drive_result_t* out)
+{
+    if (!server || !templates || !n_templates || !outputs || !copies || !out || rate_per_s <= 0 || seconds <= 0)
+        return sfail(AXHEL_ERR_INVALID, "bad drive arguments");
+    std::memset(out, 0, sizeof *out);
+    struct Live {
+        uint64_t id;
+        uint32_t t, c;
+    };
+    std::vector<std::vector<uint32_t>> free_copies(n_templates);
+    for (uint32_t t = 0; t < n_templates; ++t)
+        for (uint32_t c = 0; c < copies; ++c) free_copies[t].push_back(copies - 1 - c);
+    std::mutex fm;
+    std::deque<Live> live;
+    std::condition_variable lv;
+    bool done = false;
+    std::vector<double> lat, slow, iso;
+    uint64_t failed = 0;
+    // collector: waits for requests in submission order, frees their copies
+    std::thread collector([&] {
+        for (;;) {
+            Live l;
+            {
+                std::unique_lock<std::mutex> lk(fm);
+                lv.wait(lk, [&] { return done || !live.empty(); });
+                if (live.empty()) return;
+                l = live.front();
+                live.pop_front();
+            }
+            axhel_request_info_t info{};
+            const axhel_status_t st = axhel_server_wait(server, l.id, 120000000ull, &info);
+            std::lock_guard<std::mutex> lk(fm);
+            if (st != AXHEL_OK) {
+                ++failed;
+            } else {
+                lat.push_back(info.latency_ms);
+                if (isolated_ms) {
+                    slow.push_back(info.latency_ms / isolated_ms[l.t]);
+                    iso.push_back(isolated_ms[l.t]);
+                }
+            }
+            free_copies[l.t].push_back(l.c);
+        }
+    });
+    // producer: Poisson arrivals (exponential gaps), uniform template choice
+    uint64_t x = seed ? seed : 0x9e3779b97f4a7c15ull;
+    auto next_u = [&]() {  // xorshift64*: uniform in (0, 1)
+        x ^= x >> 12;
+        x ^= x << 25;
+        x ^= x >> 27;
+        return ((x * 0x2545F4914F6CDD1Dull) >> 11) * (1.0 / 9007199254740992.0) + 1e-18;
+    };
+    const auto t0 = Clock::now();
+    const auto end = t0 + std::chrono::duration<double>(seconds);
+    auto t = t0;
+    axhel_status_t rc = AXHEL_OK;
+    while (true) {
+        t += std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(-std::log(next_u()) / rate_per_s));
+        if (t >= end) break;
+        std::this_thread::sleep_until(t);
+        const uint32_t k = (uint32_t)(next_u() * n_templates) % n_templates;
+        uint32_t c;
+        {
+            std::lock_guard<std::mutex> lk(fm);
+            if (free_copies[k].empty()) {
+                ++out->skipped;
+                continue;
+            }
+            c = free_copies[k].back();
+            free_copies[k].pop_back();
+        }
+        axhel_request_t r = templates[k];
+        r.output = outputs[(size_t)k * copies + c];
+        uint64_t id = 0;
+        rc = axhel_server_submit(server, &r, &id);
+        if (rc) break;
+        ++out->submitted;
+        std::lock_guard<std::mutex> lk(fm);
+        live.push_back(Live{id, k, c});
+        lv.notify_one();
+    }
+    {
+        std::lock_guard<std::mutex> lk(fm);
+        done = true;
+        lv.notify_all();
+    }
+    collector.join();
+    const double wall = std::chrono::duration<double>(Clock::now() - t0).count();
+    auto pct = [](std::vector<double> v, double p) {
+        if (v.empty()) return 0.0;
+        std::sort(v.begin(), v.end());
+        return v[std::min(v.size() - 1, (size_t)(p * (v.size() - 1) + 0.5))];
+    };
+    out->completed = lat.size();
+    out->failed = failed;
+    out->wall_s = wall;
+    out->jobs_per_s = lat.size() / wall;
+    out->p50_ms = pct(lat, 0.5);
+    out->p99_ms = pct(lat, 0.99);
+    out->p50_slowdown = pct(slow, 0.5);
+    out->p99_slowdown = pct(slow, 0.99);
+    out->isolated_p99_ms = pct(iso, 0.99);
+    return rc;
+}
 
 }  // extern "C"

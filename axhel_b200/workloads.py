@@ -205,15 +205,17 @@ def uneven_batch(n_polys=512, seed=11, reps=3):
 
 class RequestPool:
     """C5 request templates: INTT -> MulMod/FMAMod -> NTT, N ~ U{2^13..2^17},
-    L ~ U{2..40}, primes of 40-59 bits; inputs and vectors in pinned host
-    memory, `copies` pinned output buffers per template."""
+    L ~ U{2..40}, primes of 40-59 bits.  Inputs and vectors live in pinned
+    host memory (host-staged requests) or in HBM (device-resident requests);
+    `copies` output buffers per template."""
 
-    def __init__(self, n_templates=32, seed=21, copies=4, logn_lo=13, logn_hi=17, L_lo=2, L_hi=40):
+    def __init__(self, n_templates=32, seed=21, copies=4, device=False, logn_lo=13, logn_hi=17, L_lo=2, L_hi=40):
         import torch
 
         rng = np.random.default_rng(seed)
         self.pool = ModulusPool()
         self.t = []
+        self.device = device
         for k in range(n_templates):
             logn = int(rng.integers(logn_lo, logn_hi + 1))
             n = 1 << logn
@@ -222,13 +224,15 @@ class RequestPool:
             qs = np.array([q for q, _ in mods], dtype=np.uint64)[:, None]
             kind = 3 if k % 2 == 0 else 4
 
-            def pin(a):
-                t = torch.from_numpy(a.reshape(-1).view(np.int64)).pin_memory()
-                return t
+            def place(a):
+                t = torch.from_numpy(a.reshape(-1).view(np.int64))
+                return t.cuda() if device else t.pin_memory()
 
-            x = pin((rng.random((L, n)) * (2 * qs)).astype(np.uint64))
-            v = pin((rng.random((L, n)) * (2 * qs)).astype(np.uint64))
-            outs = [torch.empty(L * n, dtype=torch.int64).pin_memory() for _ in range(copies)]
+            x = place((rng.random((L, n)) * (2 * qs)).astype(np.uint64))
+            v = place((rng.random((L, n)) * (2 * qs)).astype(np.uint64))
+            outs = [torch.empty(L * n, dtype=torch.int64, device="cuda" if device else "cpu") for _ in range(copies)]
+            if not device:
+                outs = [o.pin_memory() for o in outs]
             sc = [int(rng.integers(0, 2 * int(q))) for q, _ in mods]
             self.t.append(dict(n=n, L=L, kind=kind, ntts=[t for _, t in mods], x=x, v=v, outs=outs,
                                free=list(range(copies)), sc=sc))
@@ -252,109 +256,92 @@ class RequestPool:
                           vector=t["v"].data_ptr(), scalars=t["sc"] if t["kind"] == 4 else None, in_f=2, out_f=4)
 
 
-def serving(loads=(0.5, 0.7, 0.9), seconds=4.0, budget=60 << 30, inflight=3, seed=5, n_templates=32):
-    """Capacity (a burst), isolated latency (one at a time), then Poisson
-    arrivals at each load fraction of capacity: p50/p99 and jobs/s."""
-    rp = RequestPool(n_templates=n_templates, seed=seed)
-    srv = capi.Server(budget_bytes=budget, max_inflight=inflight, max_batch_requests=256)
+def _pct(v, p):
+    v = sorted(v)
+    return v[min(len(v) - 1, int(p * (len(v) - 1) + 0.5))] if v else None
+
+
+def serving(loads=(0.5, 0.7, 0.9), seconds=4.0, budget=60 << 30, inflight=4, seed=5, n_templates=32,
+            device=False, max_batch_words=0, persistent=False, plain=True, small_words=0):
+    """Isolated latency of every template (alone on an idle server), capacity
+    (a burst), then Poisson arrivals at each load fraction of capacity:
+    p50/p99 latency, p99 of each request's slowdown against its own isolated
+    latency, and jobs/s; then the plain sequential GPU path."""
+    rp = RequestPool(n_templates=n_templates, seed=seed, device=device)
+    srv = capi.Server(budget_bytes=budget, max_inflight=inflight, max_batch_requests=256,
+                      max_batch_words=max_batch_words, persistent=persistent, small_request_words=small_words)
     rng = np.random.default_rng(seed)
 
-    # isolated: each template alone on an idle server
     iso = []
     for k in range(len(rp.t)):
-        for _ in range(2):
+        runs = []
+        for _ in range(3):
             rid = rp.submit(srv, k, 0)
             st, info = srv.wait(rid)
             assert st == 0
-        iso.append(info.latency_ms)
-    iso_med = statistics.median(iso)
+            runs.append(info.latency_ms)
+        iso.append(statistics.median(runs))
 
-    # capacity: a burst of requests submitted at once
-    burst = []
-    t0 = time.perf_counter()
-    for i in range(8 * len(rp.t)):
-        got = rp.take(rng)
-        if got is None:
-            break
-        burst.append((rp.submit(srv, *got), got))
-    for rid, got in burst:
-        st, _ = srv.wait(rid)
-        assert st == 0
-        rp.give(*got)
-    cap = len(burst) / (time.perf_counter() - t0)
+    # capacity: a burst queued while admission is held, timed from its release
+    caps = []
+    for _ in range(3):
+        burst = []
+        srv.pause(True)
+        for i in range(8 * len(rp.t)):
+            got = rp.take(rng)
+            if got is None:
+                break
+            burst.append((rp.submit(srv, *got), got))
+        t0 = time.perf_counter()
+        srv.pause(False)
+        for rid, got in burst:
+            st, _ = srv.wait(rid)
+            assert st == 0
+            rp.give(*got)
+        caps.append(len(burst) / (time.perf_counter() - t0))
+    cap = statistics.median(caps)
     srv.stats(reset=True)
 
     results = []
+    templates = [dict(kind=t["kind"], ntts=t["ntts"], count=t["L"], input=t["x"].data_ptr(),
+                      vector=t["v"].data_ptr(), scalars=t["sc"] if t["kind"] == 4 else None, in_f=2, out_f=4)
+                 for t in rp.t]
+    outputs = [[o.data_ptr() for o in t["outs"]] for t in rp.t]
     for frac in loads:
-        rate = frac * cap
-        stop = threading.Event()
-        inflight_q = []
-        qlock = threading.Lock()
-        lat = []
-        dropped = [0]
-
-        def producer():
-            t = time.perf_counter()
-            end = t + seconds
-            while t < end:
-                t += rng.exponential(1.0 / rate)
-                while True:
-                    now = time.perf_counter()
-                    if now >= t:
-                        break
-                    time.sleep(min(t - now, 0.001))
-                got = rp.take(rng)
-                if got is None:
-                    dropped[0] += 1
-                    continue
-                rid = rp.submit(srv, *got)
-                with qlock:
-                    inflight_q.append((rid, got))
-            stop.set()
-
-        def consumer():
-            while True:
-                with qlock:
-                    item = inflight_q.pop(0) if inflight_q else None
-                if item is None:
-                    if stop.is_set():
-                        with qlock:
-                            if not inflight_q:
-                                return
-                    time.sleep(0.0002)
-                    continue
-                rid, got = item
-                st, info = srv.wait(rid)
-                assert st == 0
-                lat.append(info.latency_ms)
-                rp.give(*got)
-
-        t0 = time.perf_counter()
-        th = [threading.Thread(target=producer), threading.Thread(target=consumer)]
-        for x in th:
-            x.start()
-        for x in th:
-            x.join()
-        wall = time.perf_counter() - t0
-        lat.sort()
-        pct = lambda p: lat[min(len(lat) - 1, int(p * (len(lat) - 1) + 0.5))]
-        results.append({"load": frac, "offered_per_s": rate, "jobs_per_s": len(lat) / wall, "p50_ms": pct(0.5),
-                        "p99_ms": pct(0.99), "p99_over_isolated": pct(0.99) / iso_med, "requests": len(lat),
-                        "skipped_no_buffer": dropped[0]})
+        d = srv.drive(templates, outputs, iso, frac * cap, seconds, seed=int(frac * 1000) + seed)
+        results.append({"load": frac, "offered_per_s": frac * cap, "jobs_per_s": d["jobs_per_s"],
+                        "p50_ms": d["p50_ms"], "p99_ms": d["p99_ms"], "isolated_p99_ms": d["isolated_p99_ms"],
+                        "p99_over_isolated_p99": d["p99_ms"] / d["isolated_p99_ms"] if d["isolated_p99_ms"] else None,
+                        "p50_slowdown": d["p50_slowdown"], "p99_slowdown": d["p99_slowdown"],
+                        "requests": d["completed"], "skipped_no_buffer": d["skipped"], "failed": d["failed"]})
     st = srv.stats()
     srv.close()
 
-    # plain sequential GPU path: each request as per-limb C-ABI calls, one after another
+    out = {"workload": "INTT->MulMod/FMAMod->NTT requests, N in 2^13..2^17, L in 2..40, Poisson arrivals",
+           "operands": "device-resident" if device else "host pinned, staged per request",
+           "launch": "persistent" if persistent else "one launch per phase", "max_batch_words": max_batch_words,
+           "small_request_words": small_words,
+           "capacity_jobs_per_s": cap, "isolated_median_ms": statistics.median(iso), "loads": results,
+           "batches": st["batches"], "max_batch_requests": st["max_batch_requests"],
+           "peak_in_use_bytes": st["peak_in_use_bytes"], "budget_bytes": budget, "max_inflight": inflight}
+    if plain:
+        out["plain_sequential_jobs_per_s"] = plain_sequential(rp)
+    return out
+
+
+def plain_sequential(rp, limit=16):
+    """Each request as the reference call pattern: per limb ComputeInverse,
+    MulMod / FMAMod, ComputeForward through the C-ABI, one request after the
+    other, operands copied in and out as in the served form."""
     import torch
 
-    seq_n = min(len(rp.t), 16)
-    dbuf = {}
+    n_req = min(len(rp.t), limit)
     t0 = time.perf_counter()
-    for k in range(seq_n):
+    for k in range(n_req):
         t = rp.t[k]
-        n, L = t["n"], t["L"]
-        x = t["x"].cuda(non_blocking=True)
-        v = t["v"].cuda(non_blocking=True)
+        n = t["n"]
+        x = t["x"] if rp.device else t["x"].cuda(non_blocking=True)
+        v = t["v"] if rp.device else t["v"].cuda(non_blocking=True)
         y = torch.empty_like(x)
         for i, h in enumerate(t["ntts"]):
             o = 8 * n * i
@@ -365,27 +352,27 @@ def serving(loads=(0.5, 0.7, 0.9), seconds=4.0, budget=60 << 30, inflight=3, see
                 capi.fma(y.data_ptr() + o, y.data_ptr() + o, t["sc"][i], v.data_ptr() + o, n, h.modulus, 2)
             h.forward(y.data_ptr() + o, y.data_ptr() + o, 1, 4)
         t["outs"][0].copy_(y)
-        dbuf[k] = y
-    torch.cuda.synchronize()
-    seq_rate = seq_n / (time.perf_counter() - t0)
-    return {"workload": "INTT->MulMod/FMAMod->NTT requests, N in 2^13..2^17, L in 2..40, Poisson arrivals",
-            "capacity_jobs_per_s": cap, "isolated_median_ms": iso_med, "loads": results,
-            "plain_sequential_jobs_per_s": seq_rate, "batches": st["batches"],
-            "max_batch_requests": st["max_batch_requests"], "peak_in_use_bytes": st["peak_in_use_bytes"],
-            "budget_bytes": budget, "max_inflight": inflight}
+        torch.cuda.synchronize()
+    return n_req / (time.perf_counter() - t0)
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("what", choices=["tensor", "uneven", "serve"])
     ap.add_argument("--seconds", type=float, default=4.0)
+    ap.add_argument("--device", action="store_true", help="device-resident request operands")
+    ap.add_argument("--persistent", action="store_true", help="one persistent launch per batch")
+    ap.add_argument("--max-batch-words", type=int, default=0)
+    ap.add_argument("--inflight", type=int, default=4)
+    ap.add_argument("--small-words", type=int, default=0, help="high-priority lane for requests up to this size")
     a = ap.parse_args()
     if a.what == "tensor":
         out = tensor_chain()
     elif a.what == "uneven":
         out = uneven_batch()
     else:
-        out = serving(seconds=a.seconds)
+        out = serving(seconds=a.seconds, device=a.device, persistent=a.persistent,
+                      max_batch_words=a.max_batch_words, inflight=a.inflight, small_words=a.small_words)
     print(json.dumps(out), flush=True)
 
 

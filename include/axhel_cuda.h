@@ -201,10 +201,16 @@ axhel_status_t axhel_cuda_batch_debug_unreachable(axhel_batch_t batch, uint64_t 
 
 typedef struct axhel_server* axhel_server_t;
 
+#define AXHEL_SERVER_PERSISTENT 1u /* run each batch as one persistent launch (default: one launch per phase) */
+
 typedef struct axhel_server_config {
-    uint64_t hbm_budget_bytes;   /* device bytes the server may hold for staged operands */
-    uint32_t max_inflight;       /* batches concurrently on the GPU (1..16 streams) */
-    uint32_t max_batch_requests; /* requests admitted into one batch launch */
+    uint64_t hbm_budget_bytes;    /* device bytes the server may hold for staged operands */
+    uint64_t max_batch_words;     /* residues admitted into one batch (0 = no cap; a larger request runs alone) */
+    uint64_t small_request_words; /* requests up to this many residues take the high-priority lane (0 = one lane) */
+    uint32_t max_inflight;        /* batches concurrently on the GPU per lane (1..16 streams) */
+    uint32_t max_batch_requests;  /* requests admitted into one batch */
+    uint32_t flags;               /* AXHEL_SERVER_* */
+    uint32_t reserved;
 } axhel_server_config_t;
 
 /* One request: a job of the batch engine (AXHEL_JOB_*).  input / output /
@@ -252,6 +258,22 @@ axhel_status_t axhel_server_pause(axhel_server_t server, int paused);
 axhel_status_t axhel_server_stats(axhel_server_t server, axhel_server_stats_t* out, int reset_latencies);
 /* Stops admission, drains the batches in flight, frees everything. */
 axhel_status_t axhel_server_destroy(axhel_server_t server);
+
+/* Load driver (new; a measuring tool for the serving loop): submits requests
+ * drawn uniformly from `templates` at Poisson arrival times of mean rate
+ * `rate_per_s` for `seconds`, from one C++ thread, and waits for all of
+ * them.  Template t writes its result to outputs[t * copies + c] for a copy c
+ * not in use by another in-flight request of the same template (an arrival
+ * finding none free is skipped and counted).  isolated_ms[t] (may be NULL)
+ * is the template's latency alone, for the slowdown percentiles. */
+typedef struct axhel_drive_result {
+    uint64_t submitted, completed, skipped, failed;
+    double wall_s, jobs_per_s;
+    double p50_ms, p99_ms, p50_slowdown, p99_slowdown, isolated_p99_ms;
+} axhel_drive_result_t;
+axhel_status_t axhel_server_drive(axhel_server_t server, const axhel_request_t* templates, uint32_t n_templates,
+                                  uint64_t* const* outputs, uint32_t copies, const double* isolated_ms,
+                                  double rate_per_s, double seconds, uint64_t seed, axhel_drive_result_t* out);
 const char* axhel_server_last_error(void);
 
 /* ---------------------------------------------------------------------- */

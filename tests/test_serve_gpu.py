@@ -81,12 +81,15 @@ def test_same_bits_alone_and_in_a_mix(cuda, oracle):
         assert st == 0 and info.batch_size == 1
         alone.append(result(bufs, r["x"].size, k % 2 == 0))
         np.testing.assert_array_equal(alone[-1], expected(oracle, r), err_msg=f"request {k}")
-    # everything at once, twice over: batches mix requests and overlap
+    # everything at once, twice over: admission held while the requests
+    # arrive, then released, so batches mix requests (and two run at a time)
     handles = []
+    srv.pause(True)
     for rep in range(2):
         for k, r in enumerate(reqs):
             rid, bufs = submit(srv, r, on_device=(k + rep) % 2 == 0)
             handles.append((k, rid, bufs, (k + rep) % 2 == 0))
+    srv.pause(False)
     sizes = []
     for k, rid, bufs, on_dev in handles:
         st, info = srv.wait(rid)
