@@ -65,7 +65,7 @@ KernelTable& table()
 
 std::mutex g_attr_mu;
 
-size_t smem_bytes(const PassCfg& c) { return (size_t)c.tg * ((size_t(1) << c.lg) + 1) * sizeof(uint64_t); }
+size_t smem_bytes(const PassCfg& c) { return (size_t)c.tg * (size_t(1) << c.lg) * sizeof(uint64_t); }
 
 template <class Fn>
 cudaError_t ensure_smem(Fn fn, int kind, const PassCfg& c)

@@ -14,7 +14,7 @@
 // Each thread holds R = 2^LR elements of one group in registers and applies
 // LR consecutive stages to them per round.  The first round loads straight
 // from global memory and the last round stores straight back; shared memory
-// (padded, XOR-swizzled) is used only to exchange elements between rounds,
+// (XOR-swizzled, bank-conflict free) is used only to exchange elements between rounds,
 // with one barrier per exchange.  Global accesses are coalesced: in strided
 // tiles consecutive lanes take consecutive columns; in contiguous tiles a
 // round whose register bits are the low bits reads R consecutive words per
@@ -65,9 +65,38 @@ constexpr int round_lo()
     }
 }
 
-// XOR swizzle of the in-group index: flips the low 4 bits by bits 4..7 so
-// that both unit-stride and stride-16 register fetches hit distinct banks.
-__device__ __forceinline__ uint32_t swz(uint32_t r) { return r ^ ((r >> 4) & 15u); }
+// XOR swizzle of the in-group index for register depth LR: the low 4 bits
+// (the 8-byte bank pair among 16) are flipped by index bits LR..LR+3.  In a
+// round whose register bits start at lo < 4, the 16 lanes of a half-warp vary
+// in index bits [0, lo) and [lo + LR, LR + 4); the shift by LR lands the
+// latter on [lo, 4), so every round's access hits 16 distinct bank pairs.
+// (A bijection: each flipped bit is flipped by bits above it.)
+template <int LR>
+__device__ __forceinline__ uint32_t swz(uint32_t r)
+{
+    return r ^ ((r >> LR) & 15u);
+}
+
+// Shared-memory slot of in-group index r: groups are stored unpadded, G words
+// each; `hmask` (per thread, below) XORs the group's varying bits into the
+// bank pairs the element bits leave free, so half-warps that span several
+// groups stay conflict-free too.
+template <int LG, int LR>
+__device__ __forceinline__ uint32_t slot(uint32_t r, uint32_t hmask)
+{
+    if constexpr (LG < 4) return r;
+    return swz<LR>(r) ^ hmask;
+}
+
+// Group bits of a half-warp's lanes sit above the element bits: strided tiles
+// put the group first in the lane index (lgtg bits), contiguous tiles the
+// thread-in-group first (LG - LR bits).
+template <int LG, int LR>
+__device__ __forceinline__ uint32_t group_mask(bool strided, uint32_t lgtg, uint32_t gi)
+{
+    const uint32_t nk = strided ? (lgtg >= 4 ? 0u : 4u - lgtg) : ((LG - LR) >= 4 ? 4u : (uint32_t)(LG - LR));
+    return (gi << nk) & 15u;
+}
 
 // Per-CTA tile geometry.
 struct Tile {
@@ -206,11 +235,12 @@ __device__ __forceinline__ void fwd_stages(uint64_t (&v)[1 << LR], uint32_t rbas
         const int b = hi - 1 - bb;  // in-group bit = butterfly span
         const int rb = b - lo;      // register bit
         const uint32_t t = s0 + (LG - 1 - b);
+        // the twiddles of this stage are consecutive: rbase's register bits
+        // are zero, so (rbase | j << (b+1)) >> (b+1) = (rbase >> (b+1)) + j
+        const ulonglong2* tws = tw + (1ull << t) + (blk << (LG - 1 - b)) + (rbase >> (b + 1));
 #pragma unroll
         for (int j = 0; j < (R >> (rb + 1)); ++j) {
-            const uint32_t rrep = rbase | ((uint32_t)(j << (rb + 1)) << lo);
-            const uint64_t idx = (1ull << t) + (blk << (LG - 1 - b)) + (rrep >> (b + 1));
-            const ulonglong2 w = __ldg(tw + idx);
+            const ulonglong2 w = __ldg(tws + j);
 #pragma unroll
             for (int l = 0; l < (1 << rb); ++l) {
                 const int i0 = (j << (rb + 1)) | l;
@@ -245,12 +275,10 @@ __device__ __forceinline__ void inv_stages(uint64_t (&v)[1 << LR], uint32_t rbas
                 }
         } else {
             const uint32_t s = s0 + b;
-            const uint64_t stage_base = 1 + n - (n >> s);
+            const ulonglong2* tws = tw + (1 + n - (n >> s)) + (blk << (LG - b - 1)) + (rbase >> (b + 1));
 #pragma unroll
             for (int j = 0; j < (R >> (rb + 1)); ++j) {
-                const uint32_t rrep = rbase | ((uint32_t)(j << (rb + 1)) << lo);
-                const uint64_t idx = stage_base + (blk << (LG - b - 1)) + (rrep >> (b + 1));
-                const ulonglong2 w = __ldg(tw + idx);
+                const ulonglong2 w = __ldg(tws + j);
 #pragma unroll
                 for (int l = 0; l < (1 << rb); ++l) {
                     const int i0 = (j << (rb + 1)) | l;
@@ -265,54 +293,55 @@ __device__ __forceinline__ void inv_stages(uint64_t (&v)[1 << LR], uint32_t rbas
 // thread writes back the slots it held and reads its next slots; the slot
 // sets of one round are disjoint across threads, so one barrier suffices.
 template <bool INV, int LG, int LR, int RD>
-__device__ __forceinline__ void exchange(uint64_t (&v)[1 << LR], uint64_t* smg, uint32_t k)
+__device__ __forceinline__ void exchange(uint64_t (&v)[1 << LR], uint64_t* smg, uint32_t k, uint32_t hmask)
 {
     constexpr int R = 1 << LR;
     constexpr int lp = round_lo<INV, LG, LR, RD - 1>();
     constexpr int ln = round_lo<INV, LG, LR, RD>();
     const uint32_t bp = round_base<LR>(k, lp), bn = round_base<LR>(k, ln);
 #pragma unroll
-    for (int i = 0; i < R; ++i) smg[swz(bp | ((uint32_t)i << lp))] = v[i];
+    for (int i = 0; i < R; ++i) smg[slot<LG, LR>(bp | ((uint32_t)i << lp), hmask)] = v[i];
     __syncthreads();
 #pragma unroll
-    for (int i = 0; i < R; ++i) v[i] = smg[swz(bn | ((uint32_t)i << ln))];
+    for (int i = 0; i < R; ++i) v[i] = smg[slot<LG, LR>(bn | ((uint32_t)i << ln), hmask)];
 }
 
 // Rounds 1 .. NR-1 (round 0 runs on the freshly loaded registers).
 template <int LG, int LR, int... RD>
 __device__ __forceinline__ void fwd_rest(std::integer_sequence<int, RD...>, uint64_t (&v)[1 << LR], uint64_t* smg,
-                                         uint32_t k, uint64_t blk, uint32_t s0, const ulonglong2* tw, uint64_t q,
-                                         uint64_t q2)
+                                         uint32_t k, uint32_t hmask, uint64_t blk, uint32_t s0, const ulonglong2* tw,
+                                         uint64_t q, uint64_t q2)
 {
-    ((exchange<false, LG, LR, RD + 1>(v, smg, k),
+    ((exchange<false, LG, LR, RD + 1>(v, smg, k, hmask),
       fwd_stages<LG, LR, RD + 1>(v, round_base<LR>(k, round_lo<false, LG, LR, RD + 1>()), blk, s0, tw, q, q2)),
      ...);
 }
 
 template <int LG, int LR, int... RD>
 __device__ __forceinline__ void inv_rest(std::integer_sequence<int, RD...>, uint64_t (&v)[1 << LR], uint64_t* smg,
-                                         uint32_t k, uint64_t blk, uint32_t s0, uint64_t n, const ulonglong2* tw,
-                                         uint64_t q, uint64_t q2, bool last, const ModCtx* cx)
+                                         uint32_t k, uint32_t hmask, uint64_t blk, uint32_t s0, uint64_t n,
+                                         const ulonglong2* tw, uint64_t q, uint64_t q2, bool last, const ModCtx* cx)
 {
-    ((exchange<true, LG, LR, RD + 1>(v, smg, k),
+    ((exchange<true, LG, LR, RD + 1>(v, smg, k, hmask),
       inv_stages<LG, LR, RD + 1>(v, round_base<LR>(k, round_lo<true, LG, LR, RD + 1>()), blk, s0, n, tw, q, q2,
                                  last, cx)),
      ...);
 }
 
 template <bool INV, int LG, int LR>
-__device__ __forceinline__ void run_rounds(uint64_t (&v)[1 << LR], uint64_t* smg, uint32_t k, uint64_t blk,
-                                           uint32_t s0, uint64_t n, const ModCtx* cx, uint64_t q, uint64_t q2,
-                                           bool last)
+__device__ __forceinline__ void run_rounds(uint64_t (&v)[1 << LR], uint64_t* smg, uint32_t k, uint32_t hmask,
+                                           uint64_t blk, uint32_t s0, uint64_t n, const ModCtx* cx, uint64_t q,
+                                           uint64_t q2, bool last)
 {
     constexpr int NR = num_rounds<LG, LR>();
     if constexpr (INV) {
         inv_stages<LG, LR, 0>(v, round_base<LR>(k, round_lo<true, LG, LR, 0>()), blk, s0, n, cx->inv, q, q2, last,
                               cx);
-        inv_rest<LG, LR>(std::make_integer_sequence<int, NR - 1>{}, v, smg, k, blk, s0, n, cx->inv, q, q2, last, cx);
+        inv_rest<LG, LR>(std::make_integer_sequence<int, NR - 1>{}, v, smg, k, hmask, blk, s0, n, cx->inv, q, q2,
+                         last, cx);
     } else {
         fwd_stages<LG, LR, 0>(v, round_base<LR>(k, round_lo<false, LG, LR, 0>()), blk, s0, cx->fwd, q, q2);
-        fwd_rest<LG, LR>(std::make_integer_sequence<int, NR - 1>{}, v, smg, k, blk, s0, cx->fwd, q, q2);
+        fwd_rest<LG, LR>(std::make_integer_sequence<int, NR - 1>{}, v, smg, k, hmask, blk, s0, cx->fwd, q, q2);
     }
 }
 
@@ -326,7 +355,6 @@ __device__ __forceinline__ void pass_tile(const uint64_t* src, uint64_t* dst, co
                                           uint32_t flags, uint64_t* sm)
 {
     constexpr int R = 1 << LR;
-    constexpr int GP = (1 << LG) + 1;
     constexpr int NR = num_rounds<LG, LR>();
     constexpr int LO_FIRST = round_lo<INV, LG, LR, 0>();
     constexpr int LO_LAST = round_lo<INV, LG, LR, NR - 1>();
@@ -348,7 +376,8 @@ __device__ __forceinline__ void pass_tile(const uint64_t* src, uint64_t* dst, co
 #pragma unroll
         for (int i = 0; i < R; ++i) v[i] = csub_lazy(v[i], q2);
     }
-    run_rounds<INV, LG, LR>(v, sm + gi * GP, k, blk, s0, n, cx, q, q2, (flags & kLastPass) != 0);
+    run_rounds<INV, LG, LR>(v, sm + (gi << LG), k, group_mask<LG, LR>(t.strided, lgtg, gi), blk, s0, n, cx, q, q2,
+                            (flags & kLastPass) != 0);
     if (flags & kPostNorm) {
 #pragma unroll
         for (int i = 0; i < R; ++i) v[i] = INV ? csub_lazy(v[i], q) : csub_lazy(csub_lazy(v[i], q2), q);
@@ -380,7 +409,6 @@ __device__ __forceinline__ void chain_tile(const uint64_t* src, uint64_t* dst, c
                                            uint64_t* sm)
 {
     constexpr int R = 1 << LR;
-    constexpr int GP = (1 << LG) + 1;
     constexpr int NR = num_rounds<LG, LR>();
     constexpr int LO_FIRST = round_lo<true, LG, LR, 0>();
     constexpr int LO_MID = round_lo<true, LG, LR, NR - 1>();
@@ -397,7 +425,8 @@ __device__ __forceinline__ void chain_tile(const uint64_t* src, uint64_t* dst, c
     uint32_t gi, k;
     thread_role<LG, LR>(t, gi, k);
     const uint64_t blk = tile_blk<LG>(t, gi);
-    uint64_t* smg = sm + gi * GP;
+    uint64_t* smg = sm + (gi << LG);
+    const uint32_t hmask = group_mask<LG, LR>(t.strided, lgtg, gi);
 
     uint64_t v[R];
     load_global<LG, LR, LO_FIRST, CG>(v, lsrc, t, gi, round_base<LR>(k, LO_FIRST), vec_ok);
@@ -405,7 +434,7 @@ __device__ __forceinline__ void chain_tile(const uint64_t* src, uint64_t* dst, c
 #pragma unroll
         for (int i = 0; i < R; ++i) v[i] = csub_lazy(v[i], q2);
     }
-    run_rounds<true, LG, LR>(v, smg, k, blk, logn - LG, n, cx, q, q2, true);
+    run_rounds<true, LG, LR>(v, smg, k, hmask, blk, logn - LG, n, cx, q, q2, true);
 
     // Element-wise op on the inverse output (lazy [0, 2q)) with factor-2
     // inputs: EltwiseMulModNative<2> / EltwiseFMAModNative<2> formulas.
@@ -432,7 +461,7 @@ __device__ __forceinline__ void chain_tile(const uint64_t* src, uint64_t* dst, c
 
     // The forward's first pass: stages 0 .. LG-1 of block 0.
     fwd_stages<LG, LR, 0>(v, rb, 0, 0, cx->fwd, q, q2);
-    fwd_rest<LG, LR>(std::make_integer_sequence<int, NR - 1>{}, v, smg, k, 0, 0, cx->fwd, q, q2);
+    fwd_rest<LG, LR>(std::make_integer_sequence<int, NR - 1>{}, v, smg, k, hmask, 0, 0, cx->fwd, q, q2);
     if (flags & kPostNorm) {
 #pragma unroll
         for (int i = 0; i < R; ++i) v[i] = csub_lazy(csub_lazy(v[i], q2), q);
