@@ -41,7 +41,8 @@ SERVER_PERSISTENT = 1
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_batch_words", C.c_uint64),
                 ("small_request_words", C.c_uint64), ("max_inflight", C.c_uint32),
-                ("max_batch_requests", C.c_uint32), ("flags", C.c_uint32), ("reserved", C.c_uint32)]
+                ("max_batch_requests", C.c_uint32), ("flags", C.c_uint32), ("reserved", C.c_uint32),
+                ("reserve_bytes", C.c_uint64)]
 
 
 class Request(C.Structure):
@@ -269,9 +270,9 @@ class Server:
     """The continuous-batching serving loop (axhel_server_*)."""
 
     def __init__(self, budget_bytes, max_inflight=2, max_batch_requests=256, max_batch_words=0, persistent=False,
-                 small_request_words=0):
+                 small_request_words=0, reserve_bytes=0):
         cfg = ServerConfig(budget_bytes, max_batch_words, small_request_words, max_inflight, max_batch_requests,
-                           SERVER_PERSISTENT if persistent else 0, 0)
+                           SERVER_PERSISTENT if persistent else 0, 0, reserve_bytes)
         self.h = vp()
         _scheck(lib().axhel_server_create(C.byref(cfg), C.byref(self.h)), "server_create")
         self._keep = {}

@@ -9,16 +9,23 @@
 //   chain   : inverse row pass -> fused [inverse column pass, op, forward
 //             column pass] -> forward row pass
 //
-// with A = ceil(n/2), B = n - A.  The kernel is persistent (one wave of CTAs
+// with B = min(9, n - 5) and A = n - B: the contiguous pass as wide as a tile
+// allows, which measured fastest.  The kernel is persistent (one wave of CTAs
 // sized to the device); CTAs take tiles from one atomic counter in
 // phase-major order (every phase-0 tile of every job before any phase-1
 // tile), so by the time a phase-p tile is taken, every tile it depends on is
-// already held by a running CTA.  A tile of phase p >= 1 of limb l waits for
+// already held by a running CTA.  A CTA claims its next tile while it works
+// on the current one (the counter's latency is hidden); the lowest unfinished
+// tile is then still always runnable, because everything it waits for has a
+// lower index and every CTA holding a tile is resident.  A tile of phase p >= 1 of limb l waits for
 // the phase p-1 tiles of the same limb (per-limb completion counters,
 // release/acquire at device scope); the wait is bounded and, if it ever runs
 // out, the CTA records AXHEL's timeout status in the batch's error word and
 // stops.  Data written by other CTAs of the launch is read through L2
-// (ld.global.cg), never through a possibly stale L1 line.
+// (ld.global.cg), never through a possibly stale L1 line.  A finished tile
+// is published as a grid barrier publishes arrival: CTA barrier, then one
+// thread's device-scope fence and release increment (the fence is
+// cumulative over the stores the barrier ordered before it).
 //
 // Each tile is 1024 residues handled by 128 threads x 8 registers
 // (LR = 3): 2^(10-LG) groups of 2^LG for the pass widths LG = 5..9 of the
@@ -108,19 +115,21 @@ __device__ __forceinline__ void run_tile_lg(const BatchJob& j, const PhaseCfg& c
     }
 }
 
-__global__ void __launch_bounds__(kBatchThreads) batch_kernel(const __grid_constant__ BatchArgs a)
+__global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks) batch_kernel(const __grid_constant__ BatchArgs a)
 {
     __shared__ uint64_t sm[kBatchTileWords + 128];
-    __shared__ unsigned long long s_tile;
+    __shared__ unsigned long long s_tile[2];
     __shared__ int s_abort;
-    for (;;) {
-        if (threadIdx.x == 0) {
-            s_tile = atomicAdd(a.next_tile, 1ull);
-            s_abort = 0;
-        }
-        __syncthreads();
-        const uint64_t tile = s_tile;
+    if (threadIdx.x == 0) {
+        s_tile[0] = atomicAdd(a.next_tile, 1ull);
+        s_abort = 0;
+    }
+    __syncthreads();
+    for (uint32_t it = 0;; ++it) {
+        const uint64_t tile = s_tile[it & 1];
         if (tile >= a.total_tiles) break;
+        unsigned long long nxt = 0;  // the next tile, claimed now, announced after this one
+        if (threadIdx.x == 0) nxt = atomicAdd(a.next_tile, 1ull);
         // (job, phase) of this tile: last entry with tile_begin <= tile
         uint32_t lo = 0, hi = a.nentries;
         while (hi - lo > 1) {
@@ -160,9 +169,10 @@ __global__ void __launch_bounds__(kBatchThreads) batch_kernel(const __grid_const
         case 9: run_tile_lg<9>(j, c, e.phase, limb, til, sm); break;
         default: break;
         }
-        __threadfence();  // this thread's stores, before the tile is published
+        if (threadIdx.x == 0) s_tile[(it + 1) & 1] = nxt;
         __syncthreads();
         if (threadIdx.x == 0 && e.phase + 1 < j.nphase) {
+            __threadfence();
             cuda::atomic_ref<unsigned int, cuda::thread_scope_device> done(
                 a.done[j.done_off + (uint64_t)e.phase * j.count + limb]);
             done.fetch_add(1u, cuda::memory_order_release);
@@ -172,7 +182,7 @@ __global__ void __launch_bounds__(kBatchThreads) batch_kernel(const __grid_const
 
 // One phase of a batch as an ordinary launch: CTA b runs global tile
 // first + b.  Tiles of earlier phases were finished by earlier launches.
-__global__ void __launch_bounds__(kBatchThreads) batch_phase_kernel(const __grid_constant__ BatchArgs a,
+__global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks) batch_phase_kernel(const __grid_constant__ BatchArgs a,
                                                                     uint64_t first)
 {
     __shared__ uint64_t sm[kBatchTileWords + 128];
@@ -314,8 +324,8 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
         b.src = J.operand;
         b.dst = J.result;
         b.vec = J.vector;
-        b.lg_col = (logn + 1) / 2;
-        b.lg_row = logn - b.lg_col;
+        b.lg_row = logn - 5 < 9 ? logn - 5 : 9;
+        b.lg_col = logn - b.lg_row;
         const bool inv_first = J.kind != AXHEL_JOB_FORWARD;
         b.pre = inv_first && J.input_mod_factor == 4;
         b.norm = (J.kind == AXHEL_JOB_INVERSE) ? (J.output_mod_factor != 2) : (J.output_mod_factor != 4);

@@ -17,6 +17,8 @@ constexpr int kBatchThreads = 128;
 constexpr int kBatchLR = 3;
 constexpr int kBatchTileWords = kBatchThreads << kBatchLR;  // 1024 residues
 constexpr int kBatchMinLG = 5, kBatchMaxLG = 9;
+// CTAs per SM the kernels are compiled for (96 registers; 128 without the bound)
+constexpr int kBatchMinBlocks = 5;
 
 enum BatchKind : uint32_t { kJobForward = 1, kJobInverse = 2, kJobChainMul = 3, kJobChainFma = 4 };
 

@@ -53,6 +53,7 @@ axhel_status_t sfail(axhel_status_t st, const std::string& m)
 }
 
 constexpr int kPending = -1, kRunning = -2;
+constexpr size_t kStagingBytes = 1 << 20;  // pinned descriptor staging per slot at creation
 
 bool is_device(const void* p) { return p && axhel_cuda_is_device_pointer(p); }
 
@@ -76,11 +77,10 @@ struct Req {
 struct Slot {
     int lane = 0;  // 0: small requests (high-priority stream), 1: the rest
     cudaStream_t stream = nullptr;
-    void* scratch = nullptr;
-    size_t cap = 0;
     int* err_host = nullptr;        // pinned word the kernel's error status is copied into
     unsigned char* host_img = nullptr;  // pinned staging of the batch descriptors
     size_t host_cap = 0;
+    std::vector<unsigned char*> retired;  // outgrown staging, freed with the server
     bool busy = false;
 };
 
@@ -178,30 +178,34 @@ axhel_status_t axhel_server::launch(Slot& s, int slot_index, std::vector<Req*>& 
     uint64_t phases[4] = {0, 0, 0, 0};
     axhel_status_t rc = axhel_impl::batch_build(jobs.data(), jobs.size(), nullptr, img, &zo, &zb, &args, nullptr, &err);
     if (rc) return sfail(rc, err);
-    if (img.size() > s.cap) {
-        cudaStreamSynchronize(st);  // the old buffer may still be read by this stream's last batch
-        if (s.scratch) cudaFree(s.scratch);
-        s.scratch = nullptr;
-        s.cap = 0;
-        const size_t cap = std::max<size_t>(img.size() * 2, 1 << 20);
-        if (cudaMalloc(&s.scratch, cap) != cudaSuccess) return sfail(AXHEL_ERR_NOMEM, "batch descriptor buffer");
-        s.cap = cap;
-    }
-    rc = axhel_impl::batch_build(jobs.data(), jobs.size(), static_cast<unsigned char*>(s.scratch), img, &zo, &zb,
+    // Descriptors come from the stream-ordered pool and go back to it after
+    // the batch: no cudaMalloc / cudaFree (which wait for the whole device)
+    // while other batches run.
+    void* desc = nullptr;
+    if (cudaMallocFromPoolAsync(&desc, img.size(), pool, st) != cudaSuccess)
+        return sfail(AXHEL_ERR_NOMEM, "batch descriptor buffer");
+    rc = axhel_impl::batch_build(jobs.data(), jobs.size(), static_cast<unsigned char*>(desc), img, &zo, &zb,
                                  &args, nullptr, &err, phases);
-    if (rc) return sfail(rc, err);
+    if (rc) {
+        cudaFreeAsync(desc, st);
+        return sfail(rc, err);
+    }
     if (img.size() > s.host_cap) {
-        if (s.host_img) cudaFreeHost(s.host_img);
-        s.host_img = nullptr;
-        s.host_cap = 0;
-        const size_t cap = std::max<size_t>(img.size() * 2, 1 << 20);
-        if (cudaMallocHost(reinterpret_cast<void**>(&s.host_img), cap) != cudaSuccess)
+        // The outgrown buffer is kept until the server is destroyed:
+        // cudaFreeHost would wait for every stream of the device.
+        unsigned char* grown = nullptr;
+        const size_t cap = std::max<size_t>(img.size() * 2, s.host_cap * 2);
+        if (cudaMallocHost(reinterpret_cast<void**>(&grown), cap) != cudaSuccess) {
+            cudaFreeAsync(desc, st);
             return sfail(AXHEL_ERR_NOMEM, "pinned descriptor staging");
+        }
+        if (s.host_img) s.retired.push_back(s.host_img);
+        s.host_img = grown;
         s.host_cap = cap;
     }
     // the slot's previous batch has completed, so its staging copy is done
     std::memcpy(s.host_img, img.data(), img.size());
-    cudaError_t e = cudaMemcpyAsync(s.scratch, s.host_img, img.size(), cudaMemcpyHostToDevice, st);
+    cudaError_t e = cudaMemcpyAsync(desc, s.host_img, img.size(), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
         e = (cfg.flags & AXHEL_SERVER_PERSISTENT) ? axhel_impl::batch_launch_args(args, st)
                                                    : axhel_impl::batch_launch_phases(args, phases, st);
@@ -220,6 +224,7 @@ axhel_status_t axhel_server::launch(Slot& s, int slot_index, std::vector<Req*>& 
         if (!q->out_dev && q->d_out != q->d_in) cudaFreeAsync(q->d_out, st);
         if (q->r.vector && !q->vec_dev) cudaFreeAsync(q->d_vec, st);
     }
+    cudaFreeAsync(desc, st);  // after the error word's copy, in stream order
     if (e != cudaSuccess) return sfail(AXHEL_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
     f.reqs = order;
     f.slot = slot_index;
@@ -388,11 +393,25 @@ axhel_status_t axhel_server_create(const axhel_server_config_t* cfg, axhel_serve
         const int prio = sl.lane == 0 ? prio_high : prio_low;
         if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&sl.stream, cudaStreamNonBlocking, prio);
         if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&sl.err_host), sizeof(int));
+        // descriptor staging for batches of up to a few hundred requests,
+        // allocated now rather than on a slot's first batch
+        if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&sl.host_img), kStagingBytes);
+        if (e == cudaSuccess) sl.host_cap = kStagingBytes;
+    }
+    if (e == cudaSuccess && cfg->reserve_bytes) {
+        // map the pool's memory now: growing it later takes tens of
+        // milliseconds, in the path of whichever request needs it
+        void* r = nullptr;
+        cudaStream_t st = s->slots[0].stream;
+        e = cudaMallocFromPoolAsync(&r, std::min(cfg->reserve_bytes, cfg->hbm_budget_bytes), s->pool, st);
+        if (e == cudaSuccess) e = cudaFreeAsync(r, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     }
     if (e != cudaSuccess) {
         for (Slot& sl : s->slots) {
             if (sl.stream) cudaStreamDestroy(sl.stream);
             if (sl.err_host) cudaFreeHost(sl.err_host);
+            if (sl.host_img) cudaFreeHost(sl.host_img);
         }
         if (s->pool) cudaMemPoolDestroy(s->pool);
         return sfail(AXHEL_ERR_CUDA, std::string("server setup: ") + cudaGetErrorString(e));
@@ -527,10 +546,10 @@ axhel_status_t axhel_server_destroy(axhel_server_t s)
     s->comp.join();  // drains the batches still in flight
     for (Slot& sl : s->slots) {
         cudaStreamSynchronize(sl.stream);
-        if (sl.scratch) cudaFree(sl.scratch);
         cudaStreamDestroy(sl.stream);
         cudaFreeHost(sl.err_host);
         if (sl.host_img) cudaFreeHost(sl.host_img);
+        for (unsigned char* r : sl.retired) cudaFreeHost(r);
     }
     for (cudaEvent_t ev : s->event_pool) cudaEventDestroy(ev);
     for (auto& kv : s->reqs)

@@ -262,14 +262,16 @@ def _pct(v, p):
 
 
 def serving(loads=(0.5, 0.7, 0.9), seconds=4.0, budget=60 << 30, inflight=4, seed=5, n_templates=32,
-            device=False, max_batch_words=0, persistent=False, plain=True, small_words=0):
+            device=False, max_batch_words=0, persistent=False, plain=True, small_words=0, reserve=8 << 30):
     """Isolated latency of every template (alone on an idle server), capacity
-    (a burst), then Poisson arrivals at each load fraction of capacity:
-    p50/p99 latency, p99 of each request's slowdown against its own isolated
+    (a burst), then Poisson arrivals at each load fraction of capacity
+    (host-staged requests: `reserve` bytes of the staging pool mapped up
+    front): p50/p99 latency, p99 of each request's slowdown against its own isolated
     latency, and jobs/s; then the plain sequential GPU path."""
     rp = RequestPool(n_templates=n_templates, seed=seed, device=device)
     srv = capi.Server(budget_bytes=budget, max_inflight=inflight, max_batch_requests=256,
-                      max_batch_words=max_batch_words, persistent=persistent, small_request_words=small_words)
+                      max_batch_words=max_batch_words, persistent=persistent, small_request_words=small_words,
+                      reserve_bytes=0 if device else reserve)
     rng = np.random.default_rng(seed)
 
     iso = []

@@ -211,6 +211,8 @@ typedef struct axhel_server_config {
     uint32_t max_batch_requests;  /* requests admitted into one batch */
     uint32_t flags;               /* AXHEL_SERVER_* */
     uint32_t reserved;
+    uint64_t reserve_bytes;       /* device memory mapped for staging at creation (capped at the budget; 0 = on
+                                     demand): growing the pool later stalls the request that needs it */
 } axhel_server_config_t;
 
 /* One request: a job of the batch engine (AXHEL_JOB_*).  input / output /
