@@ -24,6 +24,8 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4
 
 
 JOB_FORWARD, JOB_INVERSE, JOB_CHAIN_MUL, JOB_CHAIN_FMA = 1, 2, 3, 4
+JOB_ADD, JOB_SUB, JOB_MUL, JOB_FMA, JOB_REDUCE = 5, 6, 7, 8, 9  # element-wise jobs
+FACTOR_MODULUS = 2**64 - 1  # ReduceMod input factor equal to each limb's modulus (Barrett branch)
 
 
 class Job(C.Structure):

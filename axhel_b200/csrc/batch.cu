@@ -1,13 +1,15 @@
 // Uneven batches in one persistent launch.
 //
 // A batch mixes jobs of different degree N (2^10 .. 2^17), limb count and
-// kind: forward NTT, inverse NTT, and the fused INTT -> MulMod/FMAMod -> NTT
-// chain.  Every job runs as two or three phases of tiles:
+// kind: forward NTT, inverse NTT, the fused INTT -> MulMod/FMAMod -> NTT
+// chain, and the element-wise Add/Sub/Mul/FMA/ReduceMod.  Every job runs as
+// one to three phases of tiles:
 //
 //   forward : column pass (stages 0..A-1)  -> row pass (stages A..n-1)
 //   inverse : row pass (stages 0..B-1)     -> column pass (stages B..n-1, N^-1)
 //   chain   : inverse row pass -> fused [inverse column pass, op, forward
 //             column pass] -> forward row pass
+//   element-wise : one phase, the op on 1024 residues of one limb per tile
 //
 // with B = min(9, n - 5) and A = n - B: the contiguous pass as wide as a tile
 // allows, which measured fastest.  The kernel is persistent (one wave of CTAs
@@ -46,6 +48,7 @@
 #include "internal.h"
 #include "launch.h"
 #include "batch.h"
+#include "eltwise_ops.cuh"
 #include "ntt_kernels.cuh"
 
 namespace axhel_impl {
@@ -115,6 +118,87 @@ __device__ __forceinline__ void run_tile_lg(const BatchJob& j, const PhaseCfg& c
     }
 }
 
+// Element-wise job tile: 1024 residues of one limb, 8 per thread at a
+// stride of the CTA width (every warp access is 256 contiguous bytes); all
+// loads are issued before the first store.
+template <bool HAS_B, class Op>
+__device__ __forceinline__ void elt_tile(const BatchJob& j, uint64_t base, const Op& op)
+{
+    constexpr int kPer = kBatchTileWords / kBatchThreads;
+    uint64_t a[kPer], b[kPer];
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        a[k] = j.src[base + (uint64_t)k * kBatchThreads];
+        b[k] = HAS_B ? j.vec[base + (uint64_t)k * kBatchThreads] : 0;
+    }
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) j.dst[base + (uint64_t)k * kBatchThreads] = op(a[k], b[k]);
+}
+
+template <bool ADD>
+__device__ __forceinline__ void elt_fma(const BatchJob& j, uint64_t base, uint64_t q, uint64_t mu, uint64_t s,
+                                        uint32_t sh)
+{
+    switch (j.ef) {
+    case 1: elt_tile<ADD>(j, base, OpFma<1, ADD>{q, mu, s, sh}); break;
+    case 2: elt_tile<ADD>(j, base, OpFma<2, ADD>{q, mu, s, sh}); break;
+    case 4: elt_tile<ADD>(j, base, OpFma<4, ADD>{q, mu, s, sh}); break;
+    default: elt_tile<ADD>(j, base, OpFma<8, ADD>{q, mu, s, sh}); break;
+    }
+}
+
+// The element-wise job's op on one tile, with limb `limb`'s modulus.
+__device__ __forceinline__ void run_elt_tile(const BatchJob& j, uint64_t limb, uint64_t til)
+{
+    const uint32_t mi = (uint32_t)(limb % j.nmods);
+    const ModCtx* cx = j.ctx[mi];
+    const uint64_t q = cx->q, mu = cx->mu;
+    const uint32_t sh = cx->shift;
+    const uint64_t s = j.scalars ? j.scalars[mi] : 0;
+    const uint64_t base = (limb << j.logn) + til * kBatchTileWords + threadIdx.x;
+    switch (j.eop) {
+    case kEltAddVV: elt_tile<true>(j, base, OpAddVV{q}); break;
+    case kEltAddVS: elt_tile<false>(j, base, OpAddVS{q, s}); break;
+    case kEltSubVV: elt_tile<true>(j, base, OpSubVV{q}); break;
+    case kEltSubVS: elt_tile<false>(j, base, OpSubVS{q, s}); break;
+    case kEltMul:
+        if (j.ef == 1) elt_tile<true>(j, base, OpMul<1>{q, mu, sh});
+        else if (j.ef == 2) elt_tile<true>(j, base, OpMul<2>{q, mu, sh});
+        else elt_tile<true>(j, base, OpMul<4>{q, mu, sh});
+        break;
+    case kEltFma: elt_fma<false>(j, base, q, mu, s, sh); break;
+    case kEltFmaAdd: elt_fma<true>(j, base, q, mu, s, sh); break;
+    default:  // kEltReduce
+        switch (j.ef) {
+        case 0: elt_tile<false>(j, base, OpReduce<0>{q, mu, sh}); break;
+        case 1: elt_tile<false>(j, base, OpReduce<1>{q, mu, sh}); break;
+        case 2: elt_tile<false>(j, base, OpReduce<2>{q, mu, sh}); break;
+        case 3: elt_tile<false>(j, base, OpReduce<3>{q, mu, sh}); break;
+        default: elt_tile<false>(j, base, OpReduce<4>{q, mu, sh}); break;
+        }
+        break;
+    }
+}
+
+// One tile of any job kind.
+__device__ __forceinline__ void run_tile(const BatchJob& j, uint32_t phase, uint64_t limb, uint64_t til,
+                                         uint64_t* sm)
+{
+    if (j.kind >= kJobAdd) {
+        run_elt_tile(j, limb, til);
+        return;
+    }
+    const PhaseCfg c = phase_cfg(j, phase);
+    switch (c.lg) {
+    case 5: run_tile_lg<5>(j, c, phase, limb, til, sm); break;
+    case 6: run_tile_lg<6>(j, c, phase, limb, til, sm); break;
+    case 7: run_tile_lg<7>(j, c, phase, limb, til, sm); break;
+    case 8: run_tile_lg<8>(j, c, phase, limb, til, sm); break;
+    case 9: run_tile_lg<9>(j, c, phase, limb, til, sm); break;
+    default: break;
+    }
+}
+
 __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks) batch_kernel(const __grid_constant__ BatchArgs a)
 {
     __shared__ uint64_t sm[kBatchTileWords + 128];
@@ -160,15 +244,7 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks) batch_kernel(c
         }
         __syncthreads();
         if (s_abort) break;
-        const PhaseCfg c = phase_cfg(j, e.phase);
-        switch (c.lg) {
-        case 5: run_tile_lg<5>(j, c, e.phase, limb, til, sm); break;
-        case 6: run_tile_lg<6>(j, c, e.phase, limb, til, sm); break;
-        case 7: run_tile_lg<7>(j, c, e.phase, limb, til, sm); break;
-        case 8: run_tile_lg<8>(j, c, e.phase, limb, til, sm); break;
-        case 9: run_tile_lg<9>(j, c, e.phase, limb, til, sm); break;
-        default: break;
-        }
+        run_tile(j, e.phase, limb, til, sm);
         if (threadIdx.x == 0) s_tile[(it + 1) & 1] = nxt;
         __syncthreads();
         if (threadIdx.x == 0 && e.phase + 1 < j.nphase) {
@@ -198,15 +274,7 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks) batch_phase_ke
     const uint32_t tpl = j.tiles_per_limb[e.phase];
     const uint64_t limb = lt / tpl;
     const uint64_t til = lt - limb * tpl;
-    const PhaseCfg c = phase_cfg(j, e.phase);
-    switch (c.lg) {
-    case 5: run_tile_lg<5>(j, c, e.phase, limb, til, sm); break;
-    case 6: run_tile_lg<6>(j, c, e.phase, limb, til, sm); break;
-    case 7: run_tile_lg<7>(j, c, e.phase, limb, til, sm); break;
-    case 8: run_tile_lg<8>(j, c, e.phase, limb, til, sm); break;
-    case 9: run_tile_lg<9>(j, c, e.phase, limb, til, sm); break;
-    default: break;
-    }
+    run_tile(j, e.phase, limb, til, sm);
 }
 
 }  // namespace axhel_impl
@@ -259,7 +327,105 @@ int batch_grid()
 
 }  // namespace
 
+namespace {
+
+// Branch of EltwiseReduceModNative (eltwise-reduce-mod.cpp:35-127) taken for
+// (in_f, out_f): 0 copy, 1 [0,2q)->[0,q), 2 [0,4q)->[0,q), 3 [0,4q)->[0,2q),
+// 4 Barrett (in_f equal to the modulus); -1 for a pair that does nothing.
+int reduce_branch(uint64_t in_f, uint64_t out_f)
+{
+    if (in_f == AXHEL_FACTOR_MODULUS) return 4;
+    if (in_f == 1 || (out_f == 2 && in_f <= 2)) return 0;
+    if (in_f == 2 && out_f == 1) return 1;
+    if (in_f == 4 && out_f == 1) return 2;
+    if (in_f == 4 && out_f == 2) return 3;
+    return -1;
+}
+
+}  // namespace
+
 namespace axhel_impl {
+
+axhel_status_t batch_check_job(const axhel_job_t& J, const std::string& who, std::string* err)
+{
+    const std::string job = who + ": ";
+    if (J.kind < AXHEL_JOB_FORWARD || J.kind > AXHEL_JOB_REDUCE) {
+        *err = job + "unknown kind";
+        return AXHEL_ERR_INVALID;
+    }
+    if (!J.ntts || J.n_ntts == 0 || J.n_ntts > 1024) {
+        *err = job + "1..1024 NTT handles needed";
+        return AXHEL_ERR_INVALID;
+    }
+    const uint64_t n = J.ntts[0] ? J.ntts[0]->n : 0;
+    for (uint32_t m = 0; m < J.n_ntts; ++m) {
+        if (!J.ntts[m] || J.ntts[m]->n != n) {
+            *err = job + "handles must share one degree";
+            return AXHEL_ERR_INVALID;
+        }
+    }
+    const uint32_t logn = J.ntts[0]->logn;
+    if (logn < 10 || logn > 17) {
+        *err = job + "batched degree must be in [2^10, 2^17]";
+        return AXHEL_ERR_UNSUPPORTED;
+    }
+    if (J.count && (!J.result || !J.operand)) {
+        *err = job + "null data pointer";
+        return AXHEL_ERR_INVALID;
+    }
+    const uint64_t f = J.input_mod_factor;
+    switch (J.kind) {
+    case AXHEL_JOB_CHAIN_MUL:
+        if (J.count && !J.vector) {
+            *err = job + "chain multiplicand missing";
+            return AXHEL_ERR_INVALID;
+        }
+        break;
+    case AXHEL_JOB_CHAIN_FMA:
+        if (!J.scalars) {
+            *err = job + "chain scalars missing";
+            return AXHEL_ERR_INVALID;
+        }
+        break;
+    case AXHEL_JOB_ADD:
+    case AXHEL_JOB_SUB:
+        if (!J.vector && !J.scalars) {
+            *err = job + "a vector or per-modulus scalars needed";
+            return AXHEL_ERR_INVALID;
+        }
+        break;
+    case AXHEL_JOB_MUL:
+        if (J.count && !J.vector) {
+            *err = job + "multiplicand missing";
+            return AXHEL_ERR_INVALID;
+        }
+        if (f != 1 && f != 2 && f != 4) {
+            *err = job + "MulMod input factor must be 1, 2 or 4";
+            return AXHEL_ERR_INVALID;
+        }
+        break;
+    case AXHEL_JOB_FMA:
+        if (!J.scalars) {
+            *err = job + "FMAMod scalars missing";
+            return AXHEL_ERR_INVALID;
+        }
+        if (f != 1 && f != 2 && f != 4 && f != 8) {
+            *err = job + "FMAMod input factor must be 1, 2, 4 or 8";
+            return AXHEL_ERR_INVALID;
+        }
+        break;
+    case AXHEL_JOB_REDUCE:
+        if (reduce_branch(f, J.output_mod_factor) < 0) {
+            *err = job + "ReduceMod factor pair (" + std::to_string(f) + ", " + std::to_string(J.output_mod_factor) +
+                   ") is not one the reference reduces";
+            return AXHEL_ERR_INVALID;
+        }
+        break;
+    default:
+        break;
+    }
+    return AXHEL_OK;
+}
 
 // Host layout of a batch: fills `host` (to be copied to the device at `base`)
 // and the kernel arguments.  Shared by the allocating and the static-scratch
@@ -280,43 +446,13 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
         const axhel_job_t& J = jobs[i];
         BatchJob& b = bj[i];
         std::memset(&b, 0, sizeof b);
-        if (J.kind < AXHEL_JOB_FORWARD || J.kind > AXHEL_JOB_CHAIN_FMA) {
-            *err = "job " + std::to_string(i) + ": unknown kind";
-            return AXHEL_ERR_INVALID;
-        }
-        if (!J.ntts || J.n_ntts == 0 || J.n_ntts > 1024) {
-            *err = "job " + std::to_string(i) + ": 1..1024 NTT handles needed";
-            return AXHEL_ERR_INVALID;
-        }
-        const uint64_t n = J.ntts[0] ? J.ntts[0]->n : 0;
+        const axhel_status_t st = batch_check_job(J, "job " + std::to_string(i), err);
+        if (st) return st;
         for (uint32_t m = 0; m < J.n_ntts; ++m) {
-            if (!J.ntts[m] || J.ntts[m]->n != n) {
-                *err = "job " + std::to_string(i) + ": handles must share one degree";
-                return AXHEL_ERR_INVALID;
-            }
             ctxs[i].push_back(J.ntts[m]->dctx);
             if (held) held->push_back(J.ntts[m]);
         }
         const uint32_t logn = J.ntts[0]->logn;
-        if (logn < 10 || logn > 17) {
-            *err = "job " + std::to_string(i) + ": batched degree must be in [2^10, 2^17]";
-            return AXHEL_ERR_UNSUPPORTED;
-        }
-        if (J.count && (!J.result || !J.operand)) {
-            *err = "job " + std::to_string(i) + ": null data pointer";
-            return AXHEL_ERR_INVALID;
-        }
-        if (J.kind == AXHEL_JOB_CHAIN_MUL && J.count && !J.vector) {
-            *err = "job " + std::to_string(i) + ": chain multiplicand missing";
-            return AXHEL_ERR_INVALID;
-        }
-        if (J.kind == AXHEL_JOB_CHAIN_FMA) {
-            if (!J.scalars) {
-                *err = "job " + std::to_string(i) + ": chain scalars missing";
-                return AXHEL_ERR_INVALID;
-            }
-            scal[i].assign(J.scalars, J.scalars + J.n_ntts);
-        }
         b.kind = J.kind;
         b.logn = logn;
         b.count = J.count;
@@ -324,6 +460,38 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
         b.src = J.operand;
         b.dst = J.result;
         b.vec = J.vector;
+        if (J.kind >= AXHEL_JOB_ADD) {
+            // element-wise: one phase of 1024-residue tiles, no dependencies
+            const uint64_t f = J.input_mod_factor;
+            b.nphase = 1;
+            b.tiles_per_limb[0] = (uint32_t)((1ull << logn) / kBatchTileWords);
+            if (J.kind == AXHEL_JOB_ADD || J.kind == AXHEL_JOB_SUB) {
+                const bool vv = J.vector != nullptr;
+                b.eop = J.kind == AXHEL_JOB_ADD ? (vv ? kEltAddVV : kEltAddVS) : (vv ? kEltSubVV : kEltSubVS);
+                if (!vv) scal[i].assign(J.scalars, J.scalars + J.n_ntts);
+            } else if (J.kind == AXHEL_JOB_MUL) {
+                b.eop = kEltMul;
+                b.ef = (uint32_t)f;
+            } else if (J.kind == AXHEL_JOB_FMA) {
+                b.eop = J.vector ? kEltFmaAdd : kEltFma;
+                b.ef = (uint32_t)f;
+                // the scalar enters reduced by ReduceInput<F> (eltwise-fma-mod.cpp:33)
+                for (uint32_t m = 0; m < J.n_ntts; ++m) {
+                    uint64_t v = J.scalars[m];
+                    const uint64_t q = J.ntts[m]->q;
+                    if (f == 8 && v >= 4 * q) v -= 4 * q;
+                    if (f >= 4 && v >= 2 * q) v -= 2 * q;
+                    if (f >= 2 && v >= q) v -= q;
+                    scal[i].push_back(v);
+                }
+            } else {
+                b.eop = kEltReduce;
+                b.ef = reduce_branch(f, J.output_mod_factor);
+            }
+            b.done_off = done_total;
+            continue;
+        }
+        if (J.kind == AXHEL_JOB_CHAIN_FMA) scal[i].assign(J.scalars, J.scalars + J.n_ntts);
         b.lg_row = logn - 5 < 9 ? logn - 5 : 9;
         b.lg_col = logn - b.lg_row;
         const bool inv_first = J.kind != AXHEL_JOB_FORWARD;

@@ -20,7 +20,15 @@ constexpr int kBatchMinLG = 5, kBatchMaxLG = 9;
 // CTAs per SM the kernels are compiled for (96 registers; 128 without the bound)
 constexpr int kBatchMinBlocks = 5;
 
-enum BatchKind : uint32_t { kJobForward = 1, kJobInverse = 2, kJobChainMul = 3, kJobChainFma = 4 };
+enum BatchKind : uint32_t {
+    kJobForward = 1, kJobInverse = 2, kJobChainMul = 3, kJobChainFma = 4,
+    kJobAdd = 5, kJobSub = 6, kJobMul = 7, kJobFma = 8, kJobReduce = 9  // element-wise, one phase
+};
+
+// Element-wise operation of an element-wise job, resolved on the host.
+enum EltOp : uint32_t {
+    kEltAddVV, kEltAddVS, kEltSubVV, kEltSubVS, kEltMul, kEltFma, kEltFmaAdd, kEltReduce
+};
 
 struct BatchJob {
     const uint64_t* src;
@@ -35,7 +43,7 @@ struct BatchJob {
     uint32_t tiles_per_limb[3];
     uint32_t pre, norm;               // fuse ReduceMod(4,2) on load / normalize the output
     uint32_t wait_extra;              // added to every dependency target (0; a test sets 1 to force a timeout)
-    uint32_t pad;
+    uint32_t eop, ef;                 // element-wise jobs: EltOp, and its factor (ReduceMod: branch 0..4)
 };
 
 struct BatchEntry {
@@ -53,6 +61,10 @@ struct BatchArgs {
     int* error;                         // AXHEL_OK or AXHEL_ERR_TIMEOUT
     uint64_t wait_ns;                   // a dependency wait gives up after this long
 };
+
+// Checks one job against the batch engine's contract (kinds, degrees,
+// pointers, factors); `who` names it in the message.
+axhel_status_t batch_check_job(const axhel_job_t& job, const std::string& who, std::string* err);
 
 // Lays out the device image of a batch for the device address `base`:
 // fills `host` (to be copied to `base`), the range of counters that must be

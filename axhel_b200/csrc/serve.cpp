@@ -426,11 +426,17 @@ axhel_status_t axhel_server_create(const axhel_server_config_t* cfg, axhel_serve
 axhel_status_t axhel_server_submit(axhel_server_t s, const axhel_request_t* r, uint64_t* id)
 {
     if (!s || !r || !id) return sfail(AXHEL_ERR_INVALID, "null argument");
-    if (r->kind < AXHEL_JOB_FORWARD || r->kind > AXHEL_JOB_CHAIN_FMA) return sfail(AXHEL_ERR_INVALID, "kind");
     if (!r->ntts || r->n_ntts == 0 || !r->input || !r->output || r->count == 0)
         return sfail(AXHEL_ERR_INVALID, "request needs handles, input, output and count > 0");
-    if (r->kind == AXHEL_JOB_CHAIN_MUL && !r->vector) return sfail(AXHEL_ERR_INVALID, "chain multiplicand missing");
-    if (r->kind == AXHEL_JOB_CHAIN_FMA && !r->scalars) return sfail(AXHEL_ERR_INVALID, "chain scalars missing");
+    {
+        // the batch engine's contract, checked now so that a bad request
+        // fails alone rather than the batch it would join
+        const axhel_job_t j{r->kind,  r->n_ntts, r->ntts,    r->count,           r->output,
+                            r->input, r->vector, r->scalars, r->input_mod_factor, r->output_mod_factor};
+        std::string err;
+        const axhel_status_t st = axhel_impl::batch_check_job(j, "request", &err);
+        if (st) return sfail(st, err);
+    }
     auto q = std::make_unique<Req>();
     q->r = *r;
     const uint64_t n = r->ntts[0] ? axhel_cuda_ntt_degree(r->ntts[0]) : 0;

@@ -139,11 +139,28 @@ axhel_status_t axhel_cuda_ntt_chain_fma_batch(const axhel_ntt_t* ntts, uint64_t 
 #define AXHEL_JOB_INVERSE 2u   /* ComputeInverse; in_f == 4 fuses ReduceMod(4,2) on load */
 #define AXHEL_JOB_CHAIN_MUL 3u /* ComputeInverse(in_f,2) -> MulMod(., vector, 2) -> ComputeForward(1,out_f) */
 #define AXHEL_JOB_CHAIN_FMA 4u /* ComputeInverse(in_f,2) -> FMAMod(., scalars[m], vector|NULL, 2) -> ComputeForward */
+/* Element-wise jobs: the reference's eltwise call on every limb, limb i with
+ * the modulus of ntts[i % n_ntts].  Replace the per-limb loops over
+ * EltwiseAddMod / EltwiseSubMod (eltwise-add-mod.hpp:13,17,
+ * eltwise-sub-mod.hpp:13,17), EltwiseMulMod (eltwise-mul-mod.hpp:14),
+ * EltwiseFMAMod (eltwise-fma-mod.hpp:15) and EltwiseReduceMod
+ * (eltwise-reduce-mod.hpp:14). */
+#define AXHEL_JOB_ADD 5u    /* AddMod(result, operand, vector) or, vector NULL, (operand, scalars[m]) */
+#define AXHEL_JOB_SUB 6u    /* SubMod, operands as ADD */
+#define AXHEL_JOB_MUL 7u    /* MulMod(result, operand, vector, in_f), in_f in {1, 2, 4} */
+#define AXHEL_JOB_FMA 8u    /* FMAMod(result, operand, scalars[m], vector | NULL, in_f), in_f in {1, 2, 4, 8} */
+#define AXHEL_JOB_REDUCE 9u /* ReduceMod(result, operand, in_f, out_f): the reference's matched pairs */
+/* REDUCE input factor meaning "equal to each limb's modulus": the reference's
+ * Barrett branch (EltwiseReduceMod with in_f == q) for inputs of any value. */
+#define AXHEL_FACTOR_MODULUS 0xFFFFFFFFFFFFFFFFull
 
 /* One job of a batch: `count` limbs of one degree N (2^10 <= N <= 2^17)
  * stored back to back, limb i using ntts[i % n_ntts]; result/operand/vector
  * are DEVICE pointers (result may equal operand), scalars a HOST array of
- * n_ntts values (chain FMA only). */
+ * n_ntts values (chain FMA, FMA, and ADD/SUB without a vector).  Factors the
+ * reference would silently ignore (a MulMod factor of 3, an unmatched
+ * ReduceMod pair) are refused with AXHEL_ERR_INVALID when the batch is
+ * built. */
 typedef struct axhel_job {
     uint32_t kind;
     uint32_t n_ntts;

@@ -115,3 +115,55 @@ def ptr(t, offset_words=0):
 def ntt_params(oracle, n, bits):
     q = oracle.find_ntt_prime(n, bits)
     return q, oracle.find_primitive_root(n, q)
+
+
+# Element-wise batch jobs: (kind, has_vector, in_f, out_f); in_f "q" is the
+# ReduceMod Barrett branch (input factor equal to the modulus).
+ELT_CASES = [
+    (5, True, 1, 1), (5, False, 1, 1), (6, True, 1, 1), (6, False, 1, 1),
+    (7, True, 1, 1), (7, True, 2, 1), (7, True, 4, 1),
+    (8, False, 1, 1), (8, True, 2, 1), (8, True, 4, 1), (8, False, 8, 1), (8, True, 8, 1),
+    (9, False, 1, 1), (9, False, 2, 2), (9, False, 2, 1), (9, False, 4, 1), (9, False, 4, 2), (9, False, "q", 1),
+]
+
+
+def eltwise_job_data(oracle, st, kind, has_vec, in_f, mods, n, count):
+    """Operands of an element-wise job, drawn in the reference's input ranges:
+    [0, q) for Add/Sub, [0, F*q) for Mul/FMA, [0, in_f*q) or any 64-bit value
+    (Barrett branch) for ReduceMod."""
+    L = len(mods)
+    qs = [mods[i % L][0] for i in range(count)]
+    if kind in (5, 6):
+        bound = lambda q: q
+    elif kind == 9 and in_f == "q":
+        bound = lambda q: 2**64 - 1
+    else:
+        bound = lambda q: in_f * q
+    x = np.concatenate([oracle.random_vector(st, n, bound(q)) for q in qs])
+    vec = np.concatenate([oracle.random_vector(st, n, bound(q)) for q in qs]) if has_vec else None
+    sc = None
+    if kind in (5, 6) and not has_vec:
+        sc = [oracle.bounded(st, q) for q, _ in mods]
+    elif kind == 8:
+        sc = [oracle.bounded(st, in_f * q) for q, _ in mods]
+    return x, vec, sc
+
+
+def eltwise_expected(oracle, kind, has_vec, in_f, out_f, mods, n, count, x, vec, sc):
+    """The reference's per-limb eltwise call on every limb (oracle)."""
+    L, out = len(mods), []
+    for i in range(count):
+        q = mods[i % L][0]
+        s = slice(i * n, (i + 1) * n)
+        a, b = x[s], (vec[s] if has_vec else None)
+        if kind == 5:
+            out.append(oracle.add(a, b if has_vec else sc[i % L], q))
+        elif kind == 6:
+            out.append(oracle.sub(a, b if has_vec else sc[i % L], q))
+        elif kind == 7:
+            out.append(oracle.mul(a, b, q, in_f))
+        elif kind == 8:
+            out.append(oracle.fma(a, sc[i % L], b, q, in_f))
+        else:
+            out.append(oracle.reduce(a, q, q if in_f == "q" else in_f, out_f))
+    return np.concatenate(out)

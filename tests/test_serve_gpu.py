@@ -138,3 +138,75 @@ def test_rejection_cancel_and_bounded_wait(cuda, oracle):
         assert st == 0
         np.testing.assert_array_equal(result(bufs, r["x"].size, False), expected(oracle, r))
     srv.close()
+
+
+def test_eltwise_requests_alone_and_in_a_mix(cuda, oracle):
+    """Element-wise requests (Add/Sub/Mul/FMA/ReduceMod over all limbs) are
+    admitted beside transform chains: each result equals the reference's
+    per-limb calls alone, and is the same in a concurrent mix."""
+    from helpers import eltwise_expected, eltwise_job_data
+
+    rng = np.random.default_rng(12)
+    cases = [(5, True, 1, 1), (6, False, 1, 1), (7, True, 2, 1), (8, True, 4, 1), (8, False, 8, 1),
+             (9, False, 4, 1), (9, False, "q", 1)]
+    ereqs = []
+    for c, (kind, has_vec, in_f, out_f) in enumerate(cases):
+        n, L, count = 1 << (13 + c % 3), 3, 4
+        mods = []
+        for i in range(L):
+            q = oracle.find_ntt_prime_near(n, int(rng.integers(40, 60)), int(rng.integers(1, 4)), 4)
+            mods.append((q, oracle.find_primitive_root(n, q)))
+        x, vec, sc = eltwise_job_data(oracle, oracle.rng(SEED ^ (4242 + c)), kind, has_vec, in_f, mods, n, count)
+        ereqs.append(dict(kind=kind, has_vec=has_vec, in_f=in_f, out_f=out_f, mods=mods, n=n, count=count, x=x,
+                          vec=vec, sc=sc, ntts=[cuda.NTT(n, q, psi) for q, psi in mods]))
+    chains = make_requests(cuda, oracle, 9, SPECS[:4])
+
+    def esubmit(srv, r, on_device):
+        if on_device:
+            bi, bo = dev(r["x"]), dev_empty(r["x"].size)
+            bv = dev(r["vec"]) if r["has_vec"] else None
+            pi, po, pv = ptr(bi), ptr(bo), ptr(bv) if bv is not None else 0
+        else:
+            bi, bo = pinned(r["x"]), pinned(np.zeros(r["x"].size, np.uint64))
+            bv = pinned(r["vec"]) if r["has_vec"] else None
+            pi, po, pv = bi.data_ptr(), bo.data_ptr(), bv.data_ptr() if bv is not None else 0
+        in_f = cuda.FACTOR_MODULUS if r["in_f"] == "q" else r["in_f"]
+        rid = srv.submit(r["kind"], r["ntts"], r["count"], pi, po, vector=pv, scalars=r["sc"], in_f=in_f,
+                         out_f=r["out_f"])
+        return rid, (bi, bo, bv)
+
+    srv = cuda.Server(budget_bytes=8 << 30, max_inflight=2, max_batch_requests=64)
+    alone = []
+    for k, r in enumerate(ereqs):
+        rid, bufs = esubmit(srv, r, on_device=k % 2 == 1)
+        st, info = srv.wait(rid)
+        assert st == 0 and info.batch_size == 1
+        alone.append(result(bufs, r["x"].size, k % 2 == 1))
+        np.testing.assert_array_equal(
+            alone[-1], eltwise_expected(oracle, r["kind"], r["has_vec"], r["in_f"], r["out_f"], r["mods"], r["n"],
+                                        r["count"], r["x"], r["vec"], r["sc"]), err_msg=f"request {cases[k]}")
+    chain_alone = [expected(oracle, r) for r in chains]
+    handles = []
+    srv.pause(True)
+    for k, r in enumerate(ereqs):
+        rid, bufs = esubmit(srv, r, on_device=k % 2 == 0)
+        handles.append(("e", k, rid, bufs, k % 2 == 0))
+    for k, r in enumerate(chains):
+        rid, bufs = submit(srv, r, on_device=k % 2 == 1)
+        handles.append(("c", k, rid, bufs, k % 2 == 1))
+    srv.pause(False)
+    sizes = []
+    for what, k, rid, bufs, on_dev in handles:
+        st, info = srv.wait(rid)
+        assert st == 0
+        sizes.append(info.batch_size)
+        if what == "e":
+            np.testing.assert_array_equal(result(bufs, ereqs[k]["x"].size, on_dev), alone[k], err_msg=f"mix {k}")
+        else:
+            np.testing.assert_array_equal(result(bufs, chains[k]["x"].size, on_dev), chain_alone[k])
+    assert max(sizes) > 1
+    with pytest.raises(cuda.AxhelError):  # refused at submit, alone: MulMod factor 3
+        r = ereqs[2]
+        d = dev(r["x"])
+        srv.submit(7, r["ntts"], r["count"], ptr(d), ptr(d), vector=ptr(d), in_f=3, out_f=1)
+    srv.close()
