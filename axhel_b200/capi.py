@@ -105,6 +105,7 @@ def _declare(L):
     d("axhel_last_error", C.c_char_p)
     d("axhel_version", C.c_int)
     d("axhel_cuda_ntt_create", st_t, u64, u64, u64, C.POINTER(vp))
+    d("axhel_cuda_ntt_create_many", st_t, u64, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64), C.POINTER(vp))
     d("axhel_cuda_ntt_create_external", st_t, u64, u64, vp, vp, vp, C.POINTER(vp))
     d("axhel_cuda_ntt_retain", st_t, vp)
     d("axhel_cuda_ntt_release", st_t, vp)
@@ -358,9 +359,11 @@ def _arr64(values):
 class NTT:
     """A device-resident (N, q) table context (``axhel_ntt_t``)."""
 
-    def __init__(self, degree, modulus, root=None, tables=None):
+    def __init__(self, degree, modulus, root=None, tables=None, handle=None):
         h = vp()
-        if tables is None:
+        if handle is not None:
+            h = handle
+        elif tables is None:
             check(lib().axhel_cuda_ntt_create(degree, modulus, root, C.byref(h)), "ntt_create")
         else:
             import numpy as np
@@ -371,6 +374,17 @@ class NTT:
         self.h = h
         self.degree = degree
         self.modulus = modulus
+
+    @staticmethod
+    def create_many(params):
+        """NTT objects for a list of (degree, modulus, root), the missing
+        tables generated on the device in one launch
+        (axhel_cuda_ntt_create_many)."""
+        k = len(params)
+        arr = lambda col: (u64 * max(k, 1))(*[int(p[col]) for p in params])
+        hs = (vp * max(k, 1))()
+        check(lib().axhel_cuda_ntt_create_many(k, arr(0), arr(1), arr(2), hs), "ntt_create_many")
+        return [NTT(d, q, handle=vp(hs[i])) for i, (d, q, _) in enumerate(params)]
 
     def close(self):
         if self.h:

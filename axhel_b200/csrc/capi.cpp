@@ -13,6 +13,7 @@
 
 #include "../../include/axhel_cuda.h"
 #include "internal.h"
+#include "tables.h"
 #include "launch.h"
 
 using namespace axhel_impl;
@@ -84,38 +85,29 @@ std::map<std::tuple<int, uint64_t, uint64_t, uint64_t>, axhel_ntt_ctx*> g_cache;
 
 constexpr size_t kHeader = kCtxHeaderBytes;
 
-// Builds the forward / inverse tables exactly as GenerateNTTTables
-// (axhel/ntt/ntt-tables.cpp:81-140): fwd[i] = psi^bitrev(i); inv[0] = 0,
-// inv[i] = psi^-(bitrev(i-1)+1); each with its Shoup quotient.
-void generate_tables(uint64_t n, uint32_t logn, uint64_t q, uint64_t psi, uint64_t* fwd, uint64_t* inv,
-                     uint64_t* ninv)
+// The context header (ModCtx) for tables at `base`: N^-1 with its quotient,
+// and the scaled root of the final inverse stage computed from the last
+// inverse twiddle exactly as ntt-native.cpp:101-113.
+ModCtx make_header(const axhel_ntt_ctx* c, unsigned char* base, uint64_t inv_last, uint64_t ninv, uint64_t ninv_q)
 {
-    std::vector<uint64_t> pw(n);
-    auto bitrev = [logn](uint64_t i) {
-        uint64_t r = 0;
-        for (uint32_t b = 0; b < logn; ++b) r |= ((i >> b) & 1) << (logn - 1 - b);
-        return r;
-    };
-    pw[0] = 1;
-    for (uint64_t i = 1; i < n; ++i) pw[i] = mulmod(pw[i - 1], psi, q);
-    for (uint64_t i = 0; i < n; ++i) {
-        const uint64_t w = pw[bitrev(i)];
-        fwd[2 * i] = w;
-        fwd[2 * i + 1] = shoup_quotient(w, q);
-    }
-    const uint64_t psi_inv = powmod(psi, q - 2, q);
-    for (uint64_t i = 1; i < n; ++i) pw[i] = mulmod(pw[i - 1], psi_inv, q);
-    inv[0] = inv[1] = 0;
-    for (uint64_t i = 1; i < n; ++i) {
-        const uint64_t w = pw[bitrev(i - 1) + 1];
-        inv[2 * i] = w;
-        inv[2 * i + 1] = shoup_quotient(w, q);
-    }
-    const uint64_t d = powmod(n % q, q - 2, q);
-    ninv[0] = d;
-    ninv[1] = shoup_quotient(d, q);
+    ModCtx h{};
+    h.q = c->q;
+    h.q2 = c->q << 1;
+    h.ninv = ninv;
+    h.ninv_q = ninv_q;
+    uint64_t sr = shoup_lazy(inv_last, ninv, ninv_q, c->q);
+    if (sr >= c->q) sr -= c->q;
+    h.sroot = sr;
+    h.sroot_q = shoup_quotient(sr, c->q);
+    barrett_params(c->q, &h.mu, &h.shift);
+    h.logn = c->logn;
+    h.fwd = reinterpret_cast<const ulonglong2*>(base + kHeader);
+    h.inv = reinterpret_cast<const ulonglong2*>(base + kHeader + c->n * 16);
+    return h;
 }
 
+// Caller-provided tables (the external-table constructor, ntt.cpp:124-133):
+// copied into one device allocation behind their header.
 axhel_status_t upload(axhel_ntt_ctx* c, const uint64_t* fwd, const uint64_t* inv, const uint64_t* ninv)
 {
     const size_t tab = c->n * 16;
@@ -124,20 +116,7 @@ axhel_status_t upload(axhel_ntt_ctx* c, const uint64_t* fwd, const uint64_t* inv
     cudaError_t e = cudaMalloc(&c->mem, total);
     if (e != cudaSuccess) return fail(AXHEL_ERR_NOMEM, std::string("cudaMalloc(tables): ") + cudaGetErrorString(e));
     unsigned char* base = static_cast<unsigned char*>(c->mem);
-    ModCtx h{};
-    h.q = c->q;
-    h.q2 = c->q << 1;
-    h.ninv = ninv[0];
-    h.ninv_q = ninv[1];
-    // scaled root of the final inverse stage (ntt-native.cpp:101-113)
-    uint64_t sr = shoup_lazy(inv[2 * (c->n - 1)], ninv[0], ninv[1], c->q);
-    if (sr >= c->q) sr -= c->q;
-    h.sroot = sr;
-    h.sroot_q = shoup_quotient(sr, c->q);
-    barrett_params(c->q, &h.mu, &h.shift);
-    h.logn = c->logn;
-    h.fwd = reinterpret_cast<const ulonglong2*>(base + kHeader);
-    h.inv = reinterpret_cast<const ulonglong2*>(base + kHeader + tab);
+    const ModCtx h = make_header(c, base, inv[2 * (c->n - 1)], ninv[0], ninv[1]);
     std::memcpy(img.data(), &h, sizeof h);
     std::memcpy(img.data() + kHeader, fwd, tab);
     std::memcpy(img.data() + kHeader + tab, inv, tab);
@@ -149,6 +128,33 @@ axhel_status_t upload(axhel_ntt_ctx* c, const uint64_t* fwd, const uint64_t* inv
     }
     c->dctx = reinterpret_cast<const ModCtx*>(base);
     return AXHEL_OK;
+}
+
+// Header and Montgomery constants for generating the tables of (N, q, psi)
+// on the device (tables.cu) into c->mem.  GenerateNTTTables'
+// host-side scalars (ntt-tables.cpp:109, 132-136): psi^-1 = psi^(q-2),
+// N^-1 = (N mod q)^(q-2).
+void gen_job(const axhel_ntt_ctx* c, uint64_t psi, TableGenJob* j)
+{
+    const uint64_t q = c->q, n = c->n;
+    const uint64_t psi_inv = powmod(psi, q - 2, q);
+    const uint64_t ninv = powmod(n % q, q - 2, q);
+    uint64_t rev = 0;  // bitrev(n - 2): the last inverse entry is psi^-(bitrev(n-2)+1)
+    for (uint32_t b = 0; b < c->logn; ++b) rev |= (((n - 2) >> b) & 1) << (c->logn - 1 - b);
+    unsigned char* base = static_cast<unsigned char*>(c->mem);
+    j->hdr = make_header(c, base, powmod(psi_inv, rev + 1, q), ninv, shoup_quotient(ninv, q));
+    j->base = base;
+    j->q = q;
+    uint64_t x = q;  // q^-1 mod 2^64 by Newton's iteration (q odd)
+    for (int k = 0; k < 6; ++k) x *= 2 - q * x;
+    j->mninv = 0 - x;
+    j->one_m = (uint64_t)(((u128)1 << 64) % q);
+    j->r2m = (uint64_t)(((u128)j->one_m * j->one_m) % q);
+    j->psi_m = (uint64_t)(((u128)(psi % q) << 64) % q);
+    j->psiinv_m = (uint64_t)(((u128)psi_inv << 64) % q);
+    j->n = n;
+    j->logn = c->logn;
+    j->pad = 0;
 }
 
 axhel_status_t check_modulus(uint64_t q, uint64_t limit_bits)
@@ -206,38 +212,90 @@ int axhel_cuda_is_device_pointer(const void* p)
 
 axhel_status_t axhel_cuda_ntt_create(uint64_t degree, uint64_t modulus, uint64_t root, axhel_ntt_t* out)
 {
-    if (!out) return fail(AXHEL_ERR_INVALID, "null output handle");
-    *out = nullptr;
-    uint32_t logn;
-    axhel_status_t st = check_degree(degree, &logn);
-    if (st) return st;
-    if ((st = check_modulus(modulus, 62))) return st;
-    if (root == 0 || root >= modulus) return fail(AXHEL_ERR_INVALID, "root of unity must be in [1, q)");
+    return axhel_cuda_ntt_create_many(1, &degree, &modulus, &root, out);
+}
+
+axhel_status_t axhel_cuda_ntt_create_many(uint64_t count, const uint64_t* degrees, const uint64_t* moduli,
+                                          const uint64_t* roots, axhel_ntt_t* out)
+{
+    if (!out || (count && (!degrees || !moduli || !roots))) return fail(AXHEL_ERR_INVALID, "null argument");
+    for (uint64_t i = 0; i < count; ++i) out[i] = nullptr;
+    std::vector<uint32_t> logn(count);
+    for (uint64_t i = 0; i < count; ++i) {
+        axhel_status_t st = check_degree(degrees[i], &logn[i]);
+        if (st) return st;
+        if ((st = check_modulus(moduli[i], 62))) return st;
+        if (!(moduli[i] & 1))
+            return fail(AXHEL_ERR_INVALID, "the modulus must be odd (an NTT modulus is a prime q = 1 mod 2N)");
+        if (roots[i] == 0 || roots[i] >= moduli[i]) return fail(AXHEL_ERR_INVALID, "root of unity must be in [1, q)");
+    }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     std::lock_guard<std::mutex> lk(g_cache_mu);
-    auto key = std::make_tuple(dev, degree, modulus, root);
-    auto it = g_cache.find(key);
-    if (it != g_cache.end()) {
-        it->second->refs.fetch_add(1);
-        *out = it->second;
-        return AXHEL_OK;
+    // cache hits take a reference; misses (each distinct key once) get an
+    // allocation and a generation job
+    std::map<std::tuple<int, uint64_t, uint64_t, uint64_t>, axhel_ntt_ctx*> fresh;
+    std::vector<TableGenJob> jobs;
+    auto undo = [&](axhel_status_t st, const std::string& m) {
+        for (uint64_t i = 0; i < count; ++i)
+            if (out[i] && out[i]->cached && !fresh.count(std::make_tuple(dev, degrees[i], moduli[i], roots[i])))
+                out[i]->refs.fetch_sub(1);
+        for (auto& kv : fresh) {
+            if (kv.second->mem) cudaFree(kv.second->mem);
+            delete kv.second;
+        }
+        for (uint64_t i = 0; i < count; ++i) out[i] = nullptr;
+        return fail(st, m);
+    };
+    for (uint64_t i = 0; i < count; ++i) {
+        const auto key = std::make_tuple(dev, degrees[i], moduli[i], roots[i]);
+        auto it = g_cache.find(key);
+        if (it != g_cache.end()) {
+            it->second->refs.fetch_add(1);
+            out[i] = it->second;
+            continue;
+        }
+        auto f = fresh.find(key);
+        if (f != fresh.end()) {
+            f->second->refs.fetch_add(1);
+            out[i] = f->second;
+            continue;
+        }
+        auto* c = new axhel_ntt_ctx();
+        c->n = degrees[i];
+        c->q = moduli[i];
+        c->root = roots[i];
+        c->logn = logn[i];
+        c->device = dev;
+        c->cached = true;
+        c->refs.store(2);  // the cache keeps one reference: tables stay resident for the process
+        fresh[key] = c;
+        out[i] = c;
+        e = cudaMalloc(&c->mem, kHeader + 2 * c->n * 16);
+        if (e != cudaSuccess) {
+            c->mem = nullptr;
+            return undo(AXHEL_ERR_NOMEM, std::string("cudaMalloc(tables): ") + cudaGetErrorString(e));
+        }
+        c->dctx = reinterpret_cast<const ModCtx*>(c->mem);
+        jobs.emplace_back();
+        gen_job(c, roots[i], &jobs.back());
     }
-    auto c = std::make_unique<axhel_ntt_ctx>();
-    c->n = degree;
-    c->q = modulus;
-    c->root = root;
-    c->logn = logn;
-    c->device = dev;
-    c->cached = true;
-    std::vector<uint64_t> fwd(2 * degree), inv(2 * degree);
-    uint64_t ninv[2];
-    generate_tables(degree, logn, modulus, root, fwd.data(), inv.data(), ninv);
-    if ((st = upload(c.get(), fwd.data(), inv.data(), ninv))) return st;
-    c->refs.store(2);  // the cache keeps one reference: tables stay resident for the process
-    g_cache[key] = c.get();
-    *out = c.release();
+    // one launch per 96 contexts, then wait: the tables are complete when
+    // this returns, for any stream of any thread
+    const cudaStream_t s = cudaStreamPerThread;
+    for (size_t k = 0; k < jobs.size(); k += kTableGenJobsPerLaunch) {
+        TableGenArgs a{};
+        uint64_t max_n = 0;
+        for (size_t m = k; m < jobs.size() && a.njobs < (uint32_t)kTableGenJobsPerLaunch; ++m) {
+            a.job[a.njobs++] = jobs[m];
+            max_n = std::max<uint64_t>(max_n, jobs[m].n);
+        }
+        if ((e = launch_gen_tables(a, max_n, s)) != cudaSuccess) return undo(AXHEL_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (!jobs.empty() && (e = cudaStreamSynchronize(s)) != cudaSuccess)
+        return undo(AXHEL_ERR_CUDA, std::string("table generation: ") + cudaGetErrorString(e));
+    for (auto& kv : fresh) g_cache[kv.first] = kv.second;
     return AXHEL_OK;
 }
 

@@ -131,12 +131,14 @@ def reference_roundtrip_rate(mods, data, threads, target_s):
     """Times the reference native backend (oracle/_ref) on a bounded sample of
     the workload: the lazy round trip on S limbs over `threads` host threads,
     repeated to about `target_s` seconds.  Returns (limb-transforms/s, S,
-    repeats, seconds)."""
+    repeats, seconds, table-generation seconds)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from pyoracle import Reference
 
     ref = Reference()
-    ntts = [ref.ntt(N, q, psi) for q, psi in mods]
+    t = time.perf_counter()
+    ntts = [ref.ntt(N, q, psi) for q, psi in mods]  # GenerateNTTTables, one host thread
+    tables_s = time.perf_counter() - t
     S = min(len(data), max(threads, 4 * threads))
     buf = np.ascontiguousarray(data[:S])
     t = time.perf_counter()
@@ -149,7 +151,7 @@ def reference_roundtrip_rate(mods, data, threads, target_s):
     dt = time.perf_counter() - t
     if not np.array_equal(buf, data[:S]):
         raise RuntimeError("reference round trip did not reproduce its input")
-    return 2 * S * reps / dt, S, reps, dt
+    return 2 * S * reps / dt, S, reps, dt, tables_s
 
 
 def run_reference(args):
@@ -161,7 +163,7 @@ def run_reference(args):
     data = make_inputs(mods, COUNT)
     # size each step so the whole run stays within ~2 minutes
     budget = min(10.0, 120.0 / max(1, args.steps + args.warmup))
-    rate, _, _, _ = reference_roundtrip_rate(mods, data, threads, 1.0)
+    rate = reference_roundtrip_rate(mods, data, threads, 1.0)[0]
     S = int(min(COUNT, max(threads, round(budget * rate / 2 / threads) * threads)))
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from pyoracle import Reference
@@ -212,7 +214,11 @@ def run_ours(args):
     sh = stream.cuda_stream
 
     mods = workload_moduli()
-    ntts = [capi.NTT(N, q, psi) for q, psi in mods]
+    torch.cuda.synchronize()
+    # cold start: the 24 contexts' tables generated on the device in one launch
+    t_tab = time.perf_counter()
+    ntts = capi.NTT.create_many([(N, q, psi) for q, psi in mods])
+    tables_ms = 1e3 * (time.perf_counter() - t_tab)
     data = make_inputs(mods, COUNT, SEED + rank)
     x = torch.from_numpy(data.reshape(-1).view(np.int64)).to(dev)
     y = torch.empty_like(x)
@@ -321,10 +327,11 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             threads = len(os.sched_getaffinity(0))
-            rate, S, reps, secs = reference_roundtrip_rate(mods, data, threads, args.cpu_seconds)
+            rate, S, reps, secs, tables_s = reference_roundtrip_rate(mods, data, threads, args.cpu_seconds)
             cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
                    "sample": f"{S} limbs of the N=2^16 workload x {reps} repeats, lazy round trip "
-                             f"(forward, ReduceMod 4->2, inverse), {secs:.1f} s"}
+                             f"(forward, ReduceMod 4->2, inverse), {secs:.1f} s",
+                   "tables_ms": 1e3 * tables_s}
         except Exception as e:  # the reference build is test infrastructure; report its absence
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
 
@@ -345,6 +352,11 @@ def run_ours(args):
             "plain_per_limb": plain,
             "e2e": e2e,
             "serve": serve,
+            "tables": {"contexts": len(mods), "degree": N, "device_ms": tables_ms,
+                       "reference_cpu_ms": cpu["tables_ms"] if cpu and "tables_ms" in cpu else None,
+                       "note": "cold start: twiddle tables of the 24 moduli, device generation (one launch, "
+                               "wall clock incl. allocation) vs the reference's GenerateNTTTables on one host "
+                               "thread"},
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

@@ -56,10 +56,20 @@ int axhel_version(void);
 /* Replaces NTT::NTT(degree, modulus, root_of_unity)
  * (axhel/include/axhel/ntt/ntt.hpp:32, axhel/ntt/ntt.cpp:136-152).
  * Generates the forward/inverse Shoup tables once per (degree, modulus, root)
- * (process-wide cache) and keeps them resident on the current device.  The
- * returned handle holds one reference; release it with axhel_cuda_ntt_release. */
+ * (process-wide cache), on the device, and keeps them resident there.  The
+ * returned handle holds one reference; release it with axhel_cuda_ntt_release.
+ * The modulus must be odd (NTT moduli are primes q = 1 mod 2N). */
 axhel_status_t axhel_cuda_ntt_create(uint64_t degree, uint64_t modulus, uint64_t root_of_unity,
                                      axhel_ntt_t* out);
+
+/* Many NTT::NTT(degree, modulus, root_of_unity) at once (new; the cold start
+ * of a parameter set with many RNS moduli): out[i] for (degrees[i],
+ * moduli[i], roots[i]), cache hits shared.  The tables of all contexts not
+ * yet cached are generated by one kernel launch per 96 contexts -- entry for
+ * entry equal to GenerateNTTTables (axhel/ntt/ntt-tables.cpp:81-140) -- and
+ * are ready when the call returns.  On failure no handle is returned. */
+axhel_status_t axhel_cuda_ntt_create_many(uint64_t count, const uint64_t* degrees, const uint64_t* moduli,
+                                          const uint64_t* roots, axhel_ntt_t* out);
 
 /* Replaces NTT::NTT(degree, modulus, root_powers, inv_root_powers, inv_degree_modulo)
  * (ntt.hpp:37, ntt.cpp:124-133).  root_powers / inv_root_powers are HOST

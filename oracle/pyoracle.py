@@ -114,7 +114,14 @@ class Oracle(_Common):
         self.is_prime = self._fn("is_prime", C.c_int, u64)
         self.find_ntt_prime = self._fn("find_ntt_prime", u64, u64, C.c_uint)
         self.find_ntt_prime_near = self._fn("find_ntt_prime_near", u64, u64, C.c_uint, u64, u64)
-        self.find_primitive_root = self._fn("find_primitive_root", u64, u64, u64)
+        root = self._fn("find_primitive_root", u64, u64, u64)
+
+        def find_primitive_root(n, q):
+            if q < 3 or q % (2 * n) != 1:  # also guards the C search against q = 0 (a failed prime search)
+                raise ValueError(f"no primitive 2N-th root: q={q} is not 1 mod 2N={2 * n}")
+            return root(n, q)
+
+        self.find_primitive_root = find_primitive_root
         self.pow_mod = self._fn("pow_mod", u64, u64, u64, u64)
         self.barrett_factor = self._fn("barrett_factor", u64, u64)
         self.shoup_quotient = self._fn("shoup_quotient", u64, u64, u64)
