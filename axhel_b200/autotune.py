@@ -1,4 +1,4 @@
-"""Autotuner for the NTT pass plans.
+"""Autotuner for the NTT pass plans and the uneven-batch engine's split.
 
 For each direction, degree N = 2^logn and limb-count bucket, times every
 candidate split of the log2 N stages into passes (1 or 2 passes), register
@@ -8,11 +8,18 @@ several launches of the batched C-ABI call) and writes the fastest to
 
     <inverse> <logn> <limb-bucket> <npass> (<lg> <lr> <tg>)...
 
-limb-bucket = floor(log2(limbs)).  Every candidate computes the same bits
-(tests/test_ntt_gpu.py::test_every_plan_bitexact), so the choice only
+limb-bucket = floor(log2(limbs)).  For the uneven-batch engine (fixed
+1024-residue tiles) it times, per degree, every split of a job's stages into
+its strided and contiguous passes on a batch of forward, inverse and chained
+jobs, and writes
+
+    B <logn> <contiguous-pass stages>
+
+Every candidate computes the same bits (tests/test_ntt_gpu.py::
+test_every_plan_bitexact, tests/test_batch_gpu.py), so the choice only
 affects speed.
 
-    python -m axhel_b200.autotune [--logn 12-17] [--buckets 0,3,6,9]
+    python -m axhel_b200.autotune [--what all|passes|batch] [--logn 12-17] [--buckets 0,3,6,9]
 """
 from __future__ import annotations
 
@@ -118,8 +125,60 @@ def tune(lognums, buckets, limbs_cap_bytes=1 << 30, verbose=True):
     return lines
 
 
+def tune_batch(lognums, bytes_per_job=128 << 20, reps=5, verbose=True):
+    """Per degree, the batch engine's contiguous-pass width that runs a
+    forward, an inverse and a chained job of ~128 MiB each fastest."""
+    import torch
+
+    from axhel_b200 import capi, params
+
+    lines = []
+    for logn in lognums:
+        if not 10 <= logn <= 17:
+            continue
+        n = 1 << logn
+        mods = params.rns_moduli(n, 8, 50, 59)
+        ntts = [capi.NTT(n, q, psi) for q, psi in mods]
+        count = max(8, bytes_per_job // (n * 8)) // 8 * 8
+        rng = np.random.default_rng(logn)
+        data = np.concatenate([rng.integers(0, mods[i % 8][0], n, dtype=np.uint64) for i in range(count)])
+        bufs = [torch.from_numpy(data.view(np.int64)).cuda() for _ in range(4)]
+        outs = [torch.empty_like(bufs[0]) for _ in range(3)]
+        specs = [dict(kind=capi.JOB_FORWARD, ntts=ntts, count=count, result=outs[0].data_ptr(),
+                      operand=bufs[0].data_ptr(), in_f=1, out_f=4),
+                 dict(kind=capi.JOB_INVERSE, ntts=ntts, count=count, result=outs[1].data_ptr(),
+                      operand=bufs[1].data_ptr(), in_f=2, out_f=1),
+                 dict(kind=capi.JOB_CHAIN_MUL, ntts=ntts, count=count, result=outs[2].data_ptr(),
+                      operand=bufs[2].data_ptr(), vector=bufs[3].data_ptr(), in_f=2, out_f=4)]
+        best = None
+        for row in range(max(5, logn - 9), min(9, logn - 5) + 1):
+            capi.batch_split_set(logn, row)
+            b = capi.Batch(specs)
+            b.launch()
+            torch.cuda.synchronize()
+            ts = []
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                b.launch()
+                e1.record()
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            b.close()
+            ms = statistics.median(ts)
+            if verbose:
+                print(f"batch logn={logn} row={row}: {ms:.3f} ms ({4 * count / (ms / 1e3):,.0f} limb-transforms/s)",
+                      flush=True)
+            if best is None or ms < best[0]:
+                best = (ms, row)
+        capi.batch_split_set(logn, 0)
+        lines.append(f"B {logn} {best[1]}")
+    return lines
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--what", choices=["all", "passes", "batch"], default="all")
     ap.add_argument("--logn", default="12-17")
     ap.add_argument("--buckets", default="0,3,5,7,9")
     ap.add_argument("--out", default=TABLE)
@@ -128,12 +187,24 @@ def main():
     lognums = list(range(int(lo), int(hi or lo) + 1))
     buckets = [int(b) for b in a.buckets.split(",")]
     t = time.time()
-    lines = tune(lognums, buckets)
+    old = []
+    if os.path.exists(a.out):
+        with open(a.out) as f:
+            old = [l.rstrip("\n") for l in f if l.strip() and not l.startswith("#")]
+    # lines of the part not re-tuned are kept
+    keep = [l for l in old if (l.startswith("B") if a.what == "passes" else
+                               (not l.startswith("B")) if a.what == "batch" else False)]
+    lines = []
+    if a.what in ("all", "passes"):
+        lines += tune(lognums, buckets)
+    if a.what in ("all", "batch"):
+        lines += tune_batch(list(range(10, 18)) if a.what == "all" else lognums)
+    merged = sorted(keep + lines, key=lambda l: (l.startswith("B"), l))
     with open(a.out, "w") as f:
         f.write("# NTT pass plans chosen by axhel_b200/autotune.py on one B200\n")
-        f.write("# inverse logn limb-bucket npass (lg lr tg)...\n")
-        f.write("\n".join(lines) + "\n")
-    print(f"wrote {a.out} ({len(lines)} plans, {time.time() - t:.0f} s)")
+        f.write("# inverse logn limb-bucket npass (lg lr tg)...  |  B logn contiguous-pass-stages (batch engine)\n")
+        f.write("\n".join(merged) + "\n")
+    print(f"wrote {a.out} ({len(lines)} lines tuned, {len(keep)} kept, {time.time() - t:.0f} s)")
 
 
 if __name__ == "__main__":

@@ -129,6 +129,8 @@ def _declare(L):
     d("axhel_cuda_plan_set", st_t, C.c_int, u32, u32, vp, vp, vp)
     d("axhel_cuda_plan_get", st_t, C.c_int, u32, u64, vp, vp, vp, vp)
     d("axhel_cuda_plan_load", st_t, C.c_char_p, C.POINTER(u32))
+    d("axhel_cuda_batch_split_set", st_t, u32, u32)
+    d("axhel_cuda_batch_split_get", st_t, u32, C.POINTER(u32))
     d("axhel_cuda_is_device_pointer", C.c_int, vp)
     d("axhel_cuda_launch_count", u64)
     d("axhel_cuda_profile_enable", st_t, C.c_int)
@@ -483,6 +485,17 @@ def plan_get(inverse, logn, count):
     check(lib().axhel_cuda_plan_get(int(inverse), logn, count, C.byref(npass), C.cast(lg, vp), C.cast(lr, vp),
                                     C.cast(tg, vp)), "plan_get")
     return [(lg[i], lr[i], tg[i]) for i in range(npass.value)]
+
+
+def batch_split_set(logn, row_stages):
+    """Contiguous-pass stages of the batch engine for N = 2^logn (0 restores)."""
+    check(lib().axhel_cuda_batch_split_set(logn, row_stages), "batch_split_set")
+
+
+def batch_split_get(logn):
+    r = u32()
+    check(lib().axhel_cuda_batch_split_get(logn, C.byref(r)), "batch_split_get")
+    return r.value
 
 
 def plan_load(path=None):

@@ -11,8 +11,8 @@
 //             column pass] -> forward row pass
 //   element-wise : one phase, the op on 1024 residues of one limb per tile
 //
-// with B = min(9, n - 5) and A = n - B: the contiguous pass as wide as a tile
-// allows, which measured fastest.  The kernel is persistent (one wave of CTAs
+// with B stages in the contiguous pass, from the autotuner's table per degree
+// (default min(9, n - 5): as wide as a tile allows), and A = n - B.  The kernel is persistent (one wave of CTAs
 // sized to the device); CTAs take tiles from one atomic counter in
 // phase-major order (every phase-0 tile of every job before any phase-1
 // tile), so by the time a phase-p tile is taken, every tile it depends on is
@@ -492,7 +492,7 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
             continue;
         }
         if (J.kind == AXHEL_JOB_CHAIN_FMA) scal[i].assign(J.scalars, J.scalars + J.n_ntts);
-        b.lg_row = logn - 5 < 9 ? logn - 5 : 9;
+        b.lg_row = (uint32_t)batch_row_stages(logn);
         b.lg_col = logn - b.lg_row;
         const bool inv_first = J.kind != AXHEL_JOB_FORWARD;
         b.pre = inv_first && J.input_mod_factor == 4;

@@ -647,4 +647,20 @@ axhel_status_t axhel_cuda_plan_load(const char* path, uint32_t* loaded)
     return AXHEL_OK;
 }
 
+axhel_status_t axhel_cuda_batch_split_set(uint32_t logn, uint32_t row)
+{
+    if (row && !batch_row_valid(logn, (int)row))
+        return fail(AXHEL_ERR_INVALID, "batch split: need log N in [10, 17] and contiguous stages in "
+                                       "[max(5, log N - 9), min(9, log N - 5)]");
+    batch_row_override(logn, (int)row);
+    return AXHEL_OK;
+}
+
+axhel_status_t axhel_cuda_batch_split_get(uint32_t logn, uint32_t* row)
+{
+    if (!row || logn < 10 || logn > 17) return fail(AXHEL_ERR_INVALID, "batch split: log N in [10, 17]");
+    *row = (uint32_t)batch_row_stages(logn);
+    return AXHEL_OK;
+}
+
 }  // extern "C"

@@ -79,6 +79,11 @@ NttPlan plan_for(bool inverse, uint32_t logn, uint64_t limbs);
 bool plan_valid(const NttPlan& p, uint32_t logn, bool inverse);
 int plan_load(const char* path);
 void plan_override(bool inverse, uint32_t logn, const NttPlan* p);  // nullptr clears
+// Uneven-batch engine: stages of the contiguous pass of an N = 2^logn job
+// (override > table > default); the strided pass takes the rest.
+bool batch_row_valid(uint32_t logn, int row);
+int batch_row_stages(uint32_t logn);
+void batch_row_override(uint32_t logn, int row);  // 0 clears
 
 // Bytes reserved for the ModCtx header in front of the twiddle tables.
 constexpr size_t kCtxHeaderBytes = 256;

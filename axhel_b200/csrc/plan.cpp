@@ -7,6 +7,8 @@
 //   <inverse 0|1> <logn> <limb-bucket> <npass> (<lg> <lr> <tg>){npass}
 // where limb-bucket = floor(log2(limbs)) clamped to [0, 15].  A lookup takes
 // the nearest bucket at or below the requested one, else the nearest above.
+// Lines `B <logn> <row stages>` give the uneven-batch engine's split of an
+// N = 2^logn job into its strided and contiguous passes.
 #include <dlfcn.h>
 
 #include <cstdio>
@@ -26,6 +28,7 @@ namespace {
 std::mutex g_mu;
 std::map<std::pair<int, uint32_t>, NttPlan> g_override;
 std::map<std::tuple<int, uint32_t, int>, NttPlan> g_table;
+std::map<uint32_t, int> g_batch_override, g_batch_table;  // logn -> contiguous-pass stages
 bool g_table_tried = false;
 
 int bucket_of(uint64_t limbs)
@@ -89,6 +92,15 @@ int load_table_locked(const char* path)
     int n = 0;
     while (std::fgets(line, sizeof line, fp)) {
         if (line[0] == '#' || line[0] == '\n') continue;
+        if (line[0] == 'B') {
+            int logn, row;
+            if (std::sscanf(line + 1, "%d %d", &logn, &row) == 2 && logn > 0 &&
+                batch_row_valid((uint32_t)logn, row)) {
+                g_batch_table[(uint32_t)logn] = row;
+                ++n;
+            }
+            continue;
+        }
         int inv, logn, bucket, npass, v[9] = {0};
         int got = std::sscanf(line, "%d %d %d %d %d %d %d %d %d %d %d %d %d", &inv, &logn, &bucket, &npass, &v[0],
                               &v[1], &v[2], &v[3], &v[4], &v[5], &v[6], &v[7], &v[8]);
@@ -164,6 +176,33 @@ void plan_override(bool inverse, uint32_t logn, const NttPlan* p)
         g_override[{inverse ? 1 : 0, logn}] = *p;
     else
         g_override.erase({inverse ? 1 : 0, logn});
+}
+
+bool batch_row_valid(uint32_t logn, int row)
+{
+    const int lo = (int)logn - 9 > 5 ? (int)logn - 9 : 5;
+    const int hi = (int)logn - 5 < 9 ? (int)logn - 5 : 9;
+    return logn >= 10 && logn <= 17 && row >= lo && row <= hi;
+}
+
+int batch_row_stages(uint32_t logn)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_batch_override.find(logn);
+    if (it != g_batch_override.end()) return it->second;
+    ensure_table_locked();
+    auto t = g_batch_table.find(logn);
+    if (t != g_batch_table.end()) return t->second;
+    return (int)logn - 5 < 9 ? (int)logn - 5 : 9;  // the contiguous pass as wide as a tile allows
+}
+
+void batch_row_override(uint32_t logn, int row)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (row)
+        g_batch_override[logn] = row;
+    else
+        g_batch_override.erase(logn);
 }
 
 int plan_load(const char* path)

@@ -304,6 +304,13 @@ def run_ours(args):
 
     # ---- e2e through the C-ABI with pinned host buffers, copies inside the timed region
     e2e = end_to_end(capi, ntts, data, dev, steps=max(1, min(args.steps, 10)))
+    if pg:  # whole-job rate: every rank moves its own batch over its own link; slowest rank's time
+        t = torch.tensor([e2e["ms_per_step"]], device=dev, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e["ms_per_step"] = float(t.item())
+        e2e["value"] = world * 2 * COUNT / (e2e["ms_per_step"] / 1e3)
+        e2e["h2d_bytes_per_step"] *= world
+        e2e["d2h_bytes_per_step"] *= world
 
     # ---- serving loop (continuous batching) at 70 % of its measured capacity:
     # host-staged requests (copies in the loop) and device-resident ones

@@ -358,6 +358,12 @@ axhel_status_t axhel_cuda_plan_get(int inverse, uint32_t log_degree, uint64_t co
 /* Loads an autotuner table (text, one plan per line); NULL = the table shipped
  * beside the library.  Returns the number of plans loaded via *loaded. */
 axhel_status_t axhel_cuda_plan_load(const char* path, uint32_t* loaded);
+/* Uneven-batch engine (new): stages of the contiguous pass of an N = 2^log_degree
+ * job (the strided pass takes the rest), in [max(5, log N - 9), min(9, log N - 5)];
+ * 0 restores the table / default.  Applies to batches created afterwards.
+ * Used by the autotuner; every split computes the same bits. */
+axhel_status_t axhel_cuda_batch_split_set(uint32_t log_degree, uint32_t row_stages);
+axhel_status_t axhel_cuda_batch_split_get(uint32_t log_degree, uint32_t* row_stages);
 
 /* ---------------------------------------------------------------------- */
 /* Host-pointer helpers used by the C++ drop-in                           */

@@ -151,3 +151,18 @@ def test_dependency_wait_times_out_and_device_recovers(cuda, oracle):
     assert b.status() == 0
     check(oracle, jobs, bufs)
     b.close()
+
+
+def test_every_batch_split_bitexact(cuda, oracle):
+    """Every strided/contiguous split the autotuner may pick gives the same bits."""
+    rng = np.random.default_rng(61)
+    for logn in (10, 13, 15, 17):
+        jobs = make_jobs(cuda, oracle, rng, 3, [logn], 2, 2)
+        for row in range(max(5, logn - 9), min(9, logn - 5) + 1):
+            cuda.batch_split_set(logn, row)
+            try:
+                specs, bufs = specs_for(cuda, jobs)
+                cuda.batch_run(specs)
+                check(oracle, jobs, bufs)
+            finally:
+                cuda.batch_split_set(logn, 0)

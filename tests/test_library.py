@@ -118,3 +118,19 @@ def test_params_primes_match_reference_generator(oracle):
     mods = params.rns_moduli(1 << 16, 24, 50, 59)
     assert len({q for q, _ in mods}) == 24
     assert all((q - 1) % (1 << 17) == 0 and 50 <= q.bit_length() <= 59 for q, _ in mods)
+
+
+def test_batch_split_table_and_override(tmp_path):
+    from axhel_b200 import capi
+
+    t = tmp_path / "plans.txt"
+    t.write_text("B 15 7\nB 16 4\nB 12 9\n")  # the last two are outside the valid ranges
+    assert capi.plan_load(str(t)) == 1
+    assert capi.batch_split_get(15) == 7
+    capi.batch_split_set(15, 6)
+    assert capi.batch_split_get(15) == 6
+    capi.batch_split_set(15, 0)  # back to the table
+    assert capi.batch_split_get(15) == 7
+    for logn, row in ((16, 4), (16, 12), (12, 8), (9, 5), (18, 9)):
+        with pytest.raises(capi.AxhelError):
+            capi.batch_split_set(logn, row)
