@@ -150,6 +150,32 @@ __device__ __forceinline__ void thread_role(const Tile& t, uint32_t& gi, uint32_
     }
 }
 
+// Highest thread-in-group bit (k) whose in-group bit changes between rounds
+// RD-1 and RD (-1 if none).  Element r sits in thread k(r) = r's bits below
+// the register window, then those above it shifted down by LR; bits move
+// between k and the registers, or between k positions, only up to here.
+template <bool INV, int LG, int LR, int RD>
+constexpr int exchange_max_pos()
+{
+    constexpr int lp = round_lo<INV, LG, LR, RD - 1>(), ln = round_lo<INV, LG, LR, RD>();
+    int m = -1;
+    for (int b = 0; b < LG; ++b) {
+        const bool rp = b >= lp && b < lp + LR, rn = b >= ln && b < ln + LR;
+        const int pp = rp ? -1 : (b < lp ? b : b - LR), pn = rn ? -1 : (b < ln ? b : b - LR);
+        if (pp != pn) m = (pp > m ? pp : m) > pn ? (pp > m ? pp : m) : pn;
+    }
+    return m;
+}
+
+// Lane shift of k in the thread index: 0 for contiguous tiles (thread =
+// group * threads-per-group + k), log2 groups per tile for strided ones
+// (thread = group + k * groups); 32 for CTAs under one warp, which always
+// synchronize the whole CTA.
+__device__ __forceinline__ uint32_t lane_shift(bool strided, uint32_t lgtg)
+{
+    return blockDim.x >= 32 ? (strided ? lgtg : 0u) : 32u;
+}
+
 // In-group index of register 0 for register bits [lo, lo + LR).
 template <int LR>
 __device__ __forceinline__ uint32_t round_base(uint32_t k, int lo)
@@ -293,15 +319,23 @@ __device__ __forceinline__ void inv_stages(uint64_t (&v)[1 << LR], uint32_t rbas
 // thread writes back the slots it held and reads its next slots; the slot
 // sets of one round are disjoint across threads, so one barrier suffices.
 template <bool INV, int LG, int LR, int RD>
-__device__ __forceinline__ void exchange(uint64_t (&v)[1 << LR], uint64_t* smg, uint32_t k, uint32_t hmask)
+__device__ __forceinline__ void exchange(uint64_t (&v)[1 << LR], uint64_t* smg, uint32_t k, uint32_t hmask,
+                                         uint32_t lsh)
 {
     constexpr int R = 1 << LR;
     constexpr int lp = round_lo<INV, LG, LR, RD - 1>();
     constexpr int ln = round_lo<INV, LG, LR, RD>();
+    constexpr int mp = exchange_max_pos<INV, LG, LR, RD>();
     const uint32_t bp = round_base<LR>(k, lp), bn = round_base<LR>(k, ln);
 #pragma unroll
     for (int i = 0; i < R; ++i) smg[slot<LG, LR>(bp | ((uint32_t)i << lp), hmask)] = v[i];
-    __syncthreads();
+    // Every thread writes the slots it read at the previous exchange, so when
+    // all changed k bits are lane bits (the inner stages) the elements only
+    // move inside a warp and a warp barrier orders them.  (Uniform branch.)
+    if (mp + (int)lsh < 5)
+        __syncwarp();
+    else
+        __syncthreads();
 #pragma unroll
     for (int i = 0; i < R; ++i) v[i] = smg[slot<LG, LR>(bn | ((uint32_t)i << ln), hmask)];
 }
@@ -309,20 +343,21 @@ __device__ __forceinline__ void exchange(uint64_t (&v)[1 << LR], uint64_t* smg, 
 // Rounds 1 .. NR-1 (round 0 runs on the freshly loaded registers).
 template <int LG, int LR, int... RD>
 __device__ __forceinline__ void fwd_rest(std::integer_sequence<int, RD...>, uint64_t (&v)[1 << LR], uint64_t* smg,
-                                         uint32_t k, uint32_t hmask, uint64_t blk, uint32_t s0, const ulonglong2* tw,
-                                         uint64_t q, uint64_t q2)
+                                         uint32_t k, uint32_t hmask, uint32_t lsh, uint64_t blk, uint32_t s0,
+                                         const ulonglong2* tw, uint64_t q, uint64_t q2)
 {
-    ((exchange<false, LG, LR, RD + 1>(v, smg, k, hmask),
+    ((exchange<false, LG, LR, RD + 1>(v, smg, k, hmask, lsh),
       fwd_stages<LG, LR, RD + 1>(v, round_base<LR>(k, round_lo<false, LG, LR, RD + 1>()), blk, s0, tw, q, q2)),
      ...);
 }
 
 template <int LG, int LR, int... RD>
 __device__ __forceinline__ void inv_rest(std::integer_sequence<int, RD...>, uint64_t (&v)[1 << LR], uint64_t* smg,
-                                         uint32_t k, uint32_t hmask, uint64_t blk, uint32_t s0, uint64_t n,
-                                         const ulonglong2* tw, uint64_t q, uint64_t q2, bool last, const ModCtx* cx)
+                                         uint32_t k, uint32_t hmask, uint32_t lsh, uint64_t blk, uint32_t s0,
+                                         uint64_t n, const ulonglong2* tw, uint64_t q, uint64_t q2, bool last,
+                                         const ModCtx* cx)
 {
-    ((exchange<true, LG, LR, RD + 1>(v, smg, k, hmask),
+    ((exchange<true, LG, LR, RD + 1>(v, smg, k, hmask, lsh),
       inv_stages<LG, LR, RD + 1>(v, round_base<LR>(k, round_lo<true, LG, LR, RD + 1>()), blk, s0, n, tw, q, q2,
                                  last, cx)),
      ...);
@@ -330,18 +365,18 @@ __device__ __forceinline__ void inv_rest(std::integer_sequence<int, RD...>, uint
 
 template <bool INV, int LG, int LR>
 __device__ __forceinline__ void run_rounds(uint64_t (&v)[1 << LR], uint64_t* smg, uint32_t k, uint32_t hmask,
-                                           uint64_t blk, uint32_t s0, uint64_t n, const ModCtx* cx, uint64_t q,
-                                           uint64_t q2, bool last)
+                                           uint32_t lsh, uint64_t blk, uint32_t s0, uint64_t n, const ModCtx* cx,
+                                           uint64_t q, uint64_t q2, bool last)
 {
     constexpr int NR = num_rounds<LG, LR>();
     if constexpr (INV) {
         inv_stages<LG, LR, 0>(v, round_base<LR>(k, round_lo<true, LG, LR, 0>()), blk, s0, n, cx->inv, q, q2, last,
                               cx);
-        inv_rest<LG, LR>(std::make_integer_sequence<int, NR - 1>{}, v, smg, k, hmask, blk, s0, n, cx->inv, q, q2,
-                         last, cx);
+        inv_rest<LG, LR>(std::make_integer_sequence<int, NR - 1>{}, v, smg, k, hmask, lsh, blk, s0, n, cx->inv, q,
+                         q2, last, cx);
     } else {
         fwd_stages<LG, LR, 0>(v, round_base<LR>(k, round_lo<false, LG, LR, 0>()), blk, s0, cx->fwd, q, q2);
-        fwd_rest<LG, LR>(std::make_integer_sequence<int, NR - 1>{}, v, smg, k, hmask, blk, s0, cx->fwd, q, q2);
+        fwd_rest<LG, LR>(std::make_integer_sequence<int, NR - 1>{}, v, smg, k, hmask, lsh, blk, s0, cx->fwd, q, q2);
     }
 }
 
@@ -376,8 +411,8 @@ __device__ __forceinline__ void pass_tile(const uint64_t* src, uint64_t* dst, co
 #pragma unroll
         for (int i = 0; i < R; ++i) v[i] = csub_lazy(v[i], q2);
     }
-    run_rounds<INV, LG, LR>(v, sm + (gi << LG), k, group_mask<LG, LR>(t.strided, lgtg, gi), blk, s0, n, cx, q, q2,
-                            (flags & kLastPass) != 0);
+    run_rounds<INV, LG, LR>(v, sm + (gi << LG), k, group_mask<LG, LR>(t.strided, lgtg, gi),
+                            lane_shift(t.strided, lgtg), blk, s0, n, cx, q, q2, (flags & kLastPass) != 0);
     if (flags & kPostNorm) {
 #pragma unroll
         for (int i = 0; i < R; ++i) v[i] = INV ? csub_lazy(v[i], q) : csub_lazy(csub_lazy(v[i], q2), q);
@@ -427,6 +462,7 @@ __device__ __forceinline__ void chain_tile(const uint64_t* src, uint64_t* dst, c
     const uint64_t blk = tile_blk<LG>(t, gi);
     uint64_t* smg = sm + (gi << LG);
     const uint32_t hmask = group_mask<LG, LR>(t.strided, lgtg, gi);
+    const uint32_t lsh = lane_shift(t.strided, lgtg);
 
     uint64_t v[R];
     load_global<LG, LR, LO_FIRST, CG>(v, lsrc, t, gi, round_base<LR>(k, LO_FIRST), vec_ok);
@@ -434,7 +470,7 @@ __device__ __forceinline__ void chain_tile(const uint64_t* src, uint64_t* dst, c
 #pragma unroll
         for (int i = 0; i < R; ++i) v[i] = csub_lazy(v[i], q2);
     }
-    run_rounds<true, LG, LR>(v, smg, k, hmask, blk, logn - LG, n, cx, q, q2, true);
+    run_rounds<true, LG, LR>(v, smg, k, hmask, lsh, blk, logn - LG, n, cx, q, q2, true);
 
     // Element-wise op on the inverse output (lazy [0, 2q)) with factor-2
     // inputs: EltwiseMulModNative<2> / EltwiseFMAModNative<2> formulas.
@@ -461,7 +497,7 @@ __device__ __forceinline__ void chain_tile(const uint64_t* src, uint64_t* dst, c
 
     // The forward's first pass: stages 0 .. LG-1 of block 0.
     fwd_stages<LG, LR, 0>(v, rb, 0, 0, cx->fwd, q, q2);
-    fwd_rest<LG, LR>(std::make_integer_sequence<int, NR - 1>{}, v, smg, k, hmask, 0, 0, cx->fwd, q, q2);
+    fwd_rest<LG, LR>(std::make_integer_sequence<int, NR - 1>{}, v, smg, k, hmask, lsh, 0, 0, cx->fwd, q, q2);
     if (flags & kPostNorm) {
 #pragma unroll
         for (int i = 0; i < R; ++i) v[i] = csub_lazy(csub_lazy(v[i], q2), q);
