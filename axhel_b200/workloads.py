@@ -262,14 +262,15 @@ def _pct(v, p):
 
 
 def serving(loads=(0.5, 0.7, 0.9), seconds=4.0, budget=60 << 30, inflight=4, seed=5, n_templates=32,
-            device=False, max_batch_words=0, persistent=False, plain=True, small_words=0, reserve=8 << 30):
+            device=False, max_batch_words=0, persistent=False, plain=True, small_words=0, reserve=8 << 30,
+            max_batch_requests=256):
     """Isolated latency of every template (alone on an idle server), capacity
     (a burst), then Poisson arrivals at each load fraction of capacity
     (host-staged requests: `reserve` bytes of the staging pool mapped up
     front): p50/p99 latency, p99 of each request's slowdown against its own isolated
     latency, and jobs/s; then the plain sequential GPU path."""
     rp = RequestPool(n_templates=n_templates, seed=seed, device=device)
-    srv = capi.Server(budget_bytes=budget, max_inflight=inflight, max_batch_requests=256,
+    srv = capi.Server(budget_bytes=budget, max_inflight=inflight, max_batch_requests=max_batch_requests,
                       max_batch_words=max_batch_words, persistent=persistent, small_request_words=small_words,
                       reserve_bytes=0 if device else reserve)
     rng = np.random.default_rng(seed)
@@ -367,6 +368,7 @@ def main():
     ap.add_argument("--max-batch-words", type=int, default=0)
     ap.add_argument("--inflight", type=int, default=4)
     ap.add_argument("--small-words", type=int, default=0, help="high-priority lane for requests up to this size")
+    ap.add_argument("--max-batch-requests", type=int, default=256)
     a = ap.parse_args()
     if a.what == "tensor":
         out = tensor_chain()
@@ -374,7 +376,8 @@ def main():
         out = uneven_batch()
     else:
         out = serving(seconds=a.seconds, device=a.device, persistent=a.persistent,
-                      max_batch_words=a.max_batch_words, inflight=a.inflight, small_words=a.small_words)
+                      max_batch_words=a.max_batch_words, inflight=a.inflight, small_words=a.small_words,
+                      max_batch_requests=a.max_batch_requests)
     print(json.dumps(out), flush=True)
 
 
