@@ -139,6 +139,7 @@ def _declare(L):
     d("axhel_cuda_batch_create", st_t, C.POINTER(Job), u64, C.POINTER(vp))
     d("axhel_cuda_batch_launch", st_t, vp, vp)
     d("axhel_cuda_batch_graph_launch", st_t, vp, vp)
+    d("axhel_cuda_batch_launch_phased", st_t, vp, vp)
     d("axhel_cuda_batch_status", st_t, vp, vp)
     d("axhel_cuda_batch_destroy", st_t, vp)
     d("axhel_cuda_batch_run", st_t, C.POINTER(Job), u64, vp)
@@ -229,8 +230,11 @@ class Batch:
         self.h = vp()
         _bcheck(lib().axhel_cuda_batch_create(self.jobs, len(specs), C.byref(self.h)), "batch_create")
 
-    def launch(self, stream=0, graph=False):
-        f = lib().axhel_cuda_batch_graph_launch if graph else lib().axhel_cuda_batch_launch
+    def launch(self, stream=0, graph=False, phased=False):
+        if phased:
+            f = lib().axhel_cuda_batch_launch_phased
+        else:
+            f = lib().axhel_cuda_batch_graph_launch if graph else lib().axhel_cuda_batch_launch
         _bcheck(f(self.h, stream), "batch_launch")
 
     def status(self, stream=0):

@@ -289,6 +289,7 @@ struct axhel_batch {
     size_t bytes = 0;
     size_t zero_off = 0, zero_bytes = 0;  // counters cleared before every launch
     BatchArgs args{};
+    uint64_t phase_begin[4] = {0, 0, 0, 0};  // first global tile of each phase, and the total
     unsigned grid = 0;
     std::vector<axhel_ntt_t> held;  // table contexts kept alive while the batch exists
     cudaGraphExec_t graph = nullptr;
@@ -622,7 +623,7 @@ axhel_status_t axhel_cuda_batch_create(const axhel_job_t* jobs, uint64_t n_jobs,
         cudaError_t e = cudaMalloc(&b->mem, b->bytes);
         if (e != cudaSuccess) return bfail(AXHEL_ERR_NOMEM, std::string("cudaMalloc(batch): ") + cudaGetErrorString(e));
         st = batch_build(jobs, n_jobs, static_cast<unsigned char*>(b->mem), img, &b->zero_off, &b->zero_bytes,
-                         &b->args, &held, &err);
+                         &b->args, &held, &err, b->phase_begin);
         if (st) {
             cudaFree(b->mem);
             return bfail(st, err);
@@ -648,6 +649,18 @@ axhel_status_t axhel_cuda_batch_launch(axhel_batch_t b, void* stream)
     if (b->args.total_tiles == 0) return AXHEL_OK;
     cudaError_t e = cudaMemsetAsync(static_cast<unsigned char*>(b->mem) + b->zero_off, 0, b->zero_bytes, s);
     if (e == cudaSuccess) e = batch_launch_args(b->args, s);
+    if (e != cudaSuccess) return bfail(AXHEL_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
+    return AXHEL_OK;
+}
+
+axhel_status_t axhel_cuda_batch_launch_phased(axhel_batch_t b, void* stream)
+{
+    if (!b) return bfail(AXHEL_ERR_INVALID, "null batch");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (b->args.total_tiles == 0) return AXHEL_OK;
+    // the error word is cleared as before a persistent launch (no wait can fail here)
+    cudaError_t e = cudaMemsetAsync(static_cast<unsigned char*>(b->mem) + b->zero_off, 0, b->zero_bytes, s);
+    if (e == cudaSuccess) e = batch_launch_phases(b->args, b->phase_begin, s);
     if (e != cudaSuccess) return bfail(AXHEL_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
     return AXHEL_OK;
 }

@@ -154,6 +154,9 @@ def uneven_batch(n_polys=512, seed=11, reps=3):
     def one_launch():
         b.launch()
 
+    def phased():
+        b.launch(phased=True)
+
     def per_limb():
         for j in jobs:
             n = j["n"]
@@ -192,11 +195,16 @@ def uneven_batch(n_polys=512, seed=11, reps=3):
     ms_batch = timed(one_launch, reps)
     st = b.status()
     same = st == 0 and all(torch.equal(r, j["y"]) for r, j in zip(ref, jobs))
+    for j in jobs:
+        j["y"].zero_()
+    ms_phased = timed(phased, reps)
+    same = same and b.status() == 0 and all(torch.equal(r, j["y"]) for r, j in zip(ref, jobs))
     b.close()
     limbs = sum(j["L"] for j in jobs)
     return {"workload": f"{n_polys} uneven polynomials, N in 2^12..2^17, L in 1..48, fwd/inv/chain mix",
             "limbs": limbs, "limb_transforms": transforms, "one_launch_ms": ms_batch,
-            "one_launch_rate": transforms / (ms_batch / 1e3), "per_limb_calls_ms": ms_plain,
+            "one_launch_rate": transforms / (ms_batch / 1e3), "phased_ms": ms_phased,
+            "phased_rate": transforms / (ms_phased / 1e3), "per_limb_calls_ms": ms_plain,
             "per_limb_rate": transforms / (ms_plain / 1e3), "speedup": ms_plain / ms_batch, "same_bits": same,
             "unit": UNIT}
 

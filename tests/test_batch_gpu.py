@@ -97,10 +97,10 @@ def test_batch_relaunch_and_graph_replay(cuda, oracle):
     jobs = make_jobs(cuda, oracle, rng, 10, [12, 16, 17], 3, 4)
     specs, bufs = specs_for(cuda, jobs)
     b = cuda.Batch(specs)
-    for graph in (False, False, True, True):
+    for graph, phased in ((False, False), (False, False), (True, False), (True, False), (False, True)):
         for _, o, _ in bufs:
             o.zero_()
-        b.launch(graph=graph)
+        b.launch(graph=graph, phased=phased)
         assert b.status() == 0
         check(oracle, jobs, bufs)
     b.close()
