@@ -1,8 +1,9 @@
 // Element-wise modular kernels for sm_100a (EltwiseAdd/Sub/Mul/FMA/ReduceMod).
 //
 // HBM-bound streaming kernels: a grid sized to a multiple of the SM count
-// walks the vector in 4-element chunks (two 16-byte loads per operand when all
-// pointers are 16-byte aligned, scalar 8-byte accesses otherwise).  The
+// walks the vector in chunks of four 16-byte loads per operand and thread,
+// each warp access 512 contiguous bytes (all pointers 16-byte aligned), or
+// in scalar 8-byte accesses otherwise.  The
 // arithmetic of each element is the reference native backend's formula
 // (axhel/eltwise/eltwise-*-mod.cpp), so every output is bit-identical.
 // result may alias any operand: each element is read before it is written by
@@ -25,32 +26,33 @@ template <class Op, bool HAS_B>
 __global__ void __launch_bounds__(256) eltwise_vec_kernel(uint64_t* r, const uint64_t* a, const uint64_t* b,
                                                           uint64_t n, const Op op)
 {
-    // 16-byte aligned path: 4 elements per thread per iteration.
-    const uint64_t nq = n >> 2;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += stride) {
-        const ulonglong2* a2 = reinterpret_cast<const ulonglong2*>(a) + 2 * i;
-        ulonglong2 x0 = a2[0], x1 = a2[1];
-        ulonglong2 y0 = make_ulonglong2(0, 0), y1 = y0;
-        if constexpr (HAS_B) {
-            const ulonglong2* b2 = reinterpret_cast<const ulonglong2*>(b) + 2 * i;
-            y0 = b2[0];
-            y1 = b2[1];
+    // 16-byte aligned path.  A CTA takes chunks of V * blockDim 16-byte
+    // vectors; vector k of a chunk is read by thread t at k * blockDim + t,
+    // so every warp access covers 512 contiguous bytes, and all loads of a
+    // chunk are issued before its first store (V loads per operand in flight
+    // per thread).
+    constexpr int V = 4;
+    const uint64_t nv = n >> 1;  // 16-byte vectors
+    const ulonglong2* a2 = reinterpret_cast<const ulonglong2*>(a);
+    const ulonglong2* b2 = reinterpret_cast<const ulonglong2*>(b);
+    ulonglong2* r2 = reinterpret_cast<ulonglong2*>(r);
+    const uint64_t chunk = (uint64_t)V * blockDim.x;
+    for (uint64_t c = (uint64_t)blockIdx.x * chunk + threadIdx.x; c < nv; c += (uint64_t)gridDim.x * chunk) {
+        ulonglong2 x[V], y[V];
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+            const uint64_t i = c + (uint64_t)k * blockDim.x;
+            x[k] = i < nv ? a2[i] : make_ulonglong2(0, 0);
+            y[k] = (HAS_B && i < nv) ? b2[i] : make_ulonglong2(0, 0);
         }
-        ulonglong2 z0, z1;
-        z0.x = op(x0.x, y0.x);
-        z0.y = op(x0.y, y0.y);
-        z1.x = op(x1.x, y1.x);
-        z1.y = op(x1.y, y1.y);
-        ulonglong2* r2 = reinterpret_cast<ulonglong2*>(r) + 2 * i;
-        r2[0] = z0;
-        r2[1] = z1;
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+            const uint64_t i = c + (uint64_t)k * blockDim.x;
+            if (i < nv) r2[i] = make_ulonglong2(op(x[k].x, y[k].x), op(x[k].y, y[k].y));
+        }
     }
-    // tail (< 4 elements) by the first threads of block 0
-    if (blockIdx.x == 0) {
-        const uint64_t i = (nq << 2) + threadIdx.x;
-        if (i < n) r[i] = op(a[i], HAS_B ? b[i] : 0);
-    }
+    // the odd last element by thread 0 of block 0
+    if (blockIdx.x == 0 && threadIdx.x == 0 && (n & 1)) r[n - 1] = op(a[n - 1], HAS_B ? b[n - 1] : 0);
 }
 
 template <class Op, bool HAS_B>
@@ -70,7 +72,7 @@ static cudaError_t run(uint64_t* r, const uint64_t* a, const uint64_t* b, uint64
     const uintptr_t align = reinterpret_cast<uintptr_t>(r) | reinterpret_cast<uintptr_t>(a) |
                             (HAS_B ? reinterpret_cast<uintptr_t>(b) : 0);
     const bool vec = (align & 15) == 0;
-    const uint64_t work = vec ? (n >> 2) : n;
+    const uint64_t work = vec ? (n >> 3) : n;  // vector path: 8 elements per thread per chunk
     uint64_t blocks = (work + threads - 1) / threads;
     const uint64_t cap = (uint64_t)sm_count() * 8;  // 8 resident CTAs of 256 threads per SM
     if (blocks > cap) blocks = cap;
