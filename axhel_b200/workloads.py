@@ -3,6 +3,8 @@
     python -m axhel_b200.workloads tensor   # fused tensor-product chain vs per-limb calls
     python -m axhel_b200.workloads uneven   # 512 uneven polynomials in one launch vs per-limb calls
     python -m axhel_b200.workloads serve    # Poisson arrivals at 50/70/90 % of capacity
+    python -m axhel_b200.workloads eltwise  # streaming eltwise kernels, GB/s at 2^24 elements
+    python -m axhel_b200.workloads case F   # a small case of kernel family F, for a profiler
 
 Each prints one JSON line.  Inputs are seeded synthetic residues (uniform in
 [0, f*q)), primes from the deterministic search of `params`.  GPU times are
@@ -367,9 +369,97 @@ def plain_sequential(rp, limit=16):
     return n_req / (time.perf_counter() - t0)
 
 
+# ------------------------------------------------------------------ kernels
+
+def eltwise_rates(n=1 << 24, reps=30):
+    """Algorithmic GB/s of the streaming eltwise kernels on 2^24-element
+    device vectors (128 MiB each, above the L2)."""
+    import torch
+
+    q = params.ntt_prime_near(1 << 16, 50, 1, 1)
+    rng = np.random.default_rng(1)
+    a, b, c = (_dev(rng.integers(0, q, n, dtype=np.uint64)) for _ in range(3))
+    big = _dev(rng.integers(0, 2**63, n, dtype=np.uint64))
+    r = torch.empty_like(a)
+    P = lambda t: t.data_ptr()
+    cases = [("add_vv", 24, lambda: capi.add(P(r), P(a), P(b), n, q)),
+             ("add_vs", 16, lambda: capi.add(P(r), P(a), 5, n, q, scalar=True)),
+             ("mul_f1", 24, lambda: capi.mul(P(r), P(a), P(b), n, q, 1)),
+             ("fma_f1", 24, lambda: capi.fma(P(r), P(a), 12345, P(c), n, q, 1)),
+             ("reduce_4to1", 16, lambda: capi.reduce(P(r), P(a), n, q, 4, 1)),
+             ("reduce_barrett", 16, lambda: capi.reduce(P(r), P(big), n, q, q, 1))]
+    out = {"elements": n, "unit": "GB/s (algorithmic bytes / CUDA-event time)"}
+    for name, bpe, fn in cases:
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = _events()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        out[name] = bpe * n / (e0.elapsed_time(e1) / reps / 1e3) / 1e9
+    return out
+
+
+def kernel_case(family):
+    """A small case of one kernel family, launched two or three times: the
+    command a profiler runs (inputs above the L2, a few hundred MB)."""
+    import torch
+
+    rng = np.random.default_rng(1)
+    if family == "eltwise":  # add, mul, fma, Barrett reduce on 2^24 elements, twice
+        n = 1 << 24
+        q = params.ntt_prime_near(1 << 16, 50, 1, 1)
+        a, b, c = (_dev(rng.integers(0, q, n, dtype=np.uint64)) for _ in range(3))
+        r = torch.empty_like(a)
+        for _ in range(2):
+            capi.add(r.data_ptr(), a.data_ptr(), b.data_ptr(), n, q)
+            capi.mul(r.data_ptr(), a.data_ptr(), b.data_ptr(), n, q, 1)
+            capi.fma(r.data_ptr(), a.data_ptr(), 12345, c.data_ptr(), n, q, 1)
+            capi.reduce(r.data_ptr(), a.data_ptr(), n, q, q, 1)
+    elif family == "tensor":  # 16 pairs x 16 limbs of N = 2^15
+        L, n, pairs = 16, 1 << 15, 16
+        qs = [q for q, _ in params.rns_moduli(n, L, 40, 55)]
+        cnt = pairs * L
+        ins = [_dev(np.concatenate([rng.integers(0, qs[i % L], n, dtype=np.uint64) for i in range(cnt)]))
+               for _ in range(4)]
+        outs = [torch.empty_like(ins[0]) for _ in range(3)]
+        for _ in range(2):
+            capi.tensor_product(*[o.data_ptr() for o in outs], *[x.data_ptr() for x in ins], n, cnt, qs, 1)
+    elif family == "tables":  # 3 x 24 fresh contexts of N = 2^16
+        for lo, hi in ((30, 40), (41, 51), (52, 62)):
+            capi.NTT.create_many([(1 << 16, q, psi) for q, psi in params.rns_moduli(1 << 16, 24, lo, hi)])
+    elif family in ("chain", "batch", "batch_eltwise"):  # 384 limbs of N = 2^16 (192 MiB), 24 moduli
+        n = 1 << 16
+        mods = params.rns_moduli(n, 24, 50, 59)
+        ntts = [capi.NTT(n, q, psi) for q, psi in mods]
+        x = _dev(np.concatenate([rng.integers(0, mods[i % 24][0], n, dtype=np.uint64) for i in range(384)]))
+        v = x.clone()
+        if family == "chain":  # INTT -> MulMod -> NTT, fused
+            for _ in range(2):
+                capi.chain_mul_batch(ntts, x.data_ptr(), x.data_ptr(), v.data_ptr(), 384, 2, 4)
+        elif family == "batch":  # one forward job, one persistent launch
+            b = capi.Batch([dict(kind=capi.JOB_FORWARD, ntts=ntts, count=384, result=x.data_ptr(),
+                                 operand=x.data_ptr(), in_f=4, out_f=4)])
+            for _ in range(3):
+                b.launch()
+        else:  # one MulMod job, one launch per phase
+            b = capi.Batch([dict(kind=capi.JOB_MUL, ntts=ntts, count=384, result=x.data_ptr(), operand=x.data_ptr(),
+                                 vector=v.data_ptr(), in_f=1, out_f=1)])
+            for _ in range(2):
+                b.launch(phased=True)
+    else:
+        raise SystemExit(f"unknown kernel family {family}")
+    torch.cuda.synchronize()
+    return {"case": family, "ok": True}
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["tensor", "uneven", "serve"])
+    ap.add_argument("what", choices=["tensor", "uneven", "serve", "eltwise", "case"])
+    ap.add_argument("family", nargs="?", default="eltwise",
+                    help="case: eltwise | tensor | tables | chain | batch | batch_eltwise")
     ap.add_argument("--seconds", type=float, default=4.0)
     ap.add_argument("--device", action="store_true", help="device-resident request operands")
     ap.add_argument("--persistent", action="store_true", help="one persistent launch per batch")
@@ -380,6 +470,10 @@ def main():
     a = ap.parse_args()
     if a.what == "tensor":
         out = tensor_chain()
+    elif a.what == "eltwise":
+        out = eltwise_rates()
+    elif a.what == "case":
+        out = kernel_case(a.family)
     elif a.what == "uneven":
         out = uneven_batch()
     else:
