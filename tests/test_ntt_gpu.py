@@ -267,3 +267,42 @@ def test_rejects_bad_arguments(cuda, oracle):
         cuda.NTT(1 << 18, 2 ** 61 - 1, 3)  # degree beyond the supported maximum
     with pytest.raises(cuda.AxhelError):
         cuda.NTT(8, 2 ** 62 + 1, 3)  # modulus too wide
+
+
+def schoolbook_negacyclic(a, b, q):
+    """Product in Z_q[x]/(x^n + 1) the quadratic way (test_polymul.cpp)."""
+    n = len(a)
+    A = [int(v) for v in a]
+    B = np.array([int(v) for v in b], dtype=object)
+    acc = np.zeros(2 * n, dtype=object)
+    for i in range(n):
+        acc[i:i + n] += A[i] * B
+    return np.array([(acc[k] - acc[k + n]) % q for k in range(n)], dtype=np.uint64)
+
+
+@pytest.mark.parametrize("n", [64, 256, 512])
+def test_polymul_matches_schoolbook(cuda, oracle, n):
+    """test_polymul.cpp:236-292 on the GPU path: ComputeForward on both
+    factors, EltwiseMulMod, ComputeInverse is the negacyclic product -- an
+    algorithm-independent check -- with lazy ([0,4q), MulMod factor 4) and
+    normalized forward outputs, widths up to 62 bits."""
+    st = oracle.rng(SEED ^ 0x504F4C59 ^ n)
+    for bits in (30, 50, 61, 62):
+        q, psi = ntt_params(oracle, n, bits)
+        t = cuda.NTT(n, q, psi)
+        a, b = oracle.random_vector(st, n, q), oracle.random_vector(st, n, q)
+        want = schoolbook_negacyclic(a, b, q)
+        da, db, dc = dev(a), dev(b), dev_empty(n)
+        t.forward(ptr(da), ptr(da), 1, 4)   # lazy forward outputs feed MulMod with factor 4
+        t.forward(ptr(db), ptr(db), 1, 4)
+        cuda.mul(ptr(dc), ptr(da), ptr(db), n, q, 4)
+        t.inverse(ptr(dc), ptr(dc), 1, 1)
+        np.testing.assert_array_equal(host(dc, n), want, err_msg=f"per call, q bits {bits}")
+        # normalized forward outputs, MulMod factor 1
+        A, B = dev(a), dev(b)
+        t.forward(ptr(A), ptr(A), 1, 1)
+        t.forward(ptr(B), ptr(B), 1, 1)
+        prod = dev_empty(n)
+        cuda.mul(ptr(prod), ptr(A), ptr(B), n, q, 1)  # dyadic product in the NTT domain
+        t.inverse(ptr(prod), ptr(prod), 1, 1)
+        np.testing.assert_array_equal(host(prod, n), want, err_msg=f"normalized, q bits {bits}")
