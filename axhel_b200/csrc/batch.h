@@ -17,8 +17,12 @@ constexpr int kBatchThreads = 128;
 constexpr int kBatchLR = 3;
 constexpr int kBatchTileWords = kBatchThreads << kBatchLR;  // 1024 residues
 constexpr int kBatchMinLG = 5, kBatchMaxLG = 9;
-// CTAs per SM the kernels are compiled for (96 registers; 128 without the bound)
-constexpr int kBatchMinBlocks = 5;
+// CTAs per SM the kernels are compiled for: 64 registers (128 without the
+// bound) and some spills, which cost less than the latency the extra resident
+// warps hide -- measured on the 512-polynomial uneven batch: 5 CTAs 1.08 M /
+// 1.28 M limb-transforms/s (persistent / per phase), 7 CTAs 1.25 M / 1.36 M,
+// 8 CTAs 1.29 M / 1.46 M.
+constexpr int kBatchMinBlocks = 8;
 
 enum BatchKind : uint32_t {
     kJobForward = 1, kJobInverse = 2, kJobChainMul = 3, kJobChainFma = 4,
