@@ -446,7 +446,7 @@ axhel_status_t chain(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* result,
         a.dst = result;
         a.s0 = s0;
         a.tg = (uint32_t)inv.pass[i].tg;
-        a.flags = (i == 0 && in_f == 4) ? kPreCsub2q : 0;
+        a.flags = (i == 0 && in_f == 4) ? (uint32_t)kPreCsub2q : 0u;
         cudaError_t e = launch_ntt_pass(true, inv.pass[i], a, s);
         if (e != cudaSuccess) return cuda_fail(e, "chain inverse pass");
         s0 += (uint32_t)inv.pass[i].lg;
@@ -462,7 +462,8 @@ axhel_status_t chain(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* result,
     c.pass.dst = result;
     c.pass.s0 = s0;
     c.pass.tg = (uint32_t)fc.tg;
-    c.pass.flags = (inv.npass == 1 && in_f == 4 ? kPreCsub2q : 0) | (fwd.npass == 1 && out_f != 4 ? kPostNorm : 0);
+    c.pass.flags = (inv.npass == 1 && in_f == 4 ? (uint32_t)kPreCsub2q : 0u) |
+                   (fwd.npass == 1 && out_f != 4 ? (uint32_t)kPostNorm : 0u);
     c.operand = vec;
     c.op = op;
     c.op_factor = 2;
@@ -478,7 +479,7 @@ axhel_status_t chain(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* result,
         a.dst = result;
         a.s0 = f0;
         a.tg = (uint32_t)fwd.pass[i].tg;
-        a.flags = (i == fwd.npass - 1) ? (kLastPass | (out_f != 4 ? kPostNorm : 0)) : 0;
+        a.flags = (i == fwd.npass - 1) ? ((uint32_t)kLastPass | (out_f != 4 ? (uint32_t)kPostNorm : 0u)) : 0u;
         e = launch_ntt_pass(false, fwd.pass[i], a, s);
         if (e != cudaSuccess) return cuda_fail(e, "chain forward pass");
         f0 += (uint32_t)fwd.pass[i].lg;

@@ -9,7 +9,7 @@
  * NULL = the legacy default stream).  Residues are uint64_t, moduli q < 2^62.
  *
  * Results are bit-identical to the reference native backend (AXHEL,
- * axhel/ntt/ntt-native.cpp and axhel/eltwise/*.cpp), including the lazy
+ * axhel/ntt/ntt-native.cpp and axhel/eltwise/eltwise-*-mod.cpp), including the lazy
  * representatives of forward output factor 4 ([0,4q)) and inverse output
  * factor 2 ([0,2q)).  Each entry point names the reference interface it
  * replaces (paths relative to the AXHEL project root).
