@@ -26,8 +26,8 @@
 // stops.  Data written by other CTAs of the launch is read through L2
 // (ld.global.cg), never through a possibly stale L1 line.  A finished tile
 // is published as a grid barrier publishes arrival: CTA barrier, then one
-// thread's device-scope fence and release increment (the fence is
-// cumulative over the stores the barrier ordered before it).
+// thread's device-scope release increment (cumulative over the stores the
+// barrier ordered before it).
 //
 // Each tile is 1024 residues handled by 128 threads x 8 registers
 // (LR = 3): 2^(10-LG) groups of 2^LG for the pass widths LG = 5..9 of the
@@ -199,11 +199,31 @@ __device__ __forceinline__ void run_tile(const BatchJob& j, uint32_t phase, uint
     }
 }
 
+// Last entry at or after `from` whose first tile is <= tile (tiles are
+// claimed in increasing order, so a CTA's next tile is at or after its
+// previous entry): gallop forward, then bisect.
+__device__ __forceinline__ uint32_t find_entry(const BatchArgs& a, uint64_t tile, uint32_t from)
+{
+    uint32_t lo = from, step = 1;
+    while (lo + step < a.nentries && a.entries[lo + step].tile_begin <= tile) {
+        lo += step;
+        step <<= 1;
+    }
+    uint32_t hi = lo + step < a.nentries ? lo + step : a.nentries;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (a.entries[mid].tile_begin <= tile) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
 __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks) batch_kernel(const __grid_constant__ BatchArgs a)
 {
     __shared__ uint64_t sm[kBatchTileWords + 128];
     __shared__ unsigned long long s_tile[2];
+    __shared__ uint32_t s_entry;
     __shared__ int s_abort;
+    uint32_t entry = 0;  // thread 0: entry of the CTA's latest tile
     if (threadIdx.x == 0) {
         s_tile[0] = atomicAdd(a.next_tile, 1ull);
         s_abort = 0;
@@ -213,42 +233,44 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks) batch_kernel(c
         const uint64_t tile = s_tile[it & 1];
         if (tile >= a.total_tiles) break;
         unsigned long long nxt = 0;  // the next tile, claimed now, announced after this one
-        if (threadIdx.x == 0) nxt = atomicAdd(a.next_tile, 1ull);
-        // (job, phase) of this tile: last entry with tile_begin <= tile
-        uint32_t lo = 0, hi = a.nentries;
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (a.entries[mid].tile_begin <= tile) lo = mid; else hi = mid;
+        if (threadIdx.x == 0) {
+            nxt = atomicAdd(a.next_tile, 1ull);
+            entry = find_entry(a, tile, entry);
+            s_entry = entry;
+            const BatchEntry e = a.entries[entry];
+            if (e.phase > 0) {
+                const BatchJob& j = a.jobs[e.job];
+                const uint64_t limb = (tile - e.tile_begin) / j.tiles_per_limb[e.phase];
+                cuda::atomic_ref<unsigned int, cuda::thread_scope_device> dep(
+                    a.done[j.done_off + (uint64_t)(e.phase - 1) * j.count + limb]);
+                const unsigned need = j.tiles_per_limb[e.phase - 1] + j.wait_extra;
+                const uint64_t t0 = global_ns();
+                uint32_t polls = 0;
+                while (dep.load(cuda::memory_order_acquire) < need) {
+                    // bounded in wall time and in polls
+                    if (++polls > (1u << 24) || global_ns() - t0 > a.wait_ns) {
+                        atomicExch(a.error, AXHEL_ERR_TIMEOUT);
+                        s_abort = 1;
+                        break;
+                    }
+                    __nanosleep(100);
+                }
+            }
         }
-        const BatchEntry e = a.entries[lo];
+        __syncthreads();
+        if (s_abort) break;
+        const BatchEntry e = a.entries[s_entry];
         const BatchJob& j = a.jobs[e.job];
         const uint64_t lt = tile - e.tile_begin;
         const uint32_t tpl = j.tiles_per_limb[e.phase];
         const uint64_t limb = lt / tpl;
         const uint64_t til = lt - limb * tpl;
-        if (e.phase > 0 && threadIdx.x == 0) {
-            cuda::atomic_ref<unsigned int, cuda::thread_scope_device> dep(
-                a.done[j.done_off + (uint64_t)(e.phase - 1) * j.count + limb]);
-            const unsigned need = j.tiles_per_limb[e.phase - 1] + j.wait_extra;
-            const uint64_t t0 = global_ns();
-            uint32_t polls = 0;
-            while (dep.load(cuda::memory_order_acquire) < need) {
-                // bounded in wall time and in polls
-                if (++polls > (1u << 24) || global_ns() - t0 > a.wait_ns) {
-                    atomicExch(a.error, AXHEL_ERR_TIMEOUT);
-                    s_abort = 1;
-                    break;
-                }
-                __nanosleep(100);
-            }
-        }
-        __syncthreads();
-        if (s_abort) break;
         run_tile(j, e.phase, limb, til, sm);
         if (threadIdx.x == 0) s_tile[(it + 1) & 1] = nxt;
         __syncthreads();
         if (threadIdx.x == 0 && e.phase + 1 < j.nphase) {
-            __threadfence();
+            // release at device scope, cumulative over the stores the barrier
+            // ordered before it
             cuda::atomic_ref<unsigned int, cuda::thread_scope_device> done(
                 a.done[j.done_off + (uint64_t)e.phase * j.count + limb]);
             done.fetch_add(1u, cuda::memory_order_release);
