@@ -15,8 +15,10 @@
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "../../include/axhel/axhel.hpp"
+#include "../../include/axhel/ntt/ntt-rns.hpp"
 #include "../../include/axhel_cuda.h"
 
 namespace unipi {
@@ -231,6 +233,60 @@ void NTT::ComputeInverse(uint64_t* result, const uint64_t* operand, uint64_t inp
 
 uint64_t NTT::Degree() const noexcept { return impl_ ? impl_->degree : 0; }
 uint64_t NTT::Modulus() const noexcept { return impl_ ? impl_->modulus : 0; }
+
+// ------------------------------------------------------------- RNS batches
+
+namespace detail {
+struct NTTAccess {
+    static axhel_ntt_t handle(const NTT& t) { return t.impl_ ? t.impl_->handle : nullptr; }
+};
+}  // namespace detail
+
+namespace {
+
+std::vector<axhel_ntt_t> rns_handles(const NTT* ntts, size_t n_ntts, uint64_t* degree)
+{
+    if (!ntts || n_ntts == 0 || n_ntts > 64) throw std::invalid_argument("AXHEL RNS transform: 1..64 NTT objects");
+    std::vector<axhel_ntt_t> hs(n_ntts);
+    *degree = ntts[0].Degree();
+    for (size_t i = 0; i < n_ntts; ++i) {
+        hs[i] = detail::NTTAccess::handle(ntts[i]);
+        if (!hs[i] || ntts[i].Degree() != *degree)
+            throw std::invalid_argument("AXHEL RNS transform: NTT objects of one degree needed");
+    }
+    return hs;
+}
+
+}  // namespace
+
+void ComputeForwardRNS(const NTT* ntts, size_t n_ntts, uint64_t* result, const uint64_t* operand, size_t count,
+                       uint64_t /*input_mod_factor*/, uint64_t output_mod_factor)
+{
+    if (count == 0) return;
+    uint64_t n = 0;
+    const std::vector<axhel_ntt_t> hs = rns_handles(ntts, n_ntts, &n);
+    const uint64_t words = (uint64_t)count * n;
+    Output out(result, words);
+    const uint64_t* a = input(operand, words, 0);
+    check(axhel_cuda_ntt_forward_batch(hs.data(), n_ntts, out.dev, a, count, 1, output_mod_factor, stream()),
+          "ComputeForwardRNS");
+    out.finish();
+}
+
+void ComputeInverseRNS(const NTT* ntts, size_t n_ntts, uint64_t* result, const uint64_t* operand, size_t count,
+                       uint64_t /*input_mod_factor*/, uint64_t output_mod_factor)
+{
+    if (count == 0) return;
+    uint64_t n = 0;
+    const std::vector<axhel_ntt_t> hs = rns_handles(ntts, n_ntts, &n);
+    const uint64_t words = (uint64_t)count * n;
+    Output out(result, words);
+    const uint64_t* a = input(operand, words, 0);
+    // input factor 2: the per-limb ComputeInverse's contract (inputs in [0, 2q)), no fused reduction
+    check(axhel_cuda_ntt_inverse_batch(hs.data(), n_ntts, out.dev, a, count, 2, output_mod_factor, stream()),
+          "ComputeInverseRNS");
+    out.finish();
+}
 
 }  // namespace axhel
 }  // namespace unipi

@@ -9,6 +9,8 @@
 namespace unipi {
 namespace axhel {
 
+    namespace detail { struct NTTAccess; }  // the batched functions of ntt-rns.hpp reach the device tables
+
     /// @brief A twiddle factor with its Shoup quotient floor(operand * 2^64 / q).
     struct NTTMultiplyOperand
     {
@@ -58,6 +60,7 @@ namespace axhel {
         uint64_t Modulus() const noexcept;
 
     private:
+        friend struct detail::NTTAccess;
         class Impl;
 
         std::shared_ptr<Impl> impl_;

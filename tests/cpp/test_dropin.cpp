@@ -5,6 +5,7 @@
 // test_polymul.cpp against the C oracle (oracle/axhel_oracle.c, linked in).
 // Built and run by tests/test_dropin_gpu.py; exits non-zero on any mismatch.
 #include <axhel/axhel.hpp>
+#include <axhel/ntt/ntt-rns.hpp>
 
 #include <cuda_runtime.h>
 
@@ -246,6 +247,60 @@ static void test_threads_share_one_ntt()
     for (int k = 0; k < 8; ++k) CHECK(ok[k], "thread %d", k);
 }
 
+static void test_rns_batches()
+{
+    // One call per polynomial instead of one per limb (ntt-rns.hpp): equal to
+    // the per-limb calls, host and device pointers, in and out of place.
+    const uint64_t n = 4096;
+    const size_t L = 5, count = 3 * L;
+    std::vector<NTT> ntts;
+    std::vector<uint64_t> qs;
+    for (size_t i = 0; i < L; ++i) {
+        const uint64_t q = orc_find_ntt_prime_near(n, 40 + 4 * (unsigned)i, 1, 2);
+        qs.push_back(q);
+        ntts.emplace_back(n, q, orc_find_primitive_root(n, q));
+    }
+    uint64_t st[313];
+    orc_mt64_seed(st, kSeed ^ 0x524E53);
+    Vec x(count * n);
+    for (size_t i = 0; i < count; ++i) {
+        Vec v = rand_vec(st, n, 4 * qs[i % L]);
+        std::copy(v.begin(), v.end(), x.begin() + i * n);
+    }
+    for (uint64_t out_f : {1, 4}) {
+        Vec want(count * n), got(count * n), inplace = x;
+        for (size_t i = 0; i < count; ++i)
+            ntts[i % L].ComputeForward(want.data() + i * n, x.data() + i * n, 4, out_f);
+        unipi::axhel::ComputeForwardRNS(ntts.data(), L, got.data(), x.data(), count, 4, out_f);
+        CHECK(got == want, "ComputeForwardRNS out_f=%llu", (unsigned long long)out_f);
+        unipi::axhel::ComputeForwardRNS(ntts.data(), L, inplace.data(), inplace.data(), count, 4, out_f);
+        CHECK(inplace == want, "ComputeForwardRNS in place out_f=%llu", (unsigned long long)out_f);
+        for (uint64_t inv_out : {1, 2}) {
+            Vec iwant(count * n), igot(count * n);
+            Vec lazy2 = want;  // inverse inputs in [0, 2q)
+            for (size_t i = 0; i < count; ++i)
+                for (size_t k = 0; k < n; ++k) {
+                    uint64_t& v = lazy2[i * n + k];
+                    if (v >= 2 * qs[i % L]) v -= 2 * qs[i % L];
+                }
+            for (size_t i = 0; i < count; ++i)
+                ntts[i % L].ComputeInverse(iwant.data() + i * n, lazy2.data() + i * n, 2, inv_out);
+            unipi::axhel::ComputeInverseRNS(ntts.data(), L, igot.data(), lazy2.data(), count, 2, inv_out);
+            CHECK(igot == iwant, "ComputeInverseRNS out_f=%llu", (unsigned long long)inv_out);
+        }
+    }
+    // device pointers: used in place, no staging
+    uint64_t* d = nullptr;
+    cudaMalloc(&d, count * n * 8);
+    cudaMemcpy(d, x.data(), count * n * 8, cudaMemcpyHostToDevice);
+    unipi::axhel::ComputeForwardRNS(ntts.data(), L, d, d, count, 4, 4);
+    Vec back(count * n), want(count * n);
+    cudaMemcpy(back.data(), d, count * n * 8, cudaMemcpyDeviceToHost);
+    unipi::axhel::ComputeForwardRNS(ntts.data(), L, want.data(), x.data(), count, 4, 4);
+    CHECK(back == want, "ComputeForwardRNS on device pointers");
+    cudaFree(d);
+}
+
 int main()
 {
     test_known_vector();
@@ -256,6 +311,7 @@ int main()
     test_polymul();
     test_device_pointers();
     test_threads_share_one_ntt();
+    test_rns_batches();
     if (g_fail) {
         std::fprintf(stderr, "%d failure(s)\n", g_fail);
         return 1;
