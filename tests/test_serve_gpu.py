@@ -210,3 +210,23 @@ def test_eltwise_requests_alone_and_in_a_mix(cuda, oracle):
         d = dev(r["x"])
         srv.submit(7, r["ntts"], r["count"], ptr(d), ptr(d), vector=ptr(d), in_f=3, out_f=1)
     srv.close()
+
+
+def test_pageable_host_buffers(cuda, oracle):
+    """Requests on ordinary (pageable, unpinned) host memory: same results;
+    the copies are simply not asynchronous."""
+    reqs = make_requests(cuda, oracle, 23, SPECS[:4])
+    srv = cuda.Server(budget_bytes=4 << 30, max_inflight=2, max_batch_requests=8)
+    outs, ids = [], []
+    for r in reqs:
+        x = np.ascontiguousarray(r["x"])
+        v = np.ascontiguousarray(r["v"])
+        o = np.zeros_like(x)
+        outs.append((x, v, o))
+        ids.append(srv.submit(r["kind"], r["ntts"], r["count"], x.ctypes.data, o.ctypes.data, vector=v.ctypes.data,
+                              scalars=r["sc"] if r["kind"] == 4 else None, in_f=2, out_f=4))
+    for rid, r, (x, v, o) in zip(ids, reqs, outs):
+        st, _ = srv.wait(rid)
+        assert st == 0
+        np.testing.assert_array_equal(o, expected(oracle, r))
+    srv.close()
