@@ -47,7 +47,9 @@ def test_cpp_dropin_symbols_exported():
                 "unipi::axhel::NTT::NTT(unsigned long, unsigned long, unsigned long)",
                 "unipi::axhel::NTT::NTT(unsigned long, unsigned long, unipi::axhel::NTTMultiplyOperand const*",
                 "unipi::axhel::NTT::ComputeForward(", "unipi::axhel::NTT::ComputeInverse(",
-                "unipi::axhel::NTT::Degree() const", "unipi::axhel::NTT::Modulus() const"):
+                "unipi::axhel::NTT::Degree() const", "unipi::axhel::NTT::Modulus() const",
+                "unipi::axhel::ComputeForwardRNS(unipi::axhel::NTT const*",
+                "unipi::axhel::ComputeInverseRNS(unipi::axhel::NTT const*"):
         assert sig in out, sig
 
 
