@@ -21,6 +21,7 @@
 // A request's result is computed by the same kernel code whether it runs
 // alone or in a mix, so it is bit-identical either way.
 #include <cuda_runtime.h>
+#include <sys/prctl.h>
 
 #include <algorithm>
 #include <cmath>
@@ -53,6 +54,11 @@ axhel_status_t sfail(axhel_status_t st, const std::string& m)
 }
 
 constexpr int kPending = -1, kRunning = -2;
+
+// The server's threads sleep in short waits (the completer's poll); Linux
+// stretches every such sleep by the thread's timer slack, 50 us by default,
+// which would land in each request's latency.
+void tighten_timer_slack() { prctl(PR_SET_TIMERSLACK, 1000UL, 0, 0, 0); }
 constexpr size_t kStagingBytes = 1 << 20;  // pinned descriptor staging per slot at creation
 
 bool is_device(const void* p) { return p && axhel_cuda_is_device_pointer(p); }
@@ -234,6 +240,7 @@ axhel_status_t axhel_server::launch(Slot& s, int slot_index, std::vector<Req*>& 
 void axhel_server::scheduler()
 {
     cudaSetDevice(device);
+    tighten_timer_slack();
     std::unique_lock<std::mutex> lk(mu);
     auto free_slot = [&](int lane) {
         for (size_t i = 0; i < slots.size(); ++i)
@@ -312,6 +319,7 @@ void axhel_server::scheduler()
 void axhel_server::completer()
 {
     cudaSetDevice(device);
+    tighten_timer_slack();
     std::unique_lock<std::mutex> lk(mu);
     for (;;) {
         cv_done.wait(lk, [&] { return !inflight.empty() || stop; });
@@ -621,6 +629,10 @@ axhel_status_t axhel_server_drive(axhel_server_t server, const axhel_request_t* 
         x ^= x >> 27;
         return ((x * 0x2545F4914F6CDD1Dull) >> 11) * (1.0 / 9007199254740992.0) + 1e-18;
     };
+    // arrivals on time: this (the caller's) thread sleeps with a 1 us timer
+    // slack while it produces them, and gets its own back afterwards
+    const int old_slack = prctl(PR_GET_TIMERSLACK, 0, 0, 0, 0);
+    tighten_timer_slack();
     const auto t0 = Clock::now();
     const auto end = t0 + std::chrono::duration<double>(seconds);
     auto t = t0;
@@ -656,6 +668,7 @@ axhel_status_t axhel_server_drive(axhel_server_t server, const axhel_request_t* 
         lv.notify_all();
     }
     collector.join();
+    if (old_slack > 0) prctl(PR_SET_TIMERSLACK, (unsigned long)old_slack, 0, 0, 0);
     const double wall = std::chrono::duration<double>(Clock::now() - t0).count();
     auto pct = [](std::vector<double> v, double p) {
         if (v.empty()) return 0.0;
