@@ -197,30 +197,45 @@ struct TensorArgs {
 
 // Per element of limb i (modulus m[i % nmod]):
 //   r0 = Mul(c0,d0); r1 = Add(Mul(c0,d1), Mul(c1,d0)); r2 = Mul(c1,d1)
-// with EltwiseMulMod<F> / EltwiseAddMod semantics; the trailing
-// EltwiseReduceMod(4,1) is the identity on these canonical values.
+// with EltwiseMulMod<F> / EltwiseAddMod semantics (canonical results, so the
+// middle term's evaluation order is free); the trailing EltwiseReduceMod(4,1)
+// is the identity on these canonical values.
 template <int F>
 __global__ void __launch_bounds__(256) tensor_product_kernel(const __grid_constant__ TensorArgs a)
 {
     // grid: x = chunks of one limb, y = limb.  Two elements per thread step.
     const uint64_t limb = blockIdx.y;
     const ModConst mc = a.m[limb % a.nmod];
-    const OpMul<F> mul{mc.q, mc.mu, mc.shift};
-    const OpAddVV add{mc.q};
+    const uint64_t q = mc.q;
+    const OpMul<1> mul{q, mc.mu, mc.shift};  // on inputs already reduced to [0, q)
+    const OpAddVV add{q};
+    const OpSubVV sub{q};
     const uint64_t off = limb * a.n;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x * 2;
+    // Every output is a canonical residue, so the middle term may be formed
+    // as (c0 + c1)(d0 + d1) - c0 d0 - c1 d1: three Barrett products per
+    // coefficient instead of four, the same bits.
+    auto three = [&](uint64_t c0, uint64_t c1, uint64_t d0, uint64_t d1, uint64_t& r0, uint64_t& r1,
+                     uint64_t& r2) {
+        c0 = reduce_input<F>(c0, q);
+        c1 = reduce_input<F>(c1, q);
+        d0 = reduce_input<F>(d0, q);
+        d1 = reduce_input<F>(d1, q);
+        r0 = mul(c0, d0);
+        r2 = mul(c1, d1);
+        r1 = sub(sub(mul(add(c0, c1), add(d0, d1)), r0), r2);
+    };
     for (uint64_t e = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * 2; e < a.n; e += stride) {
         const ulonglong2 x0 = *reinterpret_cast<const ulonglong2*>(a.c0 + off + e);
         const ulonglong2 x1 = *reinterpret_cast<const ulonglong2*>(a.c1 + off + e);
         const ulonglong2 y0 = *reinterpret_cast<const ulonglong2*>(a.d0 + off + e);
         const ulonglong2 y1 = *reinterpret_cast<const ulonglong2*>(a.d1 + off + e);
-        ulonglong2 o0, o1, o2;
-        o0.x = mul(x0.x, y0.x);
-        o0.y = mul(x0.y, y0.y);
-        o1.x = add(mul(x0.x, y1.x), mul(x1.x, y0.x));
-        o1.y = add(mul(x0.y, y1.y), mul(x1.y, y0.y));
-        o2.x = mul(x1.x, y1.x);
-        o2.y = mul(x1.y, y1.y);
+        uint64_t r[2][3];
+        three(x0.x, x1.x, y0.x, y1.x, r[0][0], r[0][1], r[0][2]);
+        three(x0.y, x1.y, y0.y, y1.y, r[1][0], r[1][1], r[1][2]);
+        const ulonglong2 o0 = make_ulonglong2(r[0][0], r[1][0]);
+        const ulonglong2 o1 = make_ulonglong2(r[0][1], r[1][1]);
+        const ulonglong2 o2 = make_ulonglong2(r[0][2], r[1][2]);
         *reinterpret_cast<ulonglong2*>(a.r0 + off + e) = o0;
         *reinterpret_cast<ulonglong2*>(a.r1 + off + e) = o1;
         *reinterpret_cast<ulonglong2*>(a.r2 + off + e) = o2;
