@@ -312,6 +312,24 @@ def run_ours(args):
         e2e["h2d_bytes_per_step"] *= world
         e2e["d2h_bytes_per_step"] *= world
 
+    # ---- the other configurations' workloads, once each, bit-checked against
+    # their per-limb call sequences: the fused tensor product (C3) and the
+    # 512-polynomial uneven batch (C4)
+    others = None
+    if rank == 0 and not args.no_others:
+        from axhel_b200 import workloads
+
+        t = workloads.tensor_chain()
+        u = workloads.uneven_batch()
+        others = {
+            "tensor_product": {"workload": t["workload"], "ms": t["fused_ms"], "GBps": t["fused_GBps"],
+                               "per_limb_calls_ms": t["per_limb_calls_ms"], "speedup": t["speedup"],
+                               "same_bits": t["same_bits"]},
+            "uneven_batch": {"workload": u["workload"], "limb_transforms": u["limb_transforms"],
+                             "persistent_rate": u["one_launch_rate"], "phased_rate": u["phased_rate"],
+                             "per_limb_rate": u["per_limb_rate"], "unit": u["unit"], "same_bits": u["same_bits"]},
+        }
+
     # ---- serving loop (continuous batching) at 70 % of its measured capacity:
     # host-staged requests (copies in the loop) and device-resident ones
     serve = None
@@ -359,6 +377,7 @@ def run_ours(args):
             "plain_per_limb": plain,
             "e2e": e2e,
             "serve": serve,
+            "configs": others,
             "tables": {"contexts": len(mods), "degree": N, "device_ms": tables_ms,
                        "reference_cpu_ms": cpu["tables_ms"] if cpu and "tables_ms" in cpu else None,
                        "note": "cold start: twiddle tables of the 24 moduli, device generation (one launch, "
@@ -474,6 +493,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU-baseline sample length")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop measurement")
+    ap.add_argument("--no-others", action="store_true", help="skip the tensor-product and uneven-batch workloads")
     ap.add_argument("--profile-step", action="store_true",
                     help="warm up, run one step and exit (the command profiled by ncu)")
     args = ap.parse_args()
