@@ -40,8 +40,10 @@
 
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/axhel_cuda.h"
@@ -98,7 +100,7 @@ __device__ __forceinline__ void run_tile_lg(const BatchJob& j, const PhaseCfg& c
                                             uint64_t tile_in_limb, uint64_t* sm)
 {
     constexpr uint32_t lgtg = 10 - LG;  // 1024 / 2^LG groups per tile
-    const uint32_t mi = (uint32_t)(limb % j.nmods);
+    const uint32_t mi = limb_mod(limb, j.nmods);
     const ModCtx* cx = j.ctx[mi];
     const bool first = p == 0, last = p + 1 == j.nphase;
     const uint64_t* src = first ? j.src : j.dst;
@@ -150,7 +152,7 @@ __device__ __forceinline__ void elt_fma(const BatchJob& j, uint64_t base, uint64
 // The element-wise job's op on one tile, with limb `limb`'s modulus.
 __device__ __forceinline__ void run_elt_tile(const BatchJob& j, uint64_t limb, uint64_t til)
 {
-    const uint32_t mi = (uint32_t)(limb % j.nmods);
+    const uint32_t mi = limb_mod(limb, j.nmods);
     const ModCtx* cx = j.ctx[mi];
     const uint64_t q = cx->q, mu = cx->mu;
     const uint32_t sh = cx->shift;
@@ -240,7 +242,7 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks) batch_kernel(c
             const BatchEntry e = a.entries[entry];
             if (e.phase > 0) {
                 const BatchJob& j = a.jobs[e.job];
-                const uint64_t limb = (tile - e.tile_begin) / j.tiles_per_limb[e.phase];
+                const uint64_t limb = (tile - e.tile_begin) >> (j.logn - kBatchTileLog);
                 cuda::atomic_ref<unsigned int, cuda::thread_scope_device> dep(
                     a.done[j.done_off + (uint64_t)(e.phase - 1) * j.count + limb]);
                 const unsigned need = j.tiles_per_limb[e.phase - 1] + j.wait_extra;
@@ -262,10 +264,9 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks) batch_kernel(c
         const BatchEntry e = a.entries[s_entry];
         const BatchJob& j = a.jobs[e.job];
         const uint64_t lt = tile - e.tile_begin;
-        const uint32_t tpl = j.tiles_per_limb[e.phase];
-        const uint64_t limb = lt / tpl;
-        const uint64_t til = lt - limb * tpl;
-        run_tile(j, e.phase, limb, til, sm);
+        const uint32_t lgt = j.logn - kBatchTileLog;  // tiles per limb: a power of two
+        const uint64_t limb = lt >> lgt;
+        run_tile(j, e.phase, limb, lt & ((1ull << lgt) - 1), sm);
         if (threadIdx.x == 0) s_tile[(it + 1) & 1] = nxt;
         __syncthreads();
         if (threadIdx.x == 0 && e.phase + 1 < j.nphase) {
@@ -278,25 +279,63 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks) batch_kernel(c
     }
 }
 
-// One phase of a batch as an ordinary launch: CTA b runs global tile
-// first + b.  Tiles of earlier phases were finished by earlier launches.
-__global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks) batch_phase_kernel(const __grid_constant__ BatchArgs a,
-                                                                    uint64_t first)
+// One tile of class CLS and pass width LG with LR register stages: the body
+// of run_tile_lg with the class fixed at compile time.  The strided and
+// contiguous passes take 64 threads x 16 registers per 1024-residue tile
+// when LR = 4.
+template <int CLS, int LG, int LR>
+__device__ __forceinline__ void run_tile_cls(const BatchJob& j, uint32_t p, uint64_t limb, uint64_t tile_in_limb,
+                                             uint64_t* sm)
+{
+    constexpr uint32_t lgtg = 10 - LG;
+    const uint32_t mi = limb_mod(limb, j.nmods);
+    const ModCtx* cx = j.ctx[mi];
+    const bool first = p == 0, last = p + 1 == j.nphase;
+    const uint64_t* src = first ? j.src : j.dst;
+    uint32_t flags = (first && j.pre) ? kPreCsub2q : 0;
+    if (last) flags |= kLastPass | (j.norm ? kPostNorm : 0);
+    const PhaseCfg c = phase_cfg(j, p);
+    if constexpr (CLS == kClsChain) {
+        const uint32_t op = j.kind == kJobChainMul ? kChainMul : kChainFma;
+        const uint64_t sc = j.kind == kJobChainFma ? j.scalars[mi] : 0;
+        chain_tile<LG, LR, true>(src, j.dst, j.vec, cx, op, sc, j.logn, lgtg, limb, tile_in_limb,
+                                 (first && j.pre ? kPreCsub2q : 0) | (last && j.norm ? kPostNorm : 0), sm);
+    } else if constexpr (CLS == kClsInv) {
+        const uint32_t f = flags | (c.s0 + LG == j.logn ? kLastPass : 0);
+        pass_tile<true, LG, LR, true>(src, j.dst, cx, j.logn, c.s0, lgtg, limb, tile_in_limb, f, sm);
+    } else {
+        pass_tile<false, LG, LR, true>(src, j.dst, cx, j.logn, c.s0, lgtg, limb, tile_in_limb, flags, sm);
+    }
+}
+
+template <int CLS, int LR>
+constexpr int class_min_blocks()
+{
+    return CLS == kClsChain ? 6 : (LR == 4 ? (CLS == kClsInv ? 12 : 16) : kBatchMinBlocks);
+}
+
+// One class launch: CTA b runs the class's tile b (entries in tile order).
+template <int CLS, int LG, int LR>
+__global__ void __launch_bounds__(kBatchTileWords >> LR, class_min_blocks<CLS, LR>())
+    batch_class_kernel(const __grid_constant__ BatchArgs a, const ClassEntry* __restrict__ ce, uint32_t n_ce)
 {
     __shared__ uint64_t sm[kBatchTileWords + 128];
-    const uint64_t tile = first + blockIdx.x;
-    uint32_t lo = 0, hi = a.nentries;
+    const uint64_t t = blockIdx.x;
+    uint32_t lo = 0, hi = n_ce;
     while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
-        if (a.entries[mid].tile_begin <= tile) lo = mid; else hi = mid;
+        if (ce[mid].tile0 <= t) lo = mid; else hi = mid;
     }
-    const BatchEntry e = a.entries[lo];
+    const BatchEntry e = a.entries[ce[lo].entry];
     const BatchJob& j = a.jobs[e.job];
-    const uint64_t lt = tile - e.tile_begin;
-    const uint32_t tpl = j.tiles_per_limb[e.phase];
-    const uint64_t limb = lt / tpl;
-    const uint64_t til = lt - limb * tpl;
-    run_tile(j, e.phase, limb, til, sm);
+    const uint64_t lt = t - ce[lo].tile0;
+    const uint32_t lgt = j.logn - kBatchTileLog;  // tiles per limb: a power of two
+    const uint64_t limb = lt >> lgt;
+    const uint64_t til = lt & ((1ull << lgt) - 1);
+    if constexpr (CLS == kClsElt)
+        run_elt_tile(j, limb, til);
+    else
+        run_tile_cls<CLS, LG, LR>(j, e.phase, limb, til, sm);
 }
 
 }  // namespace axhel_impl
@@ -311,7 +350,7 @@ struct axhel_batch {
     size_t bytes = 0;
     size_t zero_off = 0, zero_bytes = 0;  // counters cleared before every launch
     BatchArgs args{};
-    uint64_t phase_begin[4] = {0, 0, 0, 0};  // first global tile of each phase, and the total
+    std::vector<ClassLaunch> classes;        // the per-phase launches
     unsigned grid = 0;
     std::vector<axhel_ntt_t> held;  // table contexts kept alive while the batch exists
     cudaGraphExec_t graph = nullptr;
@@ -455,7 +494,7 @@ axhel_status_t batch_check_job(const axhel_job_t& J, const std::string& who, std
 // entry points.
 axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned char* base,
                            std::vector<unsigned char>& host, size_t* zero_off, size_t* zero_bytes, BatchArgs* args,
-                           std::vector<axhel_ntt_t>* held, std::string* err, uint64_t* phase_begin)
+                           std::vector<axhel_ntt_t>* held, std::string* err, std::vector<ClassLaunch>* classes)
 {
     if (!jobs || n_jobs == 0) {
         *err = "empty batch";
@@ -540,18 +579,53 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
     std::vector<BatchEntry> ent;
     uint64_t tiles = 0;
     for (uint32_t p = 0; p < 3; ++p) {
-        if (phase_begin) phase_begin[p] = tiles;
         for (uint64_t i = 0; i < n_jobs; ++i) {
             if (p >= bj[i].nphase || bj[i].count == 0) continue;
             ent.push_back(BatchEntry{tiles, (uint32_t)i, p});
             tiles += bj[i].count * bj[i].tiles_per_limb[p];
         }
     }
-    if (phase_begin) phase_begin[3] = tiles;
+    if (classes) classes->clear();
     if (ent.empty()) {
         *err = "";
         args->total_tiles = 0;
         return AXHEL_OK;
+    }
+    // per (phase, class, pass width): the entries, in order, with their
+    // first tile in that launch's numbering
+    std::vector<ClassLaunch> cl;
+    std::vector<std::vector<ClassEntry>> cl_ent;
+    if (classes) {
+        std::map<std::tuple<uint32_t, uint32_t, uint32_t>, size_t> at;
+        for (uint32_t k = 0; k < (uint32_t)ent.size(); ++k) {
+            const BatchEntry& e = ent[k];
+            const BatchJob& b = bj[e.job];
+            uint32_t cls, lg;
+            if (b.kind >= kJobAdd) {
+                cls = kClsElt;
+                lg = 0;
+            } else if (b.kind == kJobForward) {
+                cls = kClsFwd;
+                lg = e.phase == 0 ? b.lg_col : b.lg_row;
+            } else if (b.kind == kJobInverse) {
+                cls = kClsInv;
+                lg = e.phase == 0 ? b.lg_row : b.lg_col;
+            } else {  // chain: inverse row pass, fused column pass, forward row pass
+                cls = e.phase == 0 ? kClsInv : (e.phase == 1 ? kClsChain : kClsFwd);
+                lg = e.phase == 1 ? b.lg_col : b.lg_row;
+            }
+            const auto key = std::make_tuple(e.phase, cls, lg);
+            auto it = at.find(key);
+            if (it == at.end()) {
+                it = at.emplace(key, cl.size()).first;
+                cl.push_back(ClassLaunch{e.phase, cls, lg, 0, nullptr, 0});
+                cl_ent.emplace_back();
+            }
+            ClassLaunch& L = cl[it->second];
+            cl_ent[it->second].push_back(ClassEntry{L.tiles, k, 0});
+            L.tiles += b.count * b.tiles_per_limb[e.phase];
+            ++L.n_ce;
+        }
     }
     // device image
     size_t off = 0;
@@ -567,6 +641,12 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
             sc_off[i] = off;
             off = align_up(off + scal[i].size() * 8, 16);
         }
+    }
+    std::vector<size_t> ce_off(cl.size());
+    for (size_t c = 0; c < cl.size(); ++c) {
+        off = align_up(off, 16);
+        ce_off[c] = off;
+        off += cl_ent[c].size() * sizeof(ClassEntry);
     }
     off = align_up(off, 256);
     *zero_off = off;
@@ -586,6 +666,16 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
     }
     std::memcpy(host.data() + jobs_off, bj.data(), n_jobs * sizeof(BatchJob));
     std::memcpy(host.data() + ent_off, ent.data(), ent.size() * sizeof(BatchEntry));
+    for (size_t c = 0; c < cl.size(); ++c) {
+        std::memcpy(host.data() + ce_off[c], cl_ent[c].data(), cl_ent[c].size() * sizeof(ClassEntry));
+        cl[c].ce = reinterpret_cast<const ClassEntry*>(base + ce_off[c]);
+    }
+    if (classes) {
+        // phase by phase (the map numbered them in first-seen order, which is
+        // already phase-major)
+        std::stable_sort(cl.begin(), cl.end(), [](const ClassLaunch& x, const ClassLaunch& y) { return x.phase < y.phase; });
+        *classes = cl;
+    }
     args->jobs = reinterpret_cast<const BatchJob*>(base + jobs_off);
     args->entries = reinterpret_cast<const BatchEntry*>(base + ent_off);
     args->nentries = (uint32_t)ent.size();
@@ -597,15 +687,50 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
     return AXHEL_OK;
 }
 
-cudaError_t batch_launch_phases(const BatchArgs& a, const uint64_t* phase_begin, cudaStream_t s)
+namespace {
+
+using ClassFn = void (*)(const BatchArgs, const ClassEntry*, uint32_t);
+
+struct ClassKernel {
+    ClassFn fn = nullptr;
+    unsigned threads = 0;
+};
+
+// Register depth per class and width: 4 (64 threads per tile) for the
+// transform passes narrower than 9 stages, 3 (128 threads) otherwise.
+template <int CLS, int LG>
+ClassKernel class_kernel()
 {
-    for (int p = 0; p < 3; ++p) {
-        const uint64_t n = phase_begin[p + 1] - phase_begin[p];
-        if (n == 0) continue;
-        if (n > 0x7fffffffull) return cudaErrorInvalidValue;
+    constexpr int LR = (CLS == kClsFwd || CLS == kClsInv) && LG < 9 ? 4 : 3;
+    return ClassKernel{batch_class_kernel<CLS, LG, LR>, (unsigned)(kBatchTileWords >> LR)};
+}
+
+ClassKernel pick_class_kernel(uint32_t cls, uint32_t lg)
+{
+    if (cls == kClsElt) return class_kernel<kClsElt, 5>();
+    if (lg < (uint32_t)kBatchMinLG || lg > (uint32_t)kBatchMaxLG) return ClassKernel{};
+    static const ClassKernel table[3][5] = {
+        {class_kernel<kClsFwd, 5>(), class_kernel<kClsFwd, 6>(), class_kernel<kClsFwd, 7>(), class_kernel<kClsFwd, 8>(),
+         class_kernel<kClsFwd, 9>()},
+        {class_kernel<kClsInv, 5>(), class_kernel<kClsInv, 6>(), class_kernel<kClsInv, 7>(), class_kernel<kClsInv, 8>(),
+         class_kernel<kClsInv, 9>()},
+        {class_kernel<kClsChain, 5>(), class_kernel<kClsChain, 6>(), class_kernel<kClsChain, 7>(),
+         class_kernel<kClsChain, 8>(), class_kernel<kClsChain, 9>()}};
+    return cls < 3 ? table[cls][lg - kBatchMinLG] : ClassKernel{};
+}
+
+}  // namespace
+
+cudaError_t batch_launch_classes(const BatchArgs& a, const std::vector<ClassLaunch>& classes, cudaStream_t s)
+{
+    for (const ClassLaunch& L : classes) {
+        if (L.tiles == 0) continue;
+        if (L.tiles > 0x7fffffffull) return cudaErrorInvalidValue;
+        const ClassKernel k = pick_class_kernel(L.cls, L.lg);
+        if (!k.fn) return cudaErrorInvalidValue;
         count_launch();
-        ProfScope prof(s, "batch_phase_kernel");
-        batch_phase_kernel<<<(unsigned)n, kBatchThreads, 0, s>>>(a, phase_begin[p]);
+        ProfScope prof(s, "batch_class_kernel cls=%u lg=%u", L.cls, L.lg);
+        k.fn<<<(unsigned)L.tiles, k.threads, 0, s>>>(a, L.ce, L.n_ce);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
@@ -638,14 +763,16 @@ axhel_status_t axhel_cuda_batch_create(const axhel_job_t* jobs, uint64_t n_jobs,
     BatchArgs args{};
     std::string err;
     std::vector<axhel_ntt_t> held;
-    axhel_status_t st = batch_build(jobs, n_jobs, nullptr, img, &b->zero_off, &b->zero_bytes, &args, nullptr, &err);
+    std::vector<ClassLaunch> sizing;
+    axhel_status_t st =
+        batch_build(jobs, n_jobs, nullptr, img, &b->zero_off, &b->zero_bytes, &args, nullptr, &err, &sizing);
     if (st) return bfail(st, err);
     b->bytes = img.size();
     if (b->bytes) {
         cudaError_t e = cudaMalloc(&b->mem, b->bytes);
         if (e != cudaSuccess) return bfail(AXHEL_ERR_NOMEM, std::string("cudaMalloc(batch): ") + cudaGetErrorString(e));
         st = batch_build(jobs, n_jobs, static_cast<unsigned char*>(b->mem), img, &b->zero_off, &b->zero_bytes,
-                         &b->args, &held, &err, b->phase_begin);
+                         &b->args, &held, &err, &b->classes);
         if (st) {
             cudaFree(b->mem);
             return bfail(st, err);
@@ -682,7 +809,7 @@ axhel_status_t axhel_cuda_batch_launch_phased(axhel_batch_t b, void* stream)
     if (b->args.total_tiles == 0) return AXHEL_OK;
     // the error word is cleared as before a persistent launch (no wait can fail here)
     cudaError_t e = cudaMemsetAsync(static_cast<unsigned char*>(b->mem) + b->zero_off, 0, b->zero_bytes, s);
-    if (e == cudaSuccess) e = batch_launch_phases(b->args, b->phase_begin, s);
+    if (e == cudaSuccess) e = batch_launch_classes(b->args, b->classes, s);
     if (e != cudaSuccess) return bfail(AXHEL_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
     return AXHEL_OK;
 }

@@ -16,6 +16,8 @@ namespace axhel_impl {
 constexpr int kBatchThreads = 128;
 constexpr int kBatchLR = 3;
 constexpr int kBatchTileWords = kBatchThreads << kBatchLR;  // 1024 residues
+constexpr int kBatchTileLog = 10;                           // tiles per limb: 2^(logn - 10)
+static_assert(kBatchTileWords == 1 << kBatchTileLog, "tile size");
 constexpr int kBatchMinLG = 5, kBatchMaxLG = 9;
 // CTAs per SM the kernels are compiled for: 64 registers (128 without the
 // bound) and some spills, which cost less than the latency the extra resident
@@ -55,6 +57,24 @@ struct BatchEntry {
     uint32_t job, phase;
 };
 
+// Tile classes of the per-phase launches: each class runs in a kernel of its
+// own (its own register budget and register depth).
+enum TileClass : uint32_t { kClsFwd = 0, kClsInv = 1, kClsChain = 2, kClsElt = 3 };
+
+// One entry of a class launch: its first tile in the launch's numbering.
+struct ClassEntry {
+    uint64_t tile0;
+    uint32_t entry, pad;
+};
+
+// One launch of a phase: the tiles of one class and pass width, from
+// every job of the batch, in entry order.
+struct ClassLaunch {
+    uint32_t phase, cls, lg, n_ce;
+    const ClassEntry* ce;  // device address, n_ce entries
+    uint64_t tiles;
+};
+
 struct BatchArgs {
     const BatchJob* jobs;
     const BatchEntry* entries;
@@ -73,21 +93,25 @@ axhel_status_t batch_check_job(const axhel_job_t& job, const std::string& who, s
 // Lays out the device image of a batch for the device address `base`:
 // fills `host` (to be copied to `base`), the range of counters that must be
 // zero before a launch, and the kernel arguments.  NTT handles referenced by
-// the jobs are appended to `held` when it is not null.
-// `phase_begin`, when not null, receives the first global tile of phases
-// 0, 1, 2 and the total (4 entries; tiles are numbered phase-major).
+// the jobs are appended to `held` when it is not null.  Tiles are numbered
+// phase-major.  `classes`, when not null, receives the per-phase launches
+// (batch_launch_classes) and the image then holds their entry tables: give
+// it to the sizing pass and to the final build alike.
 axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned char* base,
                            std::vector<unsigned char>& host, size_t* zero_off, size_t* zero_bytes, BatchArgs* args,
-                           std::vector<axhel_ntt_t>* held, std::string* err, uint64_t* phase_begin = nullptr);
+                           std::vector<axhel_ntt_t>* held, std::string* err,
+                           std::vector<ClassLaunch>* classes = nullptr);
 
 // Launches the persistent batch kernel for prepared arguments.
 cudaError_t batch_launch_args(const BatchArgs& a, cudaStream_t s);
 
-// Runs a prepared batch as one ordinary (non-persistent) launch per phase,
-// one CTA per tile and no waits inside a launch: the phases are ordered by
-// the stream.  Concurrent batches on other streams share the SMs tile by
-// tile.  `phase_begin` as filled by batch_build.
-cudaError_t batch_launch_phases(const BatchArgs& a, const uint64_t* phase_begin, cudaStream_t s);
+// Runs a prepared batch as ordinary (non-persistent) launches, one per
+// (phase, tile class, pass width), one CTA per tile and no waits inside a
+// launch: the phases are ordered by the stream.  Each class runs in a kernel
+// specialized for it (register depth and budget).  Concurrent batches on
+// other streams share the SMs tile by tile.  `classes` as filled by
+// batch_build.
+cudaError_t batch_launch_classes(const BatchArgs& a, const std::vector<ClassLaunch>& classes, cudaStream_t s);
 
 // Records the message returned by axhel_cuda_batch_last_error on this thread.
 void batch_set_error(const std::string& msg);

@@ -167,6 +167,14 @@ constexpr int exchange_max_pos()
     return m;
 }
 
+// limb mod n, the limb's modulus context.  Limb indexes below 2^32 (every
+// real batch) take the 32-bit division, a fraction of the 64-bit one's
+// instructions.
+__device__ __forceinline__ uint32_t limb_mod(uint64_t limb, uint32_t n)
+{
+    return (limb >> 32) == 0 ? (uint32_t)limb % n : (uint32_t)(limb % n);
+}
+
 // Lane shift of k in the thread index: 0 for contiguous tiles (thread =
 // group * threads-per-group + k), log2 groups per tile for strided ones
 // (thread = group + k * groups); 32 for CTAs under one warp, which always
@@ -428,7 +436,7 @@ __global__ void __launch_bounds__(max_threads(LR)) ntt_pass_kernel(const __grid_
     const uint32_t lg_tiles = a.logn - LG - lgtg;  // log2 tiles per limb
     const uint64_t tile = blockIdx.x;
     const uint64_t limb = tile >> lg_tiles;
-    pass_tile<INV, LG, LR, false>(a.src, a.dst, a.ctx[limb % a.nctx], a.logn, a.s0, lgtg, limb,
+    pass_tile<INV, LG, LR, false>(a.src, a.dst, a.ctx[limb_mod(limb, a.nctx)], a.logn, a.s0, lgtg, limb,
                                   tile & ((1ull << lg_tiles) - 1), a.flags, sm);
 }
 
@@ -519,7 +527,7 @@ __global__ void __launch_bounds__(max_threads(LR)) ntt_chain_kernel(const __grid
     const uint32_t lg_tiles = a.logn - LG - lgtg;
     const uint64_t tile = blockIdx.x;
     const uint64_t limb = tile >> lg_tiles;
-    const uint32_t mi = limb % a.nctx;
+    const uint32_t mi = limb_mod(limb, a.nctx);
     chain_tile<LG, LR, false>(a.src, a.dst, c.operand, a.ctx[mi], c.op, c.scalar[mi], a.logn, lgtg, limb,
                               tile & ((1ull << lg_tiles) - 1), a.flags, sm);
 }

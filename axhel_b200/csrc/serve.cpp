@@ -181,8 +181,10 @@ axhel_status_t axhel_server::launch(Slot& s, int slot_index, std::vector<Req*>& 
     size_t zo = 0, zb = 0;
     axhel_impl::BatchArgs args{};
     std::string err;
-    uint64_t phases[4] = {0, 0, 0, 0};
-    axhel_status_t rc = axhel_impl::batch_build(jobs.data(), jobs.size(), nullptr, img, &zo, &zb, &args, nullptr, &err);
+    const bool per_phase = !(cfg.flags & AXHEL_SERVER_PERSISTENT);
+    std::vector<axhel_impl::ClassLaunch> classes;
+    axhel_status_t rc = axhel_impl::batch_build(jobs.data(), jobs.size(), nullptr, img, &zo, &zb, &args, nullptr, &err,
+                                                per_phase ? &classes : nullptr);
     if (rc) return sfail(rc, err);
     // Descriptors come from the stream-ordered pool and go back to it after
     // the batch: no cudaMalloc / cudaFree (which wait for the whole device)
@@ -191,7 +193,7 @@ axhel_status_t axhel_server::launch(Slot& s, int slot_index, std::vector<Req*>& 
     if (cudaMallocFromPoolAsync(&desc, img.size(), pool, st) != cudaSuccess)
         return sfail(AXHEL_ERR_NOMEM, "batch descriptor buffer");
     rc = axhel_impl::batch_build(jobs.data(), jobs.size(), static_cast<unsigned char*>(desc), img, &zo, &zb,
-                                 &args, nullptr, &err, phases);
+                                 &args, nullptr, &err, per_phase ? &classes : nullptr);
     if (rc) {
         cudaFreeAsync(desc, st);
         return sfail(rc, err);
@@ -213,8 +215,7 @@ axhel_status_t axhel_server::launch(Slot& s, int slot_index, std::vector<Req*>& 
     std::memcpy(s.host_img, img.data(), img.size());
     cudaError_t e = cudaMemcpyAsync(desc, s.host_img, img.size(), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
-        e = (cfg.flags & AXHEL_SERVER_PERSISTENT) ? axhel_impl::batch_launch_args(args, st)
-                                                   : axhel_impl::batch_launch_phases(args, phases, st);
+        e = per_phase ? axhel_impl::batch_launch_classes(args, classes, st) : axhel_impl::batch_launch_args(args, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(s.err_host, args.error, sizeof(int), cudaMemcpyDeviceToHost, st);
     // results back smallest first; each request completes at its own event
     std::vector<Req*> order(take);

@@ -430,7 +430,7 @@ def kernel_case(family):
     elif family == "tables":  # 3 x 24 fresh contexts of N = 2^16
         for lo, hi in ((30, 40), (41, 51), (52, 62)):
             capi.NTT.create_many([(1 << 16, q, psi) for q, psi in params.rns_moduli(1 << 16, 24, lo, hi)])
-    elif family in ("chain", "batch", "batch_eltwise"):  # 384 limbs of N = 2^16 (192 MiB), 24 moduli
+    elif family in ("chain", "batch", "batch_phased", "batch_eltwise"):  # 384 limbs of N = 2^16 (192 MiB), 24 moduli
         n = 1 << 16
         mods = params.rns_moduli(n, 24, 50, 59)
         ntts = [capi.NTT(n, q, psi) for q, psi in mods]
@@ -439,11 +439,11 @@ def kernel_case(family):
         if family == "chain":  # INTT -> MulMod -> NTT, fused
             for _ in range(2):
                 capi.chain_mul_batch(ntts, x.data_ptr(), x.data_ptr(), v.data_ptr(), 384, 2, 4)
-        elif family == "batch":  # one forward job, one persistent launch
+        elif family in ("batch", "batch_phased"):  # one forward job: one persistent launch, or one per phase
             b = capi.Batch([dict(kind=capi.JOB_FORWARD, ntts=ntts, count=384, result=x.data_ptr(),
                                  operand=x.data_ptr(), in_f=4, out_f=4)])
             for _ in range(3):
-                b.launch()
+                b.launch(phased=family == "batch_phased")
         else:  # one MulMod job, one launch per phase
             b = capi.Batch([dict(kind=capi.JOB_MUL, ntts=ntts, count=384, result=x.data_ptr(), operand=x.data_ptr(),
                                  vector=v.data_ptr(), in_f=1, out_f=1)])
@@ -459,7 +459,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("what", choices=["tensor", "uneven", "serve", "eltwise", "case"])
     ap.add_argument("family", nargs="?", default="eltwise",
-                    help="case: eltwise | tensor | tables | chain | batch | batch_eltwise")
+                    help="case: eltwise | tensor | tables | chain | batch | batch_phased | batch_eltwise")
     ap.add_argument("--seconds", type=float, default=4.0)
     ap.add_argument("--device", action="store_true", help="device-resident request operands")
     ap.add_argument("--persistent", action="store_true", help="one persistent launch per batch")

@@ -81,3 +81,9 @@ def test_largest_degree_all_kinds(cuda, oracle):
         specs, bufs = tb.specs_for(cuda, jobs)
         cuda.batch_run(specs)
         tb.check(oracle, jobs, bufs)
+        specs, bufs = tb.specs_for(cuda, jobs)
+        b = cuda.Batch(specs)
+        b.launch(phased=True)
+        assert b.status() == 0
+        tb.check(oracle, jobs, bufs)
+        b.close()

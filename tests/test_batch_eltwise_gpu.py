@@ -65,10 +65,10 @@ def test_eltwise_and_transform_jobs_in_one_launch(cuda, oracle):
     ejobs = elt_jobs(cuda, oracle, 78, logns=(11, 15), L=2, count=4)
     especs, ebufs = elt_specs(cuda, ejobs)
     b = cuda.Batch(tspecs + especs)
-    for graph in (False, True):
+    for graph, phased in ((False, False), (True, False), (False, True)):
         for _, o, _ in tbufs + ebufs:
             o.zero_()
-        b.launch(graph=graph)
+        b.launch(graph=graph, phased=phased)
         assert b.status() == 0
         tb.check(oracle, tjobs, tbufs)
         for jb, (d, o, dv) in zip(ejobs, ebufs):

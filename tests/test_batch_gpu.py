@@ -164,6 +164,12 @@ def test_every_batch_split_bitexact(cuda, oracle):
                 specs, bufs = specs_for(cuda, jobs)
                 cuda.batch_run(specs)
                 check(oracle, jobs, bufs)
+                specs, bufs = specs_for(cuda, jobs)  # the per-phase launches of every width
+                b = cuda.Batch(specs)
+                b.launch(phased=True)
+                assert b.status() == 0
+                check(oracle, jobs, bufs)
+                b.close()
             finally:
                 cuda.batch_split_set(logn, 0)
 
