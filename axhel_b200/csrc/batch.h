@@ -61,10 +61,17 @@ struct BatchEntry {
 // own (its own register budget and register depth).
 enum TileClass : uint32_t { kClsFwd = 0, kClsInv = 1, kClsChain = 2, kClsElt = 3 };
 
-// One entry of a class launch: its first tile in the launch's numbering.
+// One entry of a class launch: a (job, phase) with what its tiles read, and
+// its first tile in the launch's numbering.
 struct ClassEntry {
     uint64_t tile0;
-    uint32_t entry, pad;
+    const uint64_t* src;               // the job's operand in phase 0, its result after
+    uint64_t* dst;
+    const uint64_t* vec;               // chain multiplicand / addend, element-wise second operand
+    const ModCtx* const* ctx;          // nmods device pointers
+    const uint64_t* scalars;           // per modulus: chain FMA, element-wise scalar ops; else null
+    uint32_t nmods, logn, s0, flags;   // transform passes: first stage, the tile functions' flags
+    uint32_t op, eop, ef, pad;         // chain op; element-wise op and factor
 };
 
 // One launch of a phase: the tiles of one class and pass width, from
@@ -73,6 +80,7 @@ struct ClassLaunch {
     uint32_t phase, cls, lg, n_ce;
     const ClassEntry* ce;  // device address, n_ce entries
     uint64_t tiles;
+    ClassEntry first;      // host copy of ce[0]: a launch of one entry takes it as a kernel parameter
 };
 
 struct BatchArgs {
@@ -111,7 +119,7 @@ cudaError_t batch_launch_args(const BatchArgs& a, cudaStream_t s);
 // specialized for it (register depth and budget).  Concurrent batches on
 // other streams share the SMs tile by tile.  `classes` as filled by
 // batch_build.
-cudaError_t batch_launch_classes(const BatchArgs& a, const std::vector<ClassLaunch>& classes, cudaStream_t s);
+cudaError_t batch_launch_classes(const std::vector<ClassLaunch>& classes, cudaStream_t s);
 
 // Records the message returned by axhel_cuda_batch_last_error on this thread.
 void batch_set_error(const std::string& msg);

@@ -215,7 +215,7 @@ axhel_status_t axhel_server::launch(Slot& s, int slot_index, std::vector<Req*>& 
     std::memcpy(s.host_img, img.data(), img.size());
     cudaError_t e = cudaMemcpyAsync(desc, s.host_img, img.size(), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
-        e = per_phase ? axhel_impl::batch_launch_classes(args, classes, st) : axhel_impl::batch_launch_args(args, st);
+        e = per_phase ? axhel_impl::batch_launch_classes(classes, st) : axhel_impl::batch_launch_args(args, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(s.err_host, args.error, sizeof(int), cudaMemcpyDeviceToHost, st);
     // results back smallest first; each request completes at its own event
     std::vector<Req*> order(take);
