@@ -332,7 +332,7 @@ def serving(loads=(0.5, 0.7, 0.9), seconds=4.0, budget=60 << 30, inflight=4, see
 
     out = {"workload": "INTT->MulMod/FMAMod->NTT requests, N in 2^13..2^17, L in 2..40, Poisson arrivals",
            "operands": "device-resident" if device else "host pinned, staged per request",
-           "launch": "persistent" if persistent else "one launch per phase", "max_batch_words": max_batch_words,
+           "launch": "persistent" if persistent else "per-phase class launches", "max_batch_words": max_batch_words,
            "small_request_words": small_words,
            "capacity_jobs_per_s": cap, "isolated_median_ms": statistics.median(iso), "loads": results,
            "batches": st["batches"], "max_batch_requests": st["max_batch_requests"],

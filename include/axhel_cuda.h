@@ -195,9 +195,10 @@ axhel_status_t axhel_cuda_batch_create(const axhel_job_t* jobs, uint64_t n_jobs,
 axhel_status_t axhel_cuda_batch_launch(axhel_batch_t batch, void* stream);
 /* Same, through a CUDA graph instantiated on first use and replayed after. */
 axhel_status_t axhel_cuda_batch_graph_launch(axhel_batch_t batch, void* stream);
-/* Runs the batch as one ordinary launch per phase (at most three; every
- * phase's tiles of all jobs in one grid, one CTA per tile, no waits inside a
- * launch): same results; may be captured into a CUDA graph. */
+/* Runs the batch as ordinary launches, phase after phase: one per (phase,
+ * tile class, pass width), each a grid of that class's tiles of all jobs,
+ * one CTA per tile, no waits inside a launch; same results; may be captured
+ * into a CUDA graph. */
 axhel_status_t axhel_cuda_batch_launch_phased(axhel_batch_t batch, void* stream);
 /* Waits for `stream` and returns AXHEL_ERR_TIMEOUT if a dependency wait
  * inside the kernel gave up (bounded at 2 s), else AXHEL_OK. */
