@@ -357,6 +357,10 @@ def run_ours(args):
                    "sample": f"{S} limbs of the N=2^16 workload x {reps} repeats, lazy round trip "
                              f"(forward, ReduceMod 4->2, inverse), {secs:.1f} s",
                    "tables_ms": 1e3 * tables_s}
+            # the same on one host thread (the library itself is single-threaded)
+            r1, S1, reps1, secs1, _ = reference_roundtrip_rate(mods, data, 1, min(args.cpu_seconds, 3.0))
+            cpu["single_thread"] = {"value": r1, "unit": UNIT, "cores": 1,
+                                    "sample": f"{S1} limbs x {reps1} repeats, {secs1:.1f} s"}
         except Exception as e:  # the reference build is test infrastructure; report its absence
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
 

@@ -102,3 +102,26 @@ def test_eltwise_jobs_refuse_what_the_reference_ignores(cuda, oracle):
         with pytest.raises(cuda.AxhelError) as e:
             cuda.batch_run([dict(base, **b)])
         assert e.value.status == 1, b  # AXHEL_ERR_INVALID
+
+
+def test_single_job_batches_per_phase_every_kind(cuda, oracle):
+    """A batch of one job runs its per-phase launches with the job's entry as
+    a kernel parameter: every transform kind (at a split of each width) and
+    every element-wise form, alone, against the reference's per-limb calls."""
+    rng = np.random.default_rng(123)
+    for kind in (1, 2, 3, 4):
+        for logn in (11, 14, 16, 17):
+            jobs = tb.make_jobs(cuda, oracle, rng, 1, [logn], 3, 3, kinds=(kind,))
+            specs, bufs = tb.specs_for(cuda, jobs)
+            b = cuda.Batch(specs)
+            b.launch(phased=True)
+            assert b.status() == 0
+            tb.check(oracle, jobs, bufs)
+            b.close()
+    for jb in elt_jobs(cuda, oracle, 124, logns=(10, 14), L=2, count=3):
+        specs, bufs = elt_specs(cuda, [jb])
+        b = cuda.Batch(specs)
+        b.launch(phased=True)
+        assert b.status() == 0
+        np.testing.assert_array_equal(host(bufs[0][1], jb["x"].size), want(oracle, jb))
+        b.close()
