@@ -68,7 +68,7 @@ struct PhaseCfg {
     uint32_t lg, s0;
 };
 
-__host__ __device__ inline PhaseCfg phase_cfg(const BatchJob& j, uint32_t p)
+inline PhaseCfg phase_cfg(const BatchJob& j, uint32_t p)
 {
     PhaseCfg c{false, false, 0, 0};
     if (j.kind == kJobForward) {
@@ -93,31 +93,6 @@ __host__ __device__ inline PhaseCfg phase_cfg(const BatchJob& j, uint32_t p)
         }
     }
     return c;
-}
-
-template <int LG>
-__device__ __forceinline__ void run_tile_lg(const BatchJob& j, const PhaseCfg& c, uint32_t p, uint64_t limb,
-                                            uint64_t tile_in_limb, uint64_t* sm)
-{
-    constexpr uint32_t lgtg = 10 - LG;  // 1024 / 2^LG groups per tile
-    const uint32_t mi = limb_mod(limb, j.nmods);
-    const ModCtx* cx = j.ctx[mi];
-    const bool first = p == 0, last = p + 1 == j.nphase;
-    const uint64_t* src = first ? j.src : j.dst;
-    uint32_t flags = (first && j.pre) ? kPreCsub2q : 0;
-    if (last) flags |= kLastPass | (j.norm ? kPostNorm : 0);
-    if (c.chain) {
-        const uint32_t op = j.kind == kJobChainMul ? kChainMul : kChainFma;
-        const uint64_t sc = j.kind == kJobChainFma ? j.scalars[mi] : 0;
-        chain_tile<LG, kBatchLR, true>(src, j.dst, j.vec, cx, op, sc, j.logn, lgtg, limb, tile_in_limb,
-                                        (first && j.pre ? kPreCsub2q : 0) | (last && j.norm ? kPostNorm : 0), sm);
-    } else if (c.inv) {
-        // the inverse's last pass holds the N^-1 stage even inside a chain
-        const uint32_t f = flags | (c.s0 + LG == j.logn ? kLastPass : 0);
-        pass_tile<true, LG, kBatchLR, true>(src, j.dst, cx, j.logn, c.s0, lgtg, limb, tile_in_limb, f, sm);
-    } else {
-        pass_tile<false, LG, kBatchLR, true>(src, j.dst, cx, j.logn, c.s0, lgtg, limb, tile_in_limb, flags, sm);
-    }
 }
 
 // Element-wise job tile: 1024 residues of one limb, 8 per thread at a
@@ -184,22 +159,42 @@ __device__ __forceinline__ void run_elt_tile(const J& j, uint64_t limb, uint64_t
     }
 }
 
-// One tile of any job kind.
-__device__ __forceinline__ void run_tile(const BatchJob& j, uint32_t phase, uint64_t limb, uint64_t til,
-                                         uint64_t* sm)
+// One tile of class CLS and pass width LG with LR register stages; the
+// entry carries the pass's operands, first stage and flags (built on the
+// host from the job).  The strided and contiguous passes take 64 threads x 16
+// registers per 1024-residue tile when LR = 4.  CG: loads bypass L1, for
+// data written by other CTAs of the same launch (the persistent kernel); the
+// per-phase launches read what an earlier launch wrote and load plainly.
+template <int CLS, int LG, int LR, bool CG>
+__device__ __forceinline__ void run_class_tile(const ClassEntry& c, uint64_t limb, uint64_t tile_in_limb,
+                                               uint64_t* sm)
 {
-    if (j.kind >= kJobAdd) {
-        run_elt_tile(j, limb, til);
-        return;
+    constexpr uint32_t lgtg = 10 - LG;
+    const uint32_t mi = limb_mod(limb, c.nmods);
+    const ModCtx* cx = c.ctx[mi];
+    if constexpr (CLS == kClsChain) {
+        chain_tile<LG, LR, CG>(c.src, c.dst, c.vec, cx, c.op, c.scalars ? c.scalars[mi] : 0, c.logn, lgtg, limb,
+                               tile_in_limb, c.flags, sm);
+    } else {
+        pass_tile<CLS == kClsInv, LG, LR, CG>(c.src, c.dst, cx, c.logn, c.s0, lgtg, limb, tile_in_limb, c.flags,
+                                              sm);
     }
-    const PhaseCfg c = phase_cfg(j, phase);
-    switch (c.lg) {
-    case 5: run_tile_lg<5>(j, c, phase, limb, til, sm); break;
-    case 6: run_tile_lg<6>(j, c, phase, limb, til, sm); break;
-    case 7: run_tile_lg<7>(j, c, phase, limb, til, sm); break;
-    case 8: run_tile_lg<8>(j, c, phase, limb, til, sm); break;
-    case 9: run_tile_lg<9>(j, c, phase, limb, til, sm); break;
-    default: break;
+}
+
+// One tile of any class (the persistent kernel: 128 threads x 8 registers).
+__device__ __forceinline__ void run_any_tile(const ClassEntry& c, uint64_t limb, uint64_t til, uint64_t* sm)
+{
+    switch (c.cls_lg) {
+#define AXHEL_TILE_CASE(CLS, LG) \
+    case (CLS << 8) | LG: run_class_tile<CLS, LG, kBatchLR, true>(c, limb, til, sm); break;
+#define AXHEL_TILE_CASES(CLS) \
+    AXHEL_TILE_CASE(CLS, 5) AXHEL_TILE_CASE(CLS, 6) AXHEL_TILE_CASE(CLS, 7) AXHEL_TILE_CASE(CLS, 8) AXHEL_TILE_CASE(CLS, 9)
+    AXHEL_TILE_CASES(kClsFwd)
+    AXHEL_TILE_CASES(kClsInv)
+    AXHEL_TILE_CASES(kClsChain)
+#undef AXHEL_TILE_CASES
+#undef AXHEL_TILE_CASE
+    default: run_elt_tile(c, limb, til); break;  // kClsElt << 8
     }
 }
 
@@ -263,42 +258,24 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks) batch_kernel(c
         }
         __syncthreads();
         if (s_abort) break;
-        const BatchEntry e = a.entries[s_entry];
-        const BatchJob& j = a.jobs[e.job];
-        const uint64_t lt = tile - e.tile_begin;
-        const uint32_t lgt = j.logn - kBatchTileLog;  // tiles per limb: a power of two
+        const ClassEntry& c = a.tile_args[s_entry];
+        const uint64_t lt = tile - c.tile0;
+        const uint32_t lgt = c.logn - kBatchTileLog;  // tiles per limb: a power of two
         const uint64_t limb = lt >> lgt;
-        run_tile(j, e.phase, limb, lt & ((1ull << lgt) - 1), sm);
+        run_any_tile(c, limb, lt & ((1ull << lgt) - 1), sm);
         if (threadIdx.x == 0) s_tile[(it + 1) & 1] = nxt;
         __syncthreads();
-        if (threadIdx.x == 0 && e.phase + 1 < j.nphase) {
-            // release at device scope, cumulative over the stores the barrier
-            // ordered before it
-            cuda::atomic_ref<unsigned int, cuda::thread_scope_device> done(
-                a.done[j.done_off + (uint64_t)e.phase * j.count + limb]);
-            done.fetch_add(1u, cuda::memory_order_release);
+        if (threadIdx.x == 0) {
+            const BatchEntry e = a.entries[s_entry];
+            const BatchJob& j = a.jobs[e.job];
+            if (e.phase + 1 < j.nphase) {
+                // release at device scope, cumulative over the stores the
+                // barrier ordered before it
+                cuda::atomic_ref<unsigned int, cuda::thread_scope_device> done(
+                    a.done[j.done_off + (uint64_t)e.phase * j.count + limb]);
+                done.fetch_add(1u, cuda::memory_order_release);
+            }
         }
-    }
-}
-
-// One tile of class CLS and pass width LG with LR register stages; the
-// entry carries the pass's operands, first stage and flags as run_tile_lg
-// derives them.  The strided and contiguous passes take 64 threads x 16
-// registers per 1024-residue tile when LR = 4.  Plain (L1-cached) loads: the
-// previous phase was written by an earlier launch.
-template <int CLS, int LG, int LR>
-__device__ __forceinline__ void run_class_tile(const ClassEntry& c, uint64_t limb, uint64_t tile_in_limb,
-                                               uint64_t* sm)
-{
-    constexpr uint32_t lgtg = 10 - LG;
-    const uint32_t mi = limb_mod(limb, c.nmods);
-    const ModCtx* cx = c.ctx[mi];
-    if constexpr (CLS == kClsChain) {
-        chain_tile<LG, LR, false>(c.src, c.dst, c.vec, cx, c.op, c.scalars ? c.scalars[mi] : 0, c.logn, lgtg, limb,
-                                  tile_in_limb, c.flags, sm);
-    } else {
-        pass_tile<CLS == kClsInv, LG, LR, false>(c.src, c.dst, cx, c.logn, c.s0, lgtg, limb, tile_in_limb, c.flags,
-                                                 sm);
     }
 }
 
@@ -318,7 +295,7 @@ __device__ __forceinline__ void run_class_entry(const ClassEntry& c, uint64_t t,
     if constexpr (CLS == kClsElt)
         run_elt_tile(c, limb, til);
     else
-        run_class_tile<CLS, LG, LR>(c, limb, til, sm);
+        run_class_tile<CLS, LG, LR, false>(c, limb, til, sm);
 }
 
 // One class launch: CTA b runs the class's tile b (entries in tile order),
@@ -604,6 +581,28 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
     }
     // per (phase, class, pass width): the entries, in order, with their
     // first tile in that launch's numbering
+    // every entry's tile class and pass width
+    std::vector<uint32_t> ent_cls(ent.size()), ent_lg(ent.size());
+    for (size_t k = 0; k < ent.size(); ++k) {
+        const BatchEntry& e = ent[k];
+        const BatchJob& b = bj[e.job];
+        uint32_t cls, lg;
+        if (b.kind >= kJobAdd) {
+            cls = kClsElt;
+            lg = 0;
+        } else if (b.kind == kJobForward) {
+            cls = kClsFwd;
+            lg = e.phase == 0 ? b.lg_col : b.lg_row;
+        } else if (b.kind == kJobInverse) {
+            cls = kClsInv;
+            lg = e.phase == 0 ? b.lg_row : b.lg_col;
+        } else {  // chain: inverse row pass, fused column pass, forward row pass
+            cls = e.phase == 0 ? kClsInv : (e.phase == 1 ? kClsChain : kClsFwd);
+            lg = e.phase == 1 ? b.lg_col : b.lg_row;
+        }
+        ent_cls[k] = cls;
+        ent_lg[k] = lg;
+    }
     std::vector<ClassLaunch> cl;
     std::vector<std::vector<ClassEntry>> cl_ent;
     std::vector<std::vector<uint32_t>> cl_idx;  // the batch entry of each class entry
@@ -612,20 +611,7 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
         for (uint32_t k = 0; k < (uint32_t)ent.size(); ++k) {
             const BatchEntry& e = ent[k];
             const BatchJob& b = bj[e.job];
-            uint32_t cls, lg;
-            if (b.kind >= kJobAdd) {
-                cls = kClsElt;
-                lg = 0;
-            } else if (b.kind == kJobForward) {
-                cls = kClsFwd;
-                lg = e.phase == 0 ? b.lg_col : b.lg_row;
-            } else if (b.kind == kJobInverse) {
-                cls = kClsInv;
-                lg = e.phase == 0 ? b.lg_row : b.lg_col;
-            } else {  // chain: inverse row pass, fused column pass, forward row pass
-                cls = e.phase == 0 ? kClsInv : (e.phase == 1 ? kClsChain : kClsFwd);
-                lg = e.phase == 1 ? b.lg_col : b.lg_row;
-            }
+            const uint32_t cls = ent_cls[k], lg = ent_lg[k];
             const auto key = std::make_tuple(e.phase, cls, lg);
             auto it = at.find(key);
             if (it == at.end()) {
@@ -649,6 +635,8 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
     off = align_up(off + n_jobs * sizeof(BatchJob), 256);
     const size_t ent_off = off;
     off = align_up(off + ent.size() * sizeof(BatchEntry), 256);
+    const size_t targ_off = off;
+    off = align_up(off + ent.size() * sizeof(ClassEntry), 256);
     std::vector<size_t> ctx_off(n_jobs), sc_off(n_jobs, 0);
     for (uint64_t i = 0; i < n_jobs; ++i) {
         ctx_off[i] = off;
@@ -682,35 +670,45 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
     }
     std::memcpy(host.data() + jobs_off, bj.data(), n_jobs * sizeof(BatchJob));
     std::memcpy(host.data() + ent_off, ent.data(), ent.size() * sizeof(BatchEntry));
+    // each entry's tile arguments: operands, first stage and the tile
+    // functions' flags (the first tile of a class launch's entry is in that
+    // launch's numbering, of the persistent kernel's entry the global one)
+    std::vector<ClassEntry> targ(ent.size());
+    for (size_t k = 0; k < ent.size(); ++k) {
+        ClassEntry& x = targ[k];
+        const uint32_t p = ent[k].phase, cls = ent_cls[k];
+        const BatchJob& b = bj[ent[k].job];
+        const bool first = p == 0, last = p + 1 == b.nphase;
+        x.tile0 = ent[k].tile_begin;
+        x.src = first ? b.src : b.dst;
+        x.dst = b.dst;
+        x.vec = b.vec;
+        x.ctx = b.ctx;
+        x.scalars = (b.kind == kJobChainFma || b.kind >= kJobAdd) ? b.scalars : nullptr;
+        x.nmods = b.nmods;
+        x.logn = b.logn;
+        x.eop = b.eop;
+        x.ef = b.ef;
+        x.cls_lg = cls << 8 | ent_lg[k];
+        if (cls == kClsElt) continue;
+        const PhaseCfg pc = phase_cfg(b, p);
+        x.s0 = pc.s0;
+        if (cls == kClsChain) {
+            x.op = b.kind == kJobChainMul ? kChainMul : kChainFma;
+            x.flags = (first && b.pre ? kPreCsub2q : 0) | (last && b.norm ? kPostNorm : 0);
+        } else {
+            x.flags = (first && b.pre) ? kPreCsub2q : 0;
+            if (last) x.flags |= kLastPass | (b.norm ? kPostNorm : 0);
+            // the inverse's last pass holds the N^-1 stage even inside a chain
+            if (cls == kClsInv && pc.s0 + ent_lg[k] == b.logn) x.flags |= kLastPass;
+        }
+    }
+    std::memcpy(host.data() + targ_off, targ.data(), targ.size() * sizeof(ClassEntry));
     for (size_t c = 0; c < cl.size(); ++c) {
         for (size_t i = 0; i < cl_ent[c].size(); ++i) {
-            // operands, first stage and flags of the tile functions, as
-            // run_tile_lg derives them on the device
-            ClassEntry& x = cl_ent[c][i];
-            const uint32_t p = ent[cl_idx[c][i]].phase;
-            const BatchJob& b = bj[ent[cl_idx[c][i]].job];
-            const bool first = p == 0, last = p + 1 == b.nphase;
-            x.src = first ? b.src : b.dst;
-            x.dst = b.dst;
-            x.vec = b.vec;
-            x.ctx = b.ctx;
-            x.scalars = (b.kind == kJobChainFma || b.kind >= kJobAdd) ? b.scalars : nullptr;
-            x.nmods = b.nmods;
-            x.logn = b.logn;
-            x.eop = b.eop;
-            x.ef = b.ef;
-            if (cl[c].cls == kClsElt) continue;
-            const PhaseCfg pc = phase_cfg(b, p);
-            x.s0 = pc.s0;
-            if (cl[c].cls == kClsChain) {
-                x.op = b.kind == kJobChainMul ? kChainMul : kChainFma;
-                x.flags = (first && b.pre ? kPreCsub2q : 0) | (last && b.norm ? kPostNorm : 0);
-            } else {
-                x.flags = (first && b.pre) ? kPreCsub2q : 0;
-                if (last) x.flags |= kLastPass | (b.norm ? kPostNorm : 0);
-                // the inverse's last pass holds the N^-1 stage even inside a chain
-                if (cl[c].cls == kClsInv && pc.s0 + cl[c].lg == b.logn) x.flags |= kLastPass;
-            }
+            const uint64_t t0 = cl_ent[c][i].tile0;
+            cl_ent[c][i] = targ[cl_idx[c][i]];
+            cl_ent[c][i].tile0 = t0;
         }
         std::memcpy(host.data() + ce_off[c], cl_ent[c].data(), cl_ent[c].size() * sizeof(ClassEntry));
         cl[c].ce = reinterpret_cast<const ClassEntry*>(base + ce_off[c]);
@@ -724,6 +722,7 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
     }
     args->jobs = reinterpret_cast<const BatchJob*>(base + jobs_off);
     args->entries = reinterpret_cast<const BatchEntry*>(base + ent_off);
+    args->tile_args = reinterpret_cast<const ClassEntry*>(base + targ_off);
     args->nentries = (uint32_t)ent.size();
     args->total_tiles = tiles;
     args->done = reinterpret_cast<unsigned*>(base + done_off);

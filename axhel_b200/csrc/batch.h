@@ -71,7 +71,8 @@ struct ClassEntry {
     const ModCtx* const* ctx;          // nmods device pointers
     const uint64_t* scalars;           // per modulus: chain FMA, element-wise scalar ops; else null
     uint32_t nmods, logn, s0, flags;   // transform passes: first stage, the tile functions' flags
-    uint32_t op, eop, ef, pad;         // chain op; element-wise op and factor
+    uint32_t op, eop, ef;              // chain op; element-wise op and factor
+    uint32_t cls_lg;                   // tile class << 8 | pass width
 };
 
 // One launch of a phase: the tiles of one class and pass width, from
@@ -86,6 +87,7 @@ struct ClassLaunch {
 struct BatchArgs {
     const BatchJob* jobs;
     const BatchEntry* entries;
+    const ClassEntry* tile_args;        // per entry: what its tiles read (tile0: its first global tile)
     uint32_t nentries;
     uint64_t total_tiles;
     unsigned int* done;                 // per (job, phase, limb) completed tiles
