@@ -27,7 +27,8 @@
 // (ld.global.cg), never through a possibly stale L1 line.  A finished tile
 // is published as a grid barrier publishes arrival: CTA barrier, then one
 // thread's device-scope release increment (cumulative over the stores the
-// barrier ordered before it).
+// barrier ordered before it), by a thread of another warp than the one that
+// claims and checks the next tile, which waits on nothing before it.
 //
 // Each tile is 1024 residues handled by 128 threads x 8 registers
 // (LR = 3): 2^(10-LG) groups of 2^LG for the pass widths LG = 5..9 of the
@@ -258,15 +259,19 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks) batch_kernel(c
         }
         __syncthreads();
         if (s_abort) break;
-        const ClassEntry& c = a.tile_args[s_entry];
+        const uint32_t cur = s_entry;
+        const ClassEntry& c = a.tile_args[cur];
         const uint64_t lt = tile - c.tile0;
         const uint32_t lgt = c.logn - kBatchTileLog;  // tiles per limb: a power of two
         const uint64_t limb = lt >> lgt;
         run_any_tile(c, limb, lt & ((1ull << lgt) - 1), sm);
         if (threadIdx.x == 0) s_tile[(it + 1) & 1] = nxt;
         __syncthreads();
-        if (threadIdx.x == 0) {
-            const BatchEntry e = a.entries[s_entry];
+        // The finished tile is published by a thread of another warp than the
+        // claiming thread 0, so its release fence overlaps the next tile's
+        // lookup and dependency check instead of preceding them.
+        if (threadIdx.x == kBatchPublisher) {
+            const BatchEntry e = a.entries[cur];
             const BatchJob& j = a.jobs[e.job];
             if (e.phase + 1 < j.nphase) {
                 // release at device scope, cumulative over the stores the

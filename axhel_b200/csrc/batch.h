@@ -16,7 +16,9 @@ namespace axhel_impl {
 constexpr int kBatchThreads = 128;
 constexpr int kBatchLR = 3;
 constexpr int kBatchTileWords = kBatchThreads << kBatchLR;  // 1024 residues
-constexpr int kBatchTileLog = 10;                           // tiles per limb: 2^(logn - 10)
+constexpr int kBatchTileLog = 10;
+constexpr int kBatchPublisher = 32;                         // persistent kernel: the thread that publishes tiles
+static_assert(kBatchThreads > kBatchPublisher, "publisher in a second warp");                           // tiles per limb: 2^(logn - 10)
 static_assert(kBatchTileWords == 1 << kBatchTileLog, "tile size");
 constexpr int kBatchMinLG = 5, kBatchMaxLG = 9;
 // CTAs per SM the kernels are compiled for: 64 registers (128 without the
