@@ -344,6 +344,7 @@ struct axhel_batch {
     size_t zero_off = 0, zero_bytes = 0;  // counters cleared before every launch
     BatchArgs args{};
     std::vector<ClassLaunch> classes;        // the per-phase launches
+    LaunchLanes lanes;                       // their side-by-side streams
     unsigned grid = 0;
     std::vector<axhel_ntt_t> held;  // table contexts kept alive while the batch exists
     cudaGraphExec_t graph = nullptr;
@@ -611,12 +612,33 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
     std::vector<ClassLaunch> cl;
     std::vector<std::vector<ClassEntry>> cl_ent;
     std::vector<std::vector<uint32_t>> cl_idx;  // the batch entry of each class entry
+    std::vector<ClassLaunch> alone;             // launches of one large entry
+    std::vector<uint32_t> alone_idx;
     if (classes) {
+        // The largest entries of each phase (at least kAloneMinTiles tiles,
+        // up to kAloneMax) get launches of their own, which take the entry
+        // as a kernel parameter; the rest are grouped by class and width.
+        constexpr uint64_t kAloneMinTiles = 512;
+        constexpr size_t kAloneMax = 128;
+        const auto ent_tiles = [&](uint32_t k) { return bj[ent[k].job].count * bj[ent[k].job].tiles_per_limb[ent[k].phase]; };
+        std::vector<char> is_alone(ent.size(), 0);
+        for (uint32_t p = 0; p < 3; ++p) {
+            std::vector<uint32_t> big;
+            for (uint32_t k = 0; k < (uint32_t)ent.size(); ++k)
+                if (ent[k].phase == p && ent_tiles(k) >= kAloneMinTiles) big.push_back(k);
+            std::stable_sort(big.begin(), big.end(), [&](uint32_t x, uint32_t y) { return ent_tiles(x) > ent_tiles(y); });
+            for (size_t i = 0; i < big.size() && i < kAloneMax; ++i) is_alone[big[i]] = 1;
+        }
         std::map<std::tuple<uint32_t, uint32_t, uint32_t>, size_t> at;
         for (uint32_t k = 0; k < (uint32_t)ent.size(); ++k) {
             const BatchEntry& e = ent[k];
             const BatchJob& b = bj[e.job];
             const uint32_t cls = ent_cls[k], lg = ent_lg[k];
+            if (is_alone[k]) {
+                alone.push_back(ClassLaunch{e.phase, cls, lg, 1, nullptr, ent_tiles(k), ClassEntry{}});
+                alone_idx.push_back(k);
+                continue;
+            }
             const auto key = std::make_tuple(e.phase, cls, lg);
             auto it = at.find(key);
             if (it == at.end()) {
@@ -720,9 +742,15 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
         cl[c].first = cl_ent[c][0];
     }
     if (classes) {
-        // phase by phase (the map numbered them in first-seen order, which is
-        // already phase-major)
-        std::stable_sort(cl.begin(), cl.end(), [](const ClassLaunch& x, const ClassLaunch& y) { return x.phase < y.phase; });
+        for (size_t i = 0; i < alone.size(); ++i) {
+            alone[i].first = targ[alone_idx[i]];
+            alone[i].first.tile0 = 0;
+        }
+        cl.insert(cl.end(), alone.begin(), alone.end());
+        // phase by phase, the largest launches first (spread over the lanes)
+        std::stable_sort(cl.begin(), cl.end(), [](const ClassLaunch& x, const ClassLaunch& y) {
+            return x.phase != y.phase ? x.phase < y.phase : x.tiles > y.tiles;
+        });
         *classes = cl;
     }
     args->jobs = reinterpret_cast<const BatchJob*>(base + jobs_off);
@@ -771,21 +799,63 @@ ClassKernel pick_class_kernel(uint32_t cls, uint32_t lg)
 
 }  // namespace
 
-cudaError_t batch_launch_classes(const std::vector<ClassLaunch>& classes, cudaStream_t s)
+cudaError_t lanes_create(LaunchLanes* l, int priority)
 {
-    for (const ClassLaunch& L : classes) {
-        if (L.tiles == 0) continue;
-        if (L.tiles > 0x7fffffffull) return cudaErrorInvalidValue;
-        const ClassKernel k = pick_class_kernel(L.cls, L.lg);
-        if (!k.one) return cudaErrorInvalidValue;
-        count_launch();
-        ProfScope prof(s, "batch_class_kernel cls=%u lg=%u", L.cls, L.lg);
-        if (L.n_ce == 1)
-            k.one<<<(unsigned)L.tiles, k.threads, 0, s>>>(L.first);
-        else
-            k.many<<<(unsigned)L.tiles, k.threads, 0, s>>>(L.ce, L.n_ce);
-        const cudaError_t e = cudaGetLastError();
+    for (int i = 0; i < kLaunchLanes - 1; ++i) {
+        cudaError_t e = cudaStreamCreateWithPriority(&l->st[i], cudaStreamNonBlocking, priority);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&l->join[i], cudaEventDisableTiming);
         if (e != cudaSuccess) return e;
+    }
+    return cudaEventCreateWithFlags(&l->fork, cudaEventDisableTiming);
+}
+
+void lanes_destroy(LaunchLanes* l)
+{
+    for (int i = 0; i < kLaunchLanes - 1; ++i) {
+        if (l->st[i]) cudaStreamDestroy(l->st[i]);
+        if (l->join[i]) cudaEventDestroy(l->join[i]);
+        l->st[i] = nullptr;
+        l->join[i] = nullptr;
+    }
+    if (l->fork) cudaEventDestroy(l->fork);
+    l->fork = nullptr;
+}
+
+cudaError_t batch_launch_classes(const std::vector<ClassLaunch>& classes, cudaStream_t s, const LaunchLanes* lanes)
+{
+    for (size_t i = 0; i < classes.size();) {
+        size_t j = i;
+        while (j < classes.size() && classes[j].phase == classes[i].phase) ++j;
+        // this phase's launches, round-robin over the caller's stream and
+        // the lanes forked from it
+        const int nl = lanes ? (int)std::min<size_t>(kLaunchLanes, j - i) : 1;
+        cudaError_t e = cudaSuccess;
+        if (nl > 1) {
+            e = cudaEventRecord(lanes->fork, s);
+            for (int l = 1; l < nl && e == cudaSuccess; ++l) e = cudaStreamWaitEvent(lanes->st[l - 1], lanes->fork, 0);
+        }
+        for (size_t k = i; k < j && e == cudaSuccess; ++k) {
+            const ClassLaunch& L = classes[k];
+            if (L.tiles == 0) continue;
+            if (L.tiles > 0x7fffffffull) return cudaErrorInvalidValue;
+            const ClassKernel kn = pick_class_kernel(L.cls, L.lg);
+            if (!kn.one) return cudaErrorInvalidValue;
+            const int l = (int)((k - i) % nl);
+            cudaStream_t ls = l == 0 ? s : lanes->st[l - 1];
+            count_launch();
+            ProfScope prof(ls, "batch_class_kernel cls=%u lg=%u", L.cls, L.lg);
+            if (L.n_ce == 1)
+                kn.one<<<(unsigned)L.tiles, kn.threads, 0, ls>>>(L.first);
+            else
+                kn.many<<<(unsigned)L.tiles, kn.threads, 0, ls>>>(L.ce, L.n_ce);
+            e = cudaGetLastError();
+        }
+        for (int l = 1; l < nl && e == cudaSuccess; ++l) {
+            e = cudaEventRecord(lanes->join[l - 1], lanes->st[l - 1]);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(s, lanes->join[l - 1], 0);
+        }
+        if (e != cudaSuccess) return e;
+        i = j;
     }
     return cudaSuccess;
 }
@@ -862,7 +932,18 @@ axhel_status_t axhel_cuda_batch_launch_phased(axhel_batch_t b, void* stream)
     if (b->args.total_tiles == 0) return AXHEL_OK;
     // the error word is cleared as before a persistent launch (no wait can fail here)
     cudaError_t e = cudaMemsetAsync(static_cast<unsigned char*>(b->mem) + b->zero_off, 0, b->zero_bytes, s);
-    if (e == cudaSuccess) e = batch_launch_classes(b->classes, s);
+    if (e == cudaSuccess && !b->lanes.fork) {
+        // the lanes are made on the first launch outside a stream capture
+        // (no stream may be created while one is captured); until then a
+        // phase's launches queue on the caller's stream
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone &&
+            lanes_create(&b->lanes, 0) != cudaSuccess) {
+            lanes_destroy(&b->lanes);
+            cudaGetLastError();
+        }
+    }
+    if (e == cudaSuccess) e = batch_launch_classes(b->classes, s, b->lanes.fork ? &b->lanes : nullptr);
     if (e != cudaSuccess) return bfail(AXHEL_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
     return AXHEL_OK;
 }
@@ -911,6 +992,7 @@ axhel_status_t axhel_cuda_batch_destroy(axhel_batch_t b)
 {
     if (!b) return AXHEL_OK;
     if (b->graph) cudaGraphExecDestroy(b->graph);
+    lanes_destroy(&b->lanes);
     if (b->mem) cudaFree(b->mem);
     for (axhel_ntt_t h : b->held) axhel_cuda_ntt_release(h);
     delete b;

@@ -78,7 +78,7 @@ struct ClassEntry {
 };
 
 // One launch of a phase: the tiles of one class and pass width, from
-// every job of the batch, in entry order.
+// every job of the batch, in entry order; or one large entry alone.
 struct ClassLaunch {
     uint32_t phase, cls, lg, n_ce;
     const ClassEntry* ce;  // device address, n_ce entries
@@ -117,13 +117,25 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
 // Launches the persistent batch kernel for prepared arguments.
 cudaError_t batch_launch_args(const BatchArgs& a, cudaStream_t s);
 
+// Streams that run one phase's launches side by side: forked from the
+// caller's stream by an event and joined back into it before the next phase.
+constexpr int kLaunchLanes = 4;  // the caller's stream and three more
+struct LaunchLanes {
+    cudaStream_t st[kLaunchLanes - 1] = {};
+    cudaEvent_t fork = nullptr, join[kLaunchLanes - 1] = {};
+};
+cudaError_t lanes_create(LaunchLanes* l, int priority);
+void lanes_destroy(LaunchLanes* l);
+
 // Runs a prepared batch as ordinary (non-persistent) launches, one per
-// (phase, tile class, pass width), one CTA per tile and no waits inside a
-// launch: the phases are ordered by the stream.  Each class runs in a kernel
-// specialized for it (register depth and budget).  Concurrent batches on
-// other streams share the SMs tile by tile.  `classes` as filled by
-// batch_build.
-cudaError_t batch_launch_classes(const std::vector<ClassLaunch>& classes, cudaStream_t s);
+// (phase, tile class, pass width) plus one for each of a phase's largest
+// entries, one CTA per tile and no waits inside a launch; a phase's launches
+// run side by side on `lanes` (when given) and the phases are ordered by the
+// stream.  Each class runs in a kernel specialized for it (register depth
+// and budget).  Concurrent batches on other streams share the SMs tile by
+// tile.  `classes` as filled by batch_build.
+cudaError_t batch_launch_classes(const std::vector<ClassLaunch>& classes, cudaStream_t s,
+                                 const LaunchLanes* lanes);
 
 // Records the message returned by axhel_cuda_batch_last_error on this thread.
 void batch_set_error(const std::string& msg);

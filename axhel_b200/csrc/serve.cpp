@@ -83,6 +83,7 @@ struct Req {
 struct Slot {
     int lane = 0;  // 0: small requests (high-priority stream), 1: the rest
     cudaStream_t stream = nullptr;
+    axhel_impl::LaunchLanes lanes;  // a phase's launches side by side (same priority)
     int* err_host = nullptr;        // pinned word the kernel's error status is copied into
     unsigned char* host_img = nullptr;  // pinned staging of the batch descriptors
     size_t host_cap = 0;
@@ -215,7 +216,7 @@ axhel_status_t axhel_server::launch(Slot& s, int slot_index, std::vector<Req*>& 
     std::memcpy(s.host_img, img.data(), img.size());
     cudaError_t e = cudaMemcpyAsync(desc, s.host_img, img.size(), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
-        e = per_phase ? axhel_impl::batch_launch_classes(classes, st) : axhel_impl::batch_launch_args(args, st);
+        e = per_phase ? axhel_impl::batch_launch_classes(classes, st, &s.lanes) : axhel_impl::batch_launch_args(args, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(s.err_host, args.error, sizeof(int), cudaMemcpyDeviceToHost, st);
     // results back smallest first; each request completes at its own event
     std::vector<Req*> order(take);
@@ -401,6 +402,7 @@ axhel_status_t axhel_server_create(const axhel_server_config_t* cfg, axhel_serve
         sl.lane = s->lanes == 2 ? (int)(i / cfg->max_inflight) : 1;
         const int prio = sl.lane == 0 ? prio_high : prio_low;
         if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&sl.stream, cudaStreamNonBlocking, prio);
+        if (e == cudaSuccess) e = axhel_impl::lanes_create(&sl.lanes, prio);
         if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&sl.err_host), sizeof(int));
         // descriptor staging for batches of up to a few hundred requests,
         // allocated now rather than on a slot's first batch
@@ -419,6 +421,7 @@ axhel_status_t axhel_server_create(const axhel_server_config_t* cfg, axhel_serve
     if (e != cudaSuccess) {
         for (Slot& sl : s->slots) {
             if (sl.stream) cudaStreamDestroy(sl.stream);
+            axhel_impl::lanes_destroy(&sl.lanes);
             if (sl.err_host) cudaFreeHost(sl.err_host);
             if (sl.host_img) cudaFreeHost(sl.host_img);
         }
@@ -562,6 +565,7 @@ axhel_status_t axhel_server_destroy(axhel_server_t s)
     for (Slot& sl : s->slots) {
         cudaStreamSynchronize(sl.stream);
         cudaStreamDestroy(sl.stream);
+        axhel_impl::lanes_destroy(&sl.lanes);
         cudaFreeHost(sl.err_host);
         if (sl.host_img) cudaFreeHost(sl.host_img);
         for (unsigned char* r : sl.retired) cudaFreeHost(r);

@@ -338,7 +338,7 @@ def run_ours(args):
 
         serve = {}
         for mode, device in (("host_staged", False), ("device_resident", True)):
-            r = workloads.serving(loads=(0.7,), seconds=2.0, n_templates=24, device=device, plain=True,
+            r = workloads.serving(loads=(0.7,), seconds=4.0, n_templates=24, device=device, plain=True,
                                   small_words=0, inflight=4)
             l = r["loads"][0]
             serve[mode] = {"capacity_jobs_per_s": r["capacity_jobs_per_s"], "jobs_per_s_at_70pct": l["jobs_per_s"],

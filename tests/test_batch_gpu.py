@@ -195,3 +195,31 @@ def test_relaunches_stay_bit_identical(cuda, oracle):
         assert b.status() == 0
         assert all(torch.equal(r, o) for r, (_, o, _) in zip(ref, bufs)), f"relaunch {rep}"
     b.close()
+
+
+def test_phased_launch_replays_from_a_captured_graph(cuda, oracle):
+    """The per-phase launches fork each phase over extra streams and join
+    them back into the caller's stream: captured into a CUDA graph on that
+    stream, the batch replays to its oracle-checked result."""
+    import torch
+
+    rng = np.random.default_rng(2024)
+    jobs = make_jobs(cuda, oracle, rng, 12, [12, 14, 16, 17], 4, 4)
+    specs, bufs = specs_for(cuda, jobs)
+    b = cuda.Batch(specs)
+    b.launch(phased=True)
+    assert b.status() == 0
+    check(oracle, jobs, bufs)
+    ref = [o.clone() for _, o, _ in bufs]
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        b.launch(stream=s.cuda_stream, phased=True)
+    for rep in range(4):
+        for _, o, _ in bufs:
+            o.fill_(-1)
+        g.replay()
+        torch.cuda.synchronize()
+        assert all(torch.equal(r, o) for r, (_, o, _) in zip(ref, bufs)), f"replay {rep}"
+    del g
+    b.close()
