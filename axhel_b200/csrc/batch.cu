@@ -1,4 +1,4 @@
-// Uneven batches in one persistent launch.
+// Uneven batches: one persistent launch, or ordinary launches phase by phase.
 //
 // A batch mixes jobs of different degree N (2^10 .. 2^17), limb count and
 // kind: forward NTT, inverse NTT, the fused INTT -> MulMod/FMAMod -> NTT
@@ -30,9 +30,13 @@
 // barrier ordered before it), by a thread of another warp than the one that
 // claims and checks the next tile, which waits on nothing before it.
 //
-// Each tile is 1024 residues handled by 128 threads x 8 registers
-// (LR = 3): 2^(10-LG) groups of 2^LG for the pass widths LG = 5..9 of the
-// degrees 2^10 .. 2^17 (a tile never spans two limbs or two blocks).
+// Each tile is 1024 residues: 2^(10-LG) groups of 2^LG for the pass widths
+// LG = 5..9 of the degrees 2^10 .. 2^17 (a tile never spans two limbs or two
+// blocks), handled by 128 threads x 8 registers (LR = 3) in the persistent
+// kernel.  The per-phase launches run one kernel per tile class and pass
+// width (64 threads x 16 registers for the transform passes narrower than 9
+// stages), each phase's largest entries in launches of their own that take
+// the entry as a kernel parameter, side by side on extra streams.
 // The same tile functions as the plain kernels run the butterflies
 // (ntt_kernels.cuh), so every job's result equals the per-limb calls bit for
 // bit.

@@ -16,16 +16,17 @@ namespace axhel_impl {
 constexpr int kBatchThreads = 128;
 constexpr int kBatchLR = 3;
 constexpr int kBatchTileWords = kBatchThreads << kBatchLR;  // 1024 residues
-constexpr int kBatchTileLog = 10;
-constexpr int kBatchPublisher = 32;                         // persistent kernel: the thread that publishes tiles
-static_assert(kBatchThreads > kBatchPublisher, "publisher in a second warp");                           // tiles per limb: 2^(logn - 10)
+constexpr int kBatchTileLog = 10;                           // tiles per limb: 2^(logn - 10)
 static_assert(kBatchTileWords == 1 << kBatchTileLog, "tile size");
+constexpr int kBatchPublisher = 32;                         // persistent kernel: the thread that publishes tiles
+static_assert(kBatchThreads > kBatchPublisher, "publisher in a second warp");
 constexpr int kBatchMinLG = 5, kBatchMaxLG = 9;
-// CTAs per SM the kernels are compiled for: 64 registers (128 without the
-// bound) and some spills, which cost less than the latency the extra resident
-// warps hide -- measured on the 512-polynomial uneven batch: 5 CTAs 1.08 M /
-// 1.28 M limb-transforms/s (persistent / per phase), 7 CTAs 1.25 M / 1.36 M,
-// 8 CTAs 1.29 M / 1.46 M.
+// CTAs per SM the persistent kernel (and the grouped per-phase launches of
+// 128 threads) are compiled for: 64 registers (128 without the bound) and
+// some spills, which cost less than the latency the extra resident warps
+// hide -- measured on the 512-polynomial uneven batch with the generic
+// kernels: 5 CTAs 1.08 M / 1.28 M limb-transforms/s (persistent / per
+// phase), 7 CTAs 1.25 M / 1.36 M, 8 CTAs 1.29 M / 1.46 M.
 constexpr int kBatchMinBlocks = 8;
 
 enum BatchKind : uint32_t {
