@@ -127,7 +127,9 @@ def tune(lognums, buckets, limbs_cap_bytes=1 << 30, verbose=True):
 
 def tune_batch(lognums, bytes_per_job=128 << 20, reps=5, verbose=True):
     """Per degree, the batch engine's contiguous-pass width that runs a
-    forward, an inverse and a chained job of ~128 MiB each fastest."""
+    forward, an inverse and a chained job of ~128 MiB each fastest: the sum
+    of the persistent launch's and the per-phase launches' times (one split
+    serves both forms)."""
     import torch
 
     from axhel_b200 import capi, params
@@ -154,20 +156,23 @@ def tune_batch(lognums, bytes_per_job=128 << 20, reps=5, verbose=True):
         for row in range(max(5, logn - 9), min(9, logn - 5) + 1):
             capi.batch_split_set(logn, row)
             b = capi.Batch(specs)
-            b.launch()
-            torch.cuda.synchronize()
-            ts = []
-            for _ in range(reps):
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record()
-                b.launch()
-                e1.record()
+            form_ms = []
+            for phased in (False, True):
+                b.launch(phased=phased)
                 torch.cuda.synchronize()
-                ts.append(e0.elapsed_time(e1))
+                ts = []
+                for _ in range(reps):
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    b.launch(phased=phased)
+                    e1.record()
+                    torch.cuda.synchronize()
+                    ts.append(e0.elapsed_time(e1))
+                form_ms.append(statistics.median(ts))
             b.close()
-            ms = statistics.median(ts)
+            ms = sum(form_ms)
             if verbose:
-                print(f"batch logn={logn} row={row}: {ms:.3f} ms ({4 * count / (ms / 1e3):,.0f} limb-transforms/s)",
+                print(f"batch logn={logn} row={row}: persistent {form_ms[0]:.3f} ms, per phase {form_ms[1]:.3f} ms",
                       flush=True)
             if best is None or ms < best[0]:
                 best = (ms, row)

@@ -778,11 +778,13 @@ struct ClassKernel {
 };
 
 // Register depth per class and width: 4 (64 threads per tile) for the
-// transform passes narrower than 9 stages, 3 (128 threads) otherwise.
+// 7-stage transform passes, 3 (128 threads) otherwise -- measured per width
+// on the per-phase launches: 4 is 5 % faster at 7 stages, 3 is 8 % faster
+// at 8 stages and 15-22 % faster at 5 and 6.
 template <int CLS, int LG>
 ClassKernel class_kernel()
 {
-    constexpr int LR = (CLS == kClsFwd || CLS == kClsInv) && LG < 9 ? 4 : 3;
+    constexpr int LR = (CLS == kClsFwd || CLS == kClsInv) && LG == 7 ? 4 : 3;
     return ClassKernel{batch_class_one_kernel<CLS, LG, LR>, batch_class_kernel<CLS, LG, LR>,
                        (unsigned)(kBatchTileWords >> LR)};
 }
