@@ -223,3 +223,26 @@ def test_phased_launch_replays_from_a_captured_graph(cuda, oracle):
         assert all(torch.equal(r, o) for r, (_, o, _) in zip(ref, bufs)), f"replay {rep}"
     del g
     b.close()
+
+
+def test_phased_large_entries_alone_and_grouped(cuda, oracle):
+    """Entries of 512 tiles or more (here 4-8 limbs at N = 2^16, 2^17) get
+    per-phase launches of their own beside the grouped small entries, spread
+    over the extra streams; every kind matches its per-limb calls, and the
+    persistent launch of the same batch gives the same bits."""
+    import torch
+
+    rng = np.random.default_rng(4242)
+    jobs = make_jobs(cuda, oracle, rng, 6, [16, 17], 8, 3) + make_jobs(cuda, oracle, rng, 10, [10, 11, 12, 13], 3, 3)
+    specs, bufs = specs_for(cuda, jobs)
+    b = cuda.Batch(specs)
+    b.launch(phased=True)
+    assert b.status() == 0
+    check(oracle, jobs, bufs)
+    ref = [o.clone() for _, o, _ in bufs]
+    for _, o, _ in bufs:
+        o.fill_(-1)
+    b.launch()
+    assert b.status() == 0
+    assert all(torch.equal(r, o) for r, (_, o, _) in zip(ref, bufs))
+    b.close()
