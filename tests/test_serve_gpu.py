@@ -71,9 +71,11 @@ SPECS = [(13, 4, 4, 3), (14, 2, 2, 4), (15, 6, 6, 3), (16, 3, 3, 4), (17, 2, 2, 
          (12, 3, 3, 4)]
 
 
-def test_same_bits_alone_and_in_a_mix(cuda, oracle):
+@pytest.mark.parametrize("cfg", [{}, {"persistent": True}, {"small_request_words": 1 << 16}],
+                         ids=["per-phase", "persistent", "two-lanes"])
+def test_same_bits_alone_and_in_a_mix(cuda, oracle, cfg):
     reqs = make_requests(cuda, oracle, 5, SPECS)
-    srv = cuda.Server(budget_bytes=8 << 30, max_inflight=2, max_batch_requests=64)
+    srv = cuda.Server(budget_bytes=8 << 30, max_inflight=2, max_batch_requests=64, **cfg)
     alone = []
     for k, r in enumerate(reqs):  # one at a time on an idle server
         rid, bufs = submit(srv, r, on_device=k % 2 == 0)
