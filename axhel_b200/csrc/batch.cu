@@ -67,7 +67,8 @@ __device__ __forceinline__ uint64_t global_ns()
     return t;
 }
 
-// Per-phase pass of a job: direction, width and first stage.
+// Per-phase pass of a transform job: direction, width and first stage
+// (chain: inverse row pass, fused column pass, forward row pass).
 struct PhaseCfg {
     bool inv, chain;
     uint32_t lg, s0;
@@ -103,8 +104,8 @@ inline PhaseCfg phase_cfg(const BatchJob& j, uint32_t p)
 // Element-wise job tile: 1024 residues of one limb, 8 per thread at a
 // stride of the CTA width (every warp access is 256 contiguous bytes); all
 // loads are issued before the first store.
-template <bool HAS_B, class J, class Op>
-__device__ __forceinline__ void elt_tile(const J& j, uint64_t base, const Op& op)
+template <bool HAS_B, class Op>
+__device__ __forceinline__ void elt_tile(const ClassEntry& j, uint64_t base, const Op& op)
 {
     constexpr int kPer = kBatchTileWords / kBatchThreads;
     uint64_t a[kPer], b[kPer];
@@ -117,8 +118,8 @@ __device__ __forceinline__ void elt_tile(const J& j, uint64_t base, const Op& op
     for (int k = 0; k < kPer; ++k) j.dst[base + (uint64_t)k * kBatchThreads] = op(a[k], b[k]);
 }
 
-template <bool ADD, class J>
-__device__ __forceinline__ void elt_fma(const J& j, uint64_t base, uint64_t q, uint64_t mu, uint64_t s,
+template <bool ADD>
+__device__ __forceinline__ void elt_fma(const ClassEntry& j, uint64_t base, uint64_t q, uint64_t mu, uint64_t s,
                                         uint32_t sh)
 {
     switch (j.ef) {
@@ -129,10 +130,8 @@ __device__ __forceinline__ void elt_fma(const J& j, uint64_t base, uint64_t q, u
     }
 }
 
-// The element-wise job's op on one tile, with limb `limb`'s modulus (J: a
-// BatchJob or a ClassEntry).
-template <class J>
-__device__ __forceinline__ void run_elt_tile(const J& j, uint64_t limb, uint64_t til)
+// The element-wise job's op on one tile, with limb `limb`'s modulus.
+__device__ __forceinline__ void run_elt_tile(const ClassEntry& j, uint64_t limb, uint64_t til)
 {
     const uint32_t mi = limb_mod(limb, j.nmods);
     const ModCtx* cx = j.ctx[mi];
@@ -558,12 +557,8 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
         b.pre = inv_first && J.input_mod_factor == 4;
         b.norm = (J.kind == AXHEL_JOB_INVERSE) ? (J.output_mod_factor != 2) : (J.output_mod_factor != 4);
         b.nphase = (J.kind == AXHEL_JOB_CHAIN_MUL || J.kind == AXHEL_JOB_CHAIN_FMA) ? 3 : 2;
-        const uint32_t lgs_fwd[2] = {b.lg_col, b.lg_row};
         for (uint32_t p = 0; p < b.nphase; ++p) {
-            uint32_t lg;
-            if (J.kind == AXHEL_JOB_FORWARD) lg = lgs_fwd[p];
-            else if (J.kind == AXHEL_JOB_INVERSE) lg = p == 0 ? b.lg_row : b.lg_col;
-            else lg = p == 1 ? b.lg_col : b.lg_row;
+            const uint32_t lg = phase_cfg(b, p).lg;
             if (lg < (uint32_t)kBatchMinLG || lg > (uint32_t)kBatchMaxLG || (1ull << logn) % kBatchTileWords) {
                 *err = "job " + std::to_string(i) + ": degree outside the batched range";
                 return AXHEL_ERR_UNSUPPORTED;
@@ -589,30 +584,21 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
         args->total_tiles = 0;
         return AXHEL_OK;
     }
-    // per (phase, class, pass width): the entries, in order, with their
-    // first tile in that launch's numbering
     // every entry's tile class and pass width
     std::vector<uint32_t> ent_cls(ent.size()), ent_lg(ent.size());
     for (size_t k = 0; k < ent.size(); ++k) {
-        const BatchEntry& e = ent[k];
-        const BatchJob& b = bj[e.job];
-        uint32_t cls, lg;
+        const BatchJob& b = bj[ent[k].job];
         if (b.kind >= kJobAdd) {
-            cls = kClsElt;
-            lg = 0;
-        } else if (b.kind == kJobForward) {
-            cls = kClsFwd;
-            lg = e.phase == 0 ? b.lg_col : b.lg_row;
-        } else if (b.kind == kJobInverse) {
-            cls = kClsInv;
-            lg = e.phase == 0 ? b.lg_row : b.lg_col;
-        } else {  // chain: inverse row pass, fused column pass, forward row pass
-            cls = e.phase == 0 ? kClsInv : (e.phase == 1 ? kClsChain : kClsFwd);
-            lg = e.phase == 1 ? b.lg_col : b.lg_row;
+            ent_cls[k] = kClsElt;
+            ent_lg[k] = 0;
+            continue;
         }
-        ent_cls[k] = cls;
-        ent_lg[k] = lg;
+        const PhaseCfg pc = phase_cfg(b, ent[k].phase);
+        ent_cls[k] = pc.chain ? kClsChain : (pc.inv ? kClsInv : kClsFwd);
+        ent_lg[k] = pc.lg;
     }
+    // per (phase, class, pass width): the entries, in order, with their
+    // first tile in that launch's numbering
     std::vector<ClassLaunch> cl;
     std::vector<std::vector<ClassEntry>> cl_ent;
     std::vector<std::vector<uint32_t>> cl_idx;  // the batch entry of each class entry
