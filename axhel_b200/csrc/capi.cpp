@@ -236,15 +236,15 @@ axhel_status_t axhel_cuda_ntt_create_many(uint64_t count, const uint64_t* degree
     // cache hits take a reference; misses (each distinct key once) get an
     // allocation and a generation job
     std::map<std::tuple<int, uint64_t, uint64_t, uint64_t>, axhel_ntt_ctx*> fresh;
+    std::vector<axhel_ntt_ctx*> order;  // the fresh contexts, in creation order
     std::vector<TableGenJob> jobs;
+    void* block = nullptr;
     auto undo = [&](axhel_status_t st, const std::string& m) {
         for (uint64_t i = 0; i < count; ++i)
             if (out[i] && out[i]->cached && !fresh.count(std::make_tuple(dev, degrees[i], moduli[i], roots[i])))
                 out[i]->refs.fetch_sub(1);
-        for (auto& kv : fresh) {
-            if (kv.second->mem) cudaFree(kv.second->mem);
-            delete kv.second;
-        }
+        for (auto& kv : fresh) delete kv.second;
+        if (block) cudaFree(block);
         for (uint64_t i = 0; i < count; ++i) out[i] = nullptr;
         return fail(st, m);
     };
@@ -272,14 +272,28 @@ axhel_status_t axhel_cuda_ntt_create_many(uint64_t count, const uint64_t* degree
         c->refs.store(2);  // the cache keeps one reference: tables stay resident for the process
         fresh[key] = c;
         out[i] = c;
-        e = cudaMalloc(&c->mem, kHeader + 2 * c->n * 16);
-        if (e != cudaSuccess) {
-            c->mem = nullptr;
-            return undo(AXHEL_ERR_NOMEM, std::string("cudaMalloc(tables): ") + cudaGetErrorString(e));
-        }
+        order.push_back(c);
+    }
+    // One device block for all the fresh contexts' headers and tables: cached
+    // contexts stay resident for the process, and one cudaMalloc instead of
+    // one per context is most of a cold start's host time.
+    std::vector<size_t> offs(order.size());
+    size_t total = 0;
+    for (size_t k = 0; k < order.size(); ++k) {
+        offs[k] = total;
+        total += (kHeader + 2 * order[k]->n * 16 + 255) / 256 * 256;
+    }
+    if (total && (e = cudaMalloc(&block, total)) != cudaSuccess) {
+        block = nullptr;
+        return undo(AXHEL_ERR_NOMEM, std::string("cudaMalloc(tables): ") + cudaGetErrorString(e));
+    }
+    for (size_t k = 0; k < order.size(); ++k) {
+        axhel_ntt_ctx* c = order[k];
+        c->mem = static_cast<unsigned char*>(block) + offs[k];
+        c->shared_mem = true;
         c->dctx = reinterpret_cast<const ModCtx*>(c->mem);
         jobs.emplace_back();
-        gen_job(c, roots[i], &jobs.back());
+        gen_job(c, c->root, &jobs.back());
     }
     // one launch per 96 contexts, then wait: the tables are complete when
     // this returns, for any stream of any thread
@@ -330,7 +344,7 @@ axhel_status_t axhel_cuda_ntt_release(axhel_ntt_t h)
 {
     if (!h) return AXHEL_OK;
     if (h->refs.fetch_sub(1) == 1) {
-        if (h->mem) cudaFree(h->mem);
+        if (h->mem && !h->shared_mem) cudaFree(h->mem);
         delete h;
     }
     return AXHEL_OK;

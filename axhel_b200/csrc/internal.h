@@ -98,5 +98,6 @@ struct axhel_ntt_ctx {
     int device = 0;
     bool cached = false;
     void* mem = nullptr;                       // device allocation
+    bool shared_mem = false;                   // mem lies in one block with the contexts created beside it
     const axhel_impl::ModCtx* dctx = nullptr;  // device address of the ModCtx header
 };
