@@ -408,16 +408,19 @@ def kernel_case(family):
     import torch
 
     rng = np.random.default_rng(1)
-    if family == "eltwise":  # add, mul, fma, Barrett reduce on 2^24 elements, twice
+    if family in ("eltwise", "eltwise_unaligned"):  # add, mul, fma, Barrett reduce on 2^24 elements, twice
         n = 1 << 24
         q = params.ntt_prime_near(1 << 16, 50, 1, 1)
         a, b, c = (_dev(rng.integers(0, q, n, dtype=np.uint64)) for _ in range(3))
         r = torch.empty_like(a)
+        off = 8 if family == "eltwise_unaligned" else 0  # 8-byte aligned operands: the scalar kernel
+        m = n - 1 if off else n
+        pa, pb, pc, pr = (t.data_ptr() + off for t in (a, b, c, r))
         for _ in range(2):
-            capi.add(r.data_ptr(), a.data_ptr(), b.data_ptr(), n, q)
-            capi.mul(r.data_ptr(), a.data_ptr(), b.data_ptr(), n, q, 1)
-            capi.fma(r.data_ptr(), a.data_ptr(), 12345, c.data_ptr(), n, q, 1)
-            capi.reduce(r.data_ptr(), a.data_ptr(), n, q, q, 1)
+            capi.add(pr, pa, pb, m, q)
+            capi.mul(pr, pa, pb, m, q, 1)
+            capi.fma(pr, pa, 12345, pc, m, q, 1)
+            capi.reduce(pr, pa, m, q, q, 1)
     elif family == "tensor":  # 16 pairs x 16 limbs of N = 2^15
         L, n, pairs = 16, 1 << 15, 16
         qs = [q for q, _ in params.rns_moduli(n, L, 40, 55)]
@@ -459,7 +462,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("what", choices=["tensor", "uneven", "serve", "eltwise", "case"])
     ap.add_argument("family", nargs="?", default="eltwise",
-                    help="case: eltwise | tensor | tables | chain | batch | batch_phased | batch_eltwise")
+                    help="case: eltwise | eltwise_unaligned | tensor | tables | chain | batch | batch_phased | "
+                         "batch_eltwise")
     ap.add_argument("--seconds", type=float, default=4.0)
     ap.add_argument("--device", action="store_true", help="device-resident request operands")
     ap.add_argument("--persistent", action="store_true", help="one persistent launch per batch")

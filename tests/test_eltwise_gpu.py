@@ -242,3 +242,32 @@ def test_large_vectors_all_ops_match_oracle(cuda, oracle):
     np.testing.assert_array_equal(host(do, n), oracle.fma(a, 12345, b, q, 4))
     cuda.reduce(ptr(do), ptr(da), n, q, 4, 1)
     np.testing.assert_array_equal(host(do, n), oracle.reduce(a, q, 4, 1))
+
+
+@pytest.mark.parametrize("in_place", [False, True])
+def test_unaligned_large_all_ops(cuda, oracle, in_place):
+    """8-byte aligned (not 16-byte) operands long enough for the unaligned
+    kernel's four-elements-per-thread steps and its tail: every op against
+    the oracle, out of place and in place (result aliasing the first operand)."""
+    q = oracle.find_ntt_prime(1 << 16, 59)
+    n = (1 << 21) + 5
+    st = oracle.rng(SEED ^ 0x51)
+    a = oracle.random_vector(st, n, 2 * q)
+    b = oracle.random_vector(st, n, 2 * q)
+    c = oracle.random_vector(st, n, q)
+    cases = [
+        (lambda o, x, y, z: cuda.add(o, x, z, n, q), lambda: oracle.add(a % q, c, q), True),
+        (lambda o, x, y, z: cuda.sub(o, x, z, n, q), lambda: oracle.sub(a % q, c, q), True),
+        (lambda o, x, y, z: cuda.mul(o, x, y, n, q, 2), lambda: oracle.mul(a, b, q, 2), False),
+        (lambda o, x, y, z: cuda.fma(o, x, 12345, z, n, q, 2), lambda: oracle.fma(a, 12345, c, q, 2), False),
+        (lambda o, x, y, z: cuda.reduce(o, x, n, q, q, 1), lambda: oracle.reduce(a, q, q, 1), False),
+    ]
+    for k, (run, want, canonical_a) in enumerate(cases):
+        x = a % q if canonical_a else a
+        da, db, dc = dev_empty(n + 1), dev_empty(n + 1), dev_empty(n + 1)
+        da[1:] = dev(x)[:n]
+        db[1:] = dev(b)[:n]
+        dc[1:] = dev(c)[:n]
+        do = da if in_place else dev_empty(n + 1, fill=0)
+        run(ptr(do, 1), ptr(da, 1), ptr(db, 1), ptr(dc, 1))
+        np.testing.assert_array_equal(host(do, n + 1)[1:], want(), err_msg=f"op {k} in_place={in_place}")
