@@ -34,9 +34,9 @@
 // LG = 5..9 of the degrees 2^10 .. 2^17 (a tile never spans two limbs or two
 // blocks), handled by 128 threads x 8 registers (LR = 3) in the persistent
 // kernel.  The per-phase launches run one kernel per tile class and pass
-// width (64 threads x 16 registers for the transform passes narrower than 9
-// stages), each phase's largest entries in launches of their own that take
-// the entry as a kernel parameter, side by side on extra streams.
+// width (64 threads x 16 registers for the 7-stage transform passes), each
+// phase's largest entries in launches of their own that take the entry as a
+// kernel parameter, side by side on extra streams.
 // The same tile functions as the plain kernels run the butterflies
 // (ntt_kernels.cuh), so every job's result equals the per-limb calls bit for
 // bit.
@@ -165,8 +165,8 @@ __device__ __forceinline__ void run_elt_tile(const ClassEntry& j, uint64_t limb,
 
 // One tile of class CLS and pass width LG with LR register stages; the
 // entry carries the pass's operands, first stage and flags (built on the
-// host from the job).  The strided and contiguous passes take 64 threads x 16
-// registers per 1024-residue tile when LR = 4.  CG: loads bypass L1, for
+// host from the job).  With LR = 4 a 1024-residue tile takes 64 threads x 16
+// registers.  CG: loads bypass L1, for
 // data written by other CTAs of the same launch (the persistent kernel); the
 // per-phase launches read what an earlier launch wrote and load plainly.
 template <int CLS, int LG, int LR, bool CG>
