@@ -197,8 +197,11 @@ axhel_status_t axhel_cuda_batch_launch(axhel_batch_t batch, void* stream);
 axhel_status_t axhel_cuda_batch_graph_launch(axhel_batch_t batch, void* stream);
 /* Runs the batch as ordinary launches, phase after phase: one per (phase,
  * tile class, pass width), each a grid of that class's tiles of all jobs,
- * one CTA per tile, no waits inside a launch; same results; may be captured
- * into a CUDA graph. */
+ * plus one for each of a phase's largest jobs; one CTA per tile, no waits
+ * inside a launch; same results.  A phase's launches run side by side on
+ * three streams the batch creates on its first call outside a stream
+ * capture, forked from `stream` by an event and joined back into it; may be
+ * captured into a CUDA graph on `stream`. */
 axhel_status_t axhel_cuda_batch_launch_phased(axhel_batch_t batch, void* stream);
 /* Waits for `stream` and returns AXHEL_ERR_TIMEOUT if a dependency wait
  * inside the kernel gave up (bounded at 2 s), else AXHEL_OK. */
