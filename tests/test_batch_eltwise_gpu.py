@@ -125,3 +125,29 @@ def test_single_job_batches_per_phase_every_kind(cuda, oracle):
         assert b.status() == 0
         np.testing.assert_array_equal(host(bufs[0][1], jb["x"].size), want(oracle, jb))
         b.close()
+
+
+def test_random_mixed_batches_both_forms(cuda, oracle):
+    """Seeded random batches: 1-11 transform and chain jobs over up to three
+    degrees, 0-3 element-wise jobs, in shuffled order; the persistent launch
+    and the per-phase launches each match the reference's per-limb calls."""
+    for seed in range(24):
+        rng = np.random.default_rng(50000 + seed)
+        logns = sorted(set(int(x) for x in rng.integers(10, 18, 3)))
+        jobs = tb.make_jobs(cuda, oracle, rng, int(rng.integers(1, 12)), logns, int(rng.integers(1, 10)),
+                            int(rng.integers(1, 5)))
+        ejobs = elt_jobs(cuda, oracle, 7000 + seed, logns=(10, 12), L=2,
+                         count=int(rng.integers(1, 4)))[: int(rng.integers(0, 4))]
+        for phased in (False, True):
+            specs, bufs = tb.specs_for(cuda, jobs)
+            especs, ebufs = elt_specs(cuda, ejobs)
+            every = specs + especs
+            order = rng.permutation(len(every))
+            b = cuda.Batch([every[i] for i in order])
+            b.launch(phased=phased)
+            assert b.status() == 0
+            b.close()
+            tb.check(oracle, jobs, bufs)
+            for jb, (d, o, dv) in zip(ejobs, ebufs):
+                np.testing.assert_array_equal(host(o, jb["x"].size), want(oracle, jb),
+                                              err_msg=f"seed {seed} phased={phased}")
