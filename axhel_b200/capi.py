@@ -38,12 +38,14 @@ class Job(C.Structure):
 
 
 SERVER_PERSISTENT = 1
+SERVER_ARRIVAL_PRIORITY = 2
+SERVER_SMALLEST_FIRST = 4
 
 
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_batch_words", C.c_uint64),
                 ("small_request_words", C.c_uint64), ("max_inflight", C.c_uint32),
-                ("max_batch_requests", C.c_uint32), ("flags", C.c_uint32), ("reserved", C.c_uint32),
+                ("max_batch_requests", C.c_uint32), ("flags", C.c_uint32), ("aging_us", C.c_uint32),
                 ("reserve_bytes", C.c_uint64)]
 
 
@@ -64,7 +66,8 @@ class RequestInfo(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [("completed", C.c_uint64), ("batches", C.c_uint64), ("max_batch_requests", C.c_uint64),
                 ("pending", C.c_uint64), ("in_use_bytes", C.c_uint64), ("peak_in_use_bytes", C.c_uint64),
-                ("samples", C.c_uint64), ("p50_ms", C.c_double), ("p99_ms", C.c_double)]
+                ("samples", C.c_uint64), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
+                ("pool_used_bytes", C.c_uint64)]
 
 
 class DriveResult(C.Structure):
@@ -157,6 +160,7 @@ def _declare(L):
     d("axhel_server_drive", st_t, vp, C.POINTER(Request), C.c_uint32, C.POINTER(C.c_void_p), C.c_uint32,
       C.POINTER(C.c_double), C.c_double, C.c_double, u64, C.POINTER(DriveResult))
     d("axhel_cuda_batch_debug_unreachable", st_t, vp, u64)
+    d("axhel_server_debug_fail_staging", st_t, vp, u32)
 
 
 def check(status, where):
@@ -279,9 +283,10 @@ class Server:
     """The continuous-batching serving loop (axhel_server_*)."""
 
     def __init__(self, budget_bytes, max_inflight=2, max_batch_requests=256, max_batch_words=0, persistent=False,
-                 small_request_words=0, reserve_bytes=0):
+                 small_request_words=0, reserve_bytes=0, flags=0, aging_us=0):
+        flags |= SERVER_PERSISTENT if persistent else 0
         cfg = ServerConfig(budget_bytes, max_batch_words, small_request_words, max_inflight, max_batch_requests,
-                           SERVER_PERSISTENT if persistent else 0, 0, reserve_bytes)
+                           flags, aging_us, reserve_bytes)
         self.h = vp()
         _scheck(lib().axhel_server_create(C.byref(cfg), C.byref(self.h)), "server_create")
         self._keep = {}
@@ -313,6 +318,10 @@ class Server:
 
     def pause(self, paused=True):
         _scheck(lib().axhel_server_pause(self.h, 1 if paused else 0), "server_pause")
+
+    def debug_fail_staging(self, request):
+        """The next batch's staging fails at its request `request` (tests)."""
+        _scheck(lib().axhel_server_debug_fail_staging(self.h, request), "server_debug_fail_staging")
 
     def stats(self, reset=False):
         s = ServerStats()

@@ -44,6 +44,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -372,16 +373,24 @@ namespace {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// Persistent grid of the current device: resident CTAs per SM x SMs, kept
+// per device index (threads that race on the first call store the same
+// value).
 int batch_grid()
 {
-    static int cached = 0;
-    if (!cached) {
+    static std::atomic<int> cached[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const bool keep = dev >= 0 && dev < 64;
+    int g = keep ? cached[dev].load(std::memory_order_relaxed) : 0;
+    if (!g) {
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, kBatchThreads, 0);
         if (per_sm < 1) per_sm = 1;
-        cached = per_sm * sm_count();
+        g = per_sm * sm_count();
+        if (keep) cached[dev].store(g, std::memory_order_relaxed);
     }
-    return cached;
+    return g;
 }
 
 }  // namespace

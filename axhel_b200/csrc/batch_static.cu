@@ -15,7 +15,11 @@
 // The array's name is a host-side stand-in in host code, not a device
 // address: the first call on each device resolves the device address with
 // cudaGetSymbolAddress while that device is current, and later calls reuse
-// it.  Make that first call before any stream capture.
+// it.  Make that first call before any stream capture.  The resolved address
+// belongs to the device's context as it was then: after a cudaDeviceReset
+// the module may be loaded again elsewhere, so this entry point must not be
+// used across a reset of the device.  Every call waits for its batch to
+// finish (it reads the error word back) before it returns.
 //
 // Every call shares the one array and leaves its contents behind; each call
 // rewrites the descriptors and clears the counters it uses (they travel in

@@ -62,16 +62,16 @@ namespace axhel_impl {
 
 int sm_count()
 {
-    static int cache[64] = {0};
+    static std::atomic<int> cache[64];
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return 148;
-    if (!cache[dev]) {
-        int n = 0;
+    int n = cache[dev].load(std::memory_order_relaxed);
+    if (!n) {
         if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
-        cache[dev] = n;
+        cache[dev].store(n, std::memory_order_relaxed);
     }
-    return cache[dev];
+    return n;
 }
 
 }  // namespace axhel_impl

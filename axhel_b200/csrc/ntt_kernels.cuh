@@ -513,11 +513,8 @@ __device__ __forceinline__ void chain_tile(const uint64_t* src, uint64_t* dst, c
     store_global<LG, LR, LO_LAST>(v, ldst, t, gi, round_base<LR>(k, LO_LAST), vec_ok);
 }
 
-// Fused column pass of an INTT -> op -> NTT chain: the inverse's last pass
-// (stages logn-LG .. logn-1, incl. the N^-1 final stage) and the forward's
-// first pass (stages 0 .. LG-1) act on the same groups p = r*S + col, and the
-// inverse's last round holds the same register bits as the forward's first
-// round, so the element-wise op runs in registers between them.
+// Kernel of the fused chain pass: one CTA per tile of chain_tile above; the
+// modulus context and the FMA scalar follow the limb.
 template <int LG, int LR>
 __global__ void __launch_bounds__(max_threads(LR)) ntt_chain_kernel(const __grid_constant__ ChainArgs c)
 {

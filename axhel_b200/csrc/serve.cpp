@@ -120,6 +120,7 @@ struct axhel_server {
     std::thread sched, comp;
     std::string fatal;
     std::vector<cudaEvent_t> event_pool;  // reused completion events
+    std::atomic<int> debug_fail_at{-1};   // failure injection: staging of the next batch fails at this request
 
     cudaEvent_t get_event()
     {
@@ -139,32 +140,56 @@ struct axhel_server {
     axhel_status_t launch(Slot& s, int slot_index, std::vector<Req*>& take, Inflight& f);
 };
 
+// Gives back to the pool, in stream order on `st`, every buffer staged for
+// take[0 .. n): after a failure part-way through a batch, nothing it staged
+// stays allocated while the scheduler returns its bytes to the budget.
+static void unstage(cudaStream_t st, const std::vector<Req*>& take, size_t n)
+{
+    for (size_t i = 0; i < n && i < take.size(); ++i) {
+        Req* q = take[i];
+        if (!q->in_dev && q->d_in) cudaFreeAsync(q->d_in, st);
+        if (!q->out_dev && q->d_out && q->d_out != q->d_in) cudaFreeAsync(q->d_out, st);
+        if (!q->vec_dev && q->d_vec) cudaFreeAsync(q->d_vec, st);
+        q->d_in = q->d_out = q->d_vec = nullptr;
+    }
+}
+
 axhel_status_t axhel_server::launch(Slot& s, int slot_index, std::vector<Req*>& take, Inflight& f)
 {
     cudaStream_t st = s.stream;
     std::vector<axhel_job_t> jobs(take.size());
+    const int fail_at = debug_fail_at.exchange(-1);  // failure injection (tests): one batch
     for (size_t i = 0; i < take.size(); ++i) {
         Req* q = take[i];
         const size_t bytes = q->words * 8;
-        q->d_in = const_cast<uint64_t*>(q->r.input);
-        q->d_out = q->r.output;
-        q->d_vec = const_cast<uint64_t*>(q->r.vector);
+        // device operands are used in place; host ones get pool buffers
+        q->d_in = q->in_dev ? const_cast<uint64_t*>(q->r.input) : nullptr;
+        q->d_out = q->out_dev ? q->r.output : nullptr;
+        q->d_vec = (q->r.vector && q->vec_dev) ? const_cast<uint64_t*>(q->r.vector) : nullptr;
         cudaError_t e = cudaSuccess;
         if (!q->in_dev) {
             e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&q->d_in), bytes, pool, st);
             if (e == cudaSuccess) e = cudaMemcpyAsync(q->d_in, q->r.input, bytes, cudaMemcpyHostToDevice, st);
+            else q->d_in = nullptr;
         }
         if (e == cudaSuccess && !q->out_dev) {
-            if (q->in_dev || q->r.output != q->r.input)
+            if (q->in_dev || q->r.output != q->r.input) {
                 e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&q->d_out), bytes, pool, st);
-            else
+                if (e != cudaSuccess) q->d_out = nullptr;
+            } else {
                 q->d_out = q->d_in;  // in place on the staged copy
+            }
         }
+        if (e == cudaSuccess && (int)i == fail_at) e = cudaErrorMemoryAllocation;
         if (e == cudaSuccess && q->r.vector && !q->vec_dev) {
             e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&q->d_vec), bytes, pool, st);
             if (e == cudaSuccess) e = cudaMemcpyAsync(q->d_vec, q->r.vector, bytes, cudaMemcpyHostToDevice, st);
+            else q->d_vec = nullptr;
         }
-        if (e != cudaSuccess) return sfail(AXHEL_ERR_NOMEM, std::string("request staging: ") + cudaGetErrorString(e));
+        if (e != cudaSuccess) {
+            unstage(st, take, i + 1);
+            return sfail(AXHEL_ERR_NOMEM, std::string("request staging: ") + cudaGetErrorString(e));
+        }
         axhel_job_t& j = jobs[i];
         j.kind = q->r.kind;
         j.n_ntts = (uint32_t)q->ntts.size();
@@ -186,17 +211,23 @@ axhel_status_t axhel_server::launch(Slot& s, int slot_index, std::vector<Req*>& 
     std::vector<axhel_impl::ClassLaunch> classes;
     axhel_status_t rc = axhel_impl::batch_build(jobs.data(), jobs.size(), nullptr, img, &zo, &zb, &args, nullptr, &err,
                                                 per_phase ? &classes : nullptr);
-    if (rc) return sfail(rc, err);
+    if (rc) {
+        unstage(st, take, take.size());
+        return sfail(rc, err);
+    }
     // Descriptors come from the stream-ordered pool and go back to it after
     // the batch: no cudaMalloc / cudaFree (which wait for the whole device)
     // while other batches run.
     void* desc = nullptr;
-    if (cudaMallocFromPoolAsync(&desc, img.size(), pool, st) != cudaSuccess)
+    if (cudaMallocFromPoolAsync(&desc, img.size(), pool, st) != cudaSuccess) {
+        unstage(st, take, take.size());
         return sfail(AXHEL_ERR_NOMEM, "batch descriptor buffer");
+    }
     rc = axhel_impl::batch_build(jobs.data(), jobs.size(), static_cast<unsigned char*>(desc), img, &zo, &zb,
                                  &args, nullptr, &err, per_phase ? &classes : nullptr);
     if (rc) {
         cudaFreeAsync(desc, st);
+        unstage(st, take, take.size());
         return sfail(rc, err);
     }
     if (img.size() > s.host_cap) {
@@ -206,6 +237,7 @@ axhel_status_t axhel_server::launch(Slot& s, int slot_index, std::vector<Req*>& 
         const size_t cap = std::max<size_t>(img.size() * 2, s.host_cap * 2);
         if (cudaMallocHost(reinterpret_cast<void**>(&grown), cap) != cudaSuccess) {
             cudaFreeAsync(desc, st);
+            unstage(st, take, take.size());
             return sfail(AXHEL_ERR_NOMEM, "pinned descriptor staging");
         }
         if (s.host_img) s.retired.push_back(s.host_img);
@@ -222,16 +254,16 @@ axhel_status_t axhel_server::launch(Slot& s, int slot_index, std::vector<Req*>& 
     std::vector<Req*> order(take);
     std::stable_sort(order.begin(), order.end(), [](const Req* a, const Req* b) { return a->words < b->words; });
     for (Req* q : order) {
-        if (e != cudaSuccess) break;
-        if (!q->out_dev) e = cudaMemcpyAsync(q->r.output, q->d_out, q->words * 8, cudaMemcpyDeviceToHost, st);
-        cudaEvent_t ev = get_event();
-        if (!ev) e = cudaErrorMemoryAllocation;
-        if (e == cudaSuccess) e = cudaEventRecord(ev, st);
-        if (ev) f.done.push_back(ev);
-        if (!q->in_dev) cudaFreeAsync(q->d_in, st);
-        if (!q->out_dev && q->d_out != q->d_in) cudaFreeAsync(q->d_out, st);
-        if (q->r.vector && !q->vec_dev) cudaFreeAsync(q->d_vec, st);
+        if (e == cudaSuccess && !q->out_dev)
+            e = cudaMemcpyAsync(q->r.output, q->d_out, q->words * 8, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) {
+            cudaEvent_t ev = get_event();
+            if (!ev) e = cudaErrorMemoryAllocation;
+            if (e == cudaSuccess) e = cudaEventRecord(ev, st);
+            if (ev) f.done.push_back(ev);
+        }
     }
+    unstage(st, take, take.size());  // in stream order, after the copies back
     cudaFreeAsync(desc, st);  // after the error word's copy, in stream order
     if (e != cudaSuccess) return sfail(AXHEL_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
     f.reqs = order;
@@ -244,19 +276,57 @@ void axhel_server::scheduler()
     cudaSetDevice(device);
     tighten_timer_slack();
     std::unique_lock<std::mutex> lk(mu);
+    const bool by_arrival = cfg.flags & AXHEL_SERVER_ARRIVAL_PRIORITY;
+    const bool smallest_first = cfg.flags & AXHEL_SERVER_SMALLEST_FIRST;
     auto free_slot = [&](int lane) {
+        if (by_arrival) {
+            // A lane's slots are in decreasing stream priority: the new batch
+            // takes the first free slot below the youngest batch in flight,
+            // so every batch in flight outranks the ones launched after it
+            // (the highest free one when the lane is idle; the lowest free
+            // one when none is left below).
+            int youngest = -1, first = -1, last = -1;
+            for (size_t i = 0; i < slots.size(); ++i) {
+                if (slots[i].lane != lane) continue;
+                if (slots[i].busy) {
+                    youngest = (int)i;
+                } else {
+                    if (first < 0) first = (int)i;
+                    last = (int)i;
+                }
+            }
+            if (youngest < 0) return first;
+            for (size_t i = (size_t)youngest + 1; i < slots.size(); ++i)
+                if (slots[i].lane == lane && !slots[i].busy) return (int)i;
+            return last;
+        }
         for (size_t i = 0; i < slots.size(); ++i)
             if (slots[i].lane == lane && !slots[i].busy) return (int)i;
         return -1;
     };
     auto runnable = [&](int lane) { return !pending[lane].empty() && free_slot(lane) >= 0; };
+    // Admission order of a lane's queue: arrival order, or (smallest first)
+    // requests pending longer than the aging bound in arrival order, then
+    // the rest by size.
+    const auto aging = std::chrono::microseconds(cfg.aging_us);
+    auto order_queue = [&](std::deque<Req*>& queue) {
+        if (!smallest_first || queue.size() < 2) return;
+        const auto now = Clock::now();
+        std::stable_sort(queue.begin(), queue.end(), [&](const Req* a, const Req* b) {
+            const bool ao = now - a->t_submit >= aging, bo = now - b->t_submit >= aging;
+            if (ao != bo) return ao;
+            if (ao) return a->id < b->id;
+            return a->words < b->words;
+        });
+    };
     for (;;) {
         cv_sched.wait(lk, [&] { return stop || (!paused && (runnable(0) || runnable(1))); });
         if (stop) break;
         // the small-request lane first, then the other
         const int lane = runnable(0) ? 0 : 1;
         std::deque<Req*>& queue = pending[lane];
-        // admit in arrival order while the budget allows
+        order_queue(queue);
+        // admit in queue order while the budget allows
         std::vector<Req*> take;
         size_t bytes = 0;
         uint64_t words = 0;
@@ -400,7 +470,13 @@ axhel_status_t axhel_server_create(const axhel_server_config_t* cfg, axhel_serve
         // with two lanes, lane 0 (small requests) gets the highest priority:
         // its CTAs are dispatched ahead of the large lane's as SMs free up
         sl.lane = s->lanes == 2 ? (int)(i / cfg->max_inflight) : 1;
-        const int prio = sl.lane == 0 ? prio_high : prio_low;
+        int prio = sl.lane == 0 ? prio_high : prio_low;
+        if (cfg->flags & AXHEL_SERVER_ARRIVAL_PRIORITY) {
+            // the lane's k-th slot at the k-th highest priority (the rest at
+            // the lowest): the order in which the scheduler fills them
+            const int k = (int)(i % cfg->max_inflight);
+            prio = std::min(prio_high + k, prio_low);  // greater numbers are lower priorities
+        }
         if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&sl.stream, cudaStreamNonBlocking, prio);
         if (e == cudaSuccess) e = axhel_impl::lanes_create(&sl.lanes, prio);
         if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&sl.err_host), sizeof(int));
@@ -547,6 +623,9 @@ axhel_status_t axhel_server_stats(axhel_server_t s, axhel_server_stats_t* out, i
     out->p50_ms = pct(0.50);
     out->p99_ms = pct(0.99);
     out->samples = v.size();
+    uint64_t used = 0;  // a 64-bit attribute value
+    out->pool_used_bytes =
+        cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess ? (uint64_t)used : 0;
     if (reset_latencies) s->lat_ms.clear();
     return AXHEL_OK;
 }
@@ -579,6 +658,13 @@ axhel_status_t axhel_server_destroy(axhel_server_t s)
 }
 
 const char* axhel_server_last_error(void) { return t_serve_error.c_str(); }
+
+axhel_status_t axhel_server_debug_fail_staging(axhel_server_t s, uint32_t request)
+{
+    if (!s) return sfail(AXHEL_ERR_INVALID, "null server");
+    s->debug_fail_at.store((int)std::min<uint32_t>(request, 1u << 30));
+    return AXHEL_OK;
+}
 
 axhel_status_t axhel_server_drive(axhel_server_t server, const axhel_request_t* templates, uint32_t n_templates,
                                   uint64_t* const* outputs, uint32_t copies, const double* isolated_ms,

@@ -40,7 +40,8 @@ def _dev(arr):
 
 
 class ModulusPool:
-    """NTT handles per (N, bits), shared by all jobs (tables stay resident)."""
+    """NTT handles per (N, bits, position), shared by all jobs (tables stay
+    resident); `moduli` alone needs no GPU."""
 
     def __init__(self):
         self.cache = {}
@@ -48,24 +49,56 @@ class ModulusPool:
     def get(self, n, bits, pos):
         key = (n, bits, pos)
         if key not in self.cache:
-            q = params.ntt_prime_near(n, bits, pos, 4)
-            self.cache[key] = (q, capi.NTT(n, q, params.primitive_root(n, q)))
+            q, psi = modulus(n, bits, pos)
+            self.cache[key] = (q, capi.NTT(n, q, psi))
         return self.cache[key]
+
+
+_MODULI = {}
+
+
+def modulus(n, bits, pos):
+    """(q, psi): the NTT-friendly prime of width `bits` nearest position
+    pos/4 of its range, q = 1 mod 2n, and its primitive 2n-th root."""
+    key = (n, bits, pos)
+    if key not in _MODULI:
+        q = params.ntt_prime_near(n, bits, pos, 4)
+        _MODULI[key] = (q, params.primitive_root(n, q))
+    return _MODULI[key]
+
+
+def uniform_rows(rng, bounds, n):
+    """One row of n residues per bound, uniform integers in [0, bound)."""
+    b = np.asarray(bounds, dtype=np.uint64).reshape(-1, 1)
+    return rng.integers(0, b, size=(b.shape[0], n), dtype=np.uint64)
 
 
 # ------------------------------------------------------------------ tensor
 
-def tensor_chain(pairs=64, L=16, logn=15, reps=5, seed=3):
-    """C3: (c0*d0, c0*d1 + c1*d0, c1*d1) then ReduceMod(4,1): one fused launch
-    over all limbs vs the reference's per-limb call sequence."""
-    import torch
+TENSOR_SHAPE = dict(pairs=64, L=16, logn=15, seed=3)
 
+
+def tensor_inputs(pairs=64, L=16, logn=15, seed=3):
+    """C3 operands on the host: `pairs` ciphertext pairs x L limbs of
+    N = 2^logn residues, 16 primes of 40-55 bits; c0, c1, d0, d1 as
+    (pairs*L, N) arrays uniform in [0, q_i).  Returns (n, qs, count, arrays)."""
     n = 1 << logn
     qs = [params.ntt_prime_near(n, 40 + (i % 16), 1 + i // 16, 4) for i in range(L)]
     count = pairs * L
     rng = np.random.default_rng(seed)
-    bounds = np.array([qs[i % L] for i in range(count)], dtype=np.uint64)[:, None]
-    c0, c1, d0, d1 = (_dev((rng.random((count, n)) * bounds).astype(np.uint64)) for _ in range(4))
+    bounds = [qs[i % L] for i in range(count)]
+    return n, qs, count, tuple(uniform_rows(rng, bounds, n) for _ in range(4))
+
+
+def tensor_chain(pairs=64, L=16, logn=15, reps=5, seed=3, keep=False):
+    """C3: (c0*d0, c0*d1 + c1*d0, c1*d1) then ReduceMod(4,1): one fused launch
+    over all limbs vs the reference's per-limb call sequence.  keep=True
+    also returns the fused results (device tensors) under "results"."""
+    import torch
+
+    n, qs, count, host_in = tensor_inputs(pairs, L, logn, seed)
+    c0, c1, d0, d1 = (_dev(a) for a in host_in)
+    del host_in
     r0, r1, r2 = (torch.empty_like(c0) for _ in range(3))
     t1 = torch.empty_like(c0)
     P = lambda t, i=0: t.data_ptr() + 8 * n * i
@@ -102,17 +135,22 @@ def tensor_chain(pairs=64, L=16, logn=15, reps=5, seed=3):
     same = all(torch.equal(a, b) for a, b in zip(ref, (r0, r1, r2)))
     elems = count * n
     alg = 56 * elems  # 4 reads + 3 writes of 8 bytes per coefficient-limb
-    return {"workload": f"tensor product chain, N=2^{logn}, L={L}, {pairs} ciphertext pairs",
-            "elements": elems, "fused_ms": ms_fused, "per_limb_calls_ms": ms_sep,
-            "speedup": ms_sep / ms_fused, "fused_GBps": alg / (ms_fused / 1e3) / 1e9, "same_bits": same}
+    out = {"workload": f"tensor product chain, N=2^{logn}, L={L}, {pairs} ciphertext pairs",
+           "elements": elems, "fused_ms": ms_fused, "per_limb_calls_ms": ms_sep,
+           "speedup": ms_sep / ms_fused, "fused_GBps": alg / (ms_fused / 1e3) / 1e9, "same_bits": same}
+    if keep:
+        out["results"] = (r0, r1, r2)
+    return out
 
 
 # ------------------------------------------------------------------ uneven
 
-def uneven_jobs(pool, n_polys=512, seed=11, logn_lo=12, logn_hi=17, max_L=48):
-    """C4: polynomials with N ~ U{2^12..2^17}, L ~ U{1..48} limbs (primes of
-    30-60 bits), input factor ~ U{1,2,4}; a third forward, a third inverse,
-    a third INTT -> MulMod -> NTT with a plaintext vector."""
+def uneven_specs(n_polys=512, seed=11, logn_lo=12, logn_hi=17, max_L=48):
+    """C4 job list (host only): polynomials with N ~ U{2^12..2^17}, L ~
+    U{1..48} limbs (primes of 30-60 bits), input factor ~ U{1,2,4}; a third
+    forward, a third inverse, a third INTT -> MulMod -> NTT with a plaintext
+    vector.  Each job: kind, n, L, mods [(q, psi)] per limb, in_f, out_f and
+    the seed of its operands (`uneven_arrays`)."""
     rng = np.random.default_rng(seed)
     jobs = []
     for j in range(n_polys):
@@ -120,27 +158,47 @@ def uneven_jobs(pool, n_polys=512, seed=11, logn_lo=12, logn_hi=17, max_L=48):
         n = 1 << logn
         L = int(rng.integers(1, max_L + 1))
         kind = (1, 2, 3)[j % 3]
-        mods = [pool.get(n, int(rng.integers(30, 61)), int(rng.integers(1, 4))) for _ in range(L)]
+        keys = [(n, int(rng.integers(30, 61)), int(rng.integers(1, 4))) for _ in range(L)]
         in_f = int(rng.choice([1, 2, 4]))
         out_f = int(rng.choice([1, 2])) if kind == 2 else int(rng.choice([1, 4]))
-        jobs.append(dict(kind=kind, n=n, L=L, mods=mods, in_f=in_f, out_f=out_f, seed=int(rng.integers(1 << 30))))
+        jobs.append(dict(kind=kind, n=n, L=L, keys=keys, mods=[modulus(*k) for k in keys], in_f=in_f, out_f=out_f,
+                         seed=int(rng.integers(1 << 30))))
+    return jobs
+
+
+def uneven_arrays(job):
+    """A C4 job's operands on the host: x (L, N) uniform in [0, in_f*q_i),
+    and for chains the vector (L, N) uniform in [0, 2 q_i)."""
+    rng = np.random.default_rng(job["seed"])
+    qs = [q for q, _ in job["mods"]]
+    x = uniform_rows(rng, [job["in_f"] * q for q in qs], job["n"])
+    v = uniform_rows(rng, [2 * q for q in qs], job["n"]) if job["kind"] == 3 else None
+    return x, v
+
+
+def uneven_jobs(pool, n_polys=512, seed=11, logn_lo=12, logn_hi=17, max_L=48):
+    """C4 jobs with device handles (`ModulusPool`) for their moduli."""
+    jobs = uneven_specs(n_polys, seed, logn_lo, logn_hi, max_L)
+    for job in jobs:
+        job["mods"] = [pool.get(*k) for k in job["keys"]]
     return jobs
 
 
 def _job_arrays(job):
     import torch
 
-    n, L = job["n"], job["L"]
-    rng = np.random.default_rng(job["seed"])
-    qs = np.array([q for q, _ in job["mods"]], dtype=np.uint64)[:, None]
-    x = (rng.random((L, n)) * (qs * np.uint64(job["in_f"]))).astype(np.uint64)
+    x, v = uneven_arrays(job)
     job["x"] = _dev(x)
     job["y"] = torch.empty_like(job["x"])
-    if job["kind"] == 3:
-        job["v"] = _dev((rng.random((L, n)) * (2 * qs)).astype(np.uint64))
+    if v is not None:
+        job["v"] = _dev(v)
 
 
-def uneven_batch(n_polys=512, seed=11, reps=3):
+def uneven_batch(n_polys=512, seed=11, reps=3, keep=False):
+    """C4 timed three ways (per-limb calls, one persistent launch, per-phase
+    launches), each checked against the per-limb results; keep=True also
+    returns the jobs with their device results ("y", from the per-phase
+    launches) under "jobs"."""
     import torch
 
     pool = ModulusPool()
@@ -202,13 +260,17 @@ def uneven_batch(n_polys=512, seed=11, reps=3):
     ms_phased = timed(phased, reps)
     same = same and b.status() == 0 and all(torch.equal(r, j["y"]) for r, j in zip(ref, jobs))
     b.close()
+    del ref
     limbs = sum(j["L"] for j in jobs)
-    return {"workload": f"{n_polys} uneven polynomials, N in 2^12..2^17, L in 1..48, fwd/inv/chain mix",
-            "limbs": limbs, "limb_transforms": transforms, "one_launch_ms": ms_batch,
-            "one_launch_rate": transforms / (ms_batch / 1e3), "phased_ms": ms_phased,
-            "phased_rate": transforms / (ms_phased / 1e3), "per_limb_calls_ms": ms_plain,
-            "per_limb_rate": transforms / (ms_plain / 1e3), "speedup": ms_plain / ms_batch, "same_bits": same,
-            "unit": UNIT}
+    out = {"workload": f"{n_polys} uneven polynomials, N in 2^12..2^17, L in 1..48, fwd/inv/chain mix",
+           "limbs": limbs, "limb_transforms": transforms, "one_launch_ms": ms_batch,
+           "one_launch_rate": transforms / (ms_batch / 1e3), "phased_ms": ms_phased,
+           "phased_rate": transforms / (ms_phased / 1e3), "per_limb_calls_ms": ms_plain,
+           "per_limb_rate": transforms / (ms_plain / 1e3), "speedup": ms_plain / ms_batch, "same_bits": same,
+           "unit": UNIT}
+    if keep:
+        out["jobs"] = jobs
+    return out
 
 
 # ------------------------------------------------------------------ serving
@@ -231,15 +293,15 @@ class RequestPool:
             n = 1 << logn
             L = int(rng.integers(L_lo, L_hi + 1))
             mods = [self.pool.get(n, 40 + (i % 20), 1 + (i // 20) % 3) for i in range(L)]
-            qs = np.array([q for q, _ in mods], dtype=np.uint64)[:, None]
+            qs = [2 * q for q, _ in mods]
             kind = 3 if k % 2 == 0 else 4
 
             def place(a):
                 t = torch.from_numpy(a.reshape(-1).view(np.int64))
                 return t.cuda() if device else t.pin_memory()
 
-            x = place((rng.random((L, n)) * (2 * qs)).astype(np.uint64))
-            v = place((rng.random((L, n)) * (2 * qs)).astype(np.uint64))
+            x = place(uniform_rows(rng, qs, n))
+            v = place(uniform_rows(rng, qs, n))
             outs = [torch.empty(L * n, dtype=torch.int64, device="cuda" if device else "cpu") for _ in range(copies)]
             if not device:
                 outs = [o.pin_memory() for o in outs]
@@ -273,7 +335,7 @@ def _pct(v, p):
 
 def serving(loads=(0.5, 0.7, 0.9), seconds=4.0, budget=60 << 30, inflight=4, seed=5, n_templates=32,
             device=False, max_batch_words=0, persistent=False, plain=True, small_words=0, reserve=8 << 30,
-            max_batch_requests=256):
+            max_batch_requests=256, flags=0, aging_us=0):
     """Isolated latency of every template (alone on an idle server), capacity
     (a burst), then Poisson arrivals at each load fraction of capacity
     (host-staged requests: `reserve` bytes of the staging pool mapped up
@@ -282,7 +344,7 @@ def serving(loads=(0.5, 0.7, 0.9), seconds=4.0, budget=60 << 30, inflight=4, see
     rp = RequestPool(n_templates=n_templates, seed=seed, device=device)
     srv = capi.Server(budget_bytes=budget, max_inflight=inflight, max_batch_requests=max_batch_requests,
                       max_batch_words=max_batch_words, persistent=persistent, small_request_words=small_words,
-                      reserve_bytes=0 if device else reserve)
+                      reserve_bytes=0 if device else reserve, flags=flags, aging_us=aging_us)
     rng = np.random.default_rng(seed)
 
     iso = []
@@ -333,13 +395,23 @@ def serving(loads=(0.5, 0.7, 0.9), seconds=4.0, budget=60 << 30, inflight=4, see
     out = {"workload": "INTT->MulMod/FMAMod->NTT requests, N in 2^13..2^17, L in 2..40, Poisson arrivals",
            "operands": "device-resident" if device else "host pinned, staged per request",
            "launch": "persistent" if persistent else "per-phase class launches", "max_batch_words": max_batch_words,
-           "small_request_words": small_words,
+           "small_request_words": small_words, "policy": policy_name(flags, aging_us),
            "capacity_jobs_per_s": cap, "isolated_median_ms": statistics.median(iso), "loads": results,
            "batches": st["batches"], "max_batch_requests": st["max_batch_requests"],
            "peak_in_use_bytes": st["peak_in_use_bytes"], "budget_bytes": budget, "max_inflight": inflight}
     if plain:
         out["plain_sequential_jobs_per_s"] = plain_sequential(rp)
     return out
+
+
+def policy_name(flags, aging_us=0):
+    """Readable name of the server's scheduling flags."""
+    parts = []
+    if flags & capi.SERVER_ARRIVAL_PRIORITY:
+        parts.append("arrival-priority streams")
+    if flags & capi.SERVER_SMALLEST_FIRST:
+        parts.append(f"smallest-first admission (aging {aging_us} us)")
+    return ", ".join(parts) or "arrival-order admission, equal-priority streams"
 
 
 def plain_sequential(rp, limit=16):
@@ -471,6 +543,12 @@ def main():
     ap.add_argument("--inflight", type=int, default=4)
     ap.add_argument("--small-words", type=int, default=0, help="high-priority lane for requests up to this size")
     ap.add_argument("--max-batch-requests", type=int, default=256)
+    ap.add_argument("--arrival-priority", action="store_true", help="batches in flight prioritised by launch order")
+    ap.add_argument("--smallest-first", action="store_true", help="admit the smallest pending requests first")
+    ap.add_argument("--aging-us", type=int, default=0, help="smallest-first: pending time after which arrival wins")
+    ap.add_argument("--loads", default="0.5,0.7,0.9")
+    ap.add_argument("--templates", type=int, default=24, help="request templates (the bench uses 24)")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain sequential comparison")
     a = ap.parse_args()
     if a.what == "tensor":
         out = tensor_chain()
@@ -481,9 +559,12 @@ def main():
     elif a.what == "uneven":
         out = uneven_batch()
     else:
-        out = serving(seconds=a.seconds, device=a.device, persistent=a.persistent,
-                      max_batch_words=a.max_batch_words, inflight=a.inflight, small_words=a.small_words,
-                      max_batch_requests=a.max_batch_requests)
+        flags = (capi.SERVER_ARRIVAL_PRIORITY if a.arrival_priority else 0) | \
+            (capi.SERVER_SMALLEST_FIRST if a.smallest_first else 0)
+        out = serving(loads=tuple(float(x) for x in a.loads.split(",")), seconds=a.seconds, device=a.device,
+                      persistent=a.persistent, max_batch_words=a.max_batch_words, inflight=a.inflight,
+                      small_words=a.small_words, max_batch_requests=a.max_batch_requests, flags=flags,
+                      aging_us=a.aging_us, n_templates=a.templates, plain=not a.no_plain)
     print(json.dumps(out), flush=True)
 
 

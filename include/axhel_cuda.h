@@ -221,8 +221,10 @@ axhel_status_t axhel_cuda_batch_set_wait_ns(axhel_batch_t batch, uint64_t ns);
  * synchronize the device).  The batch's descriptors and counters live in a
  * static 1 MiB device array per device; a batch that needs more returns
  * AXHEL_ERR_UNSUPPORTED.  The first call on a device resolves that array's
- * address (make it before any stream capture).  All calls share the array:
- * calls that overlap on the GPU race and must not be issued.  Synchronous;
+ * address (make it before any stream capture); the address is kept for the
+ * process, so the entry point must not be used across a cudaDeviceReset.
+ * All calls share the array: calls that overlap on the GPU race and must not
+ * be issued.  Each call waits for its batch to finish before it returns;
  * results equal axhel_cuda_batch_run's bit for bit. */
 axhel_status_t axhel_cuda_batch_run_static(const axhel_job_t* jobs, uint64_t n_jobs, void* stream);
 /* Failure-detection hook: makes every dependency of job `job` unreachable
@@ -237,6 +239,14 @@ axhel_status_t axhel_cuda_batch_debug_unreachable(axhel_batch_t batch, uint64_t 
 typedef struct axhel_server* axhel_server_t;
 
 #define AXHEL_SERVER_PERSISTENT 1u /* run each batch as one persistent launch (default: one launch per phase) */
+/* Batches in flight get stream priorities in launch order (the oldest the
+ * highest), so the GPU dispatches their tiles first come first served
+ * instead of sharing the SMs between them. */
+#define AXHEL_SERVER_ARRIVAL_PRIORITY 2u
+/* Admission takes the smallest pending requests first (fewest residues);
+ * a request pending longer than aging_us goes ahead of them in arrival
+ * order, so large requests are not starved. */
+#define AXHEL_SERVER_SMALLEST_FIRST 4u
 
 typedef struct axhel_server_config {
     uint64_t hbm_budget_bytes;    /* device bytes the server may hold for staged operands */
@@ -245,7 +255,7 @@ typedef struct axhel_server_config {
     uint32_t max_inflight;        /* batches concurrently on the GPU per lane (1..16 streams) */
     uint32_t max_batch_requests;  /* requests admitted into one batch */
     uint32_t flags;               /* AXHEL_SERVER_* */
-    uint32_t reserved;
+    uint32_t aging_us;            /* AXHEL_SERVER_SMALLEST_FIRST: pending time after which arrival order wins */
     uint64_t reserve_bytes;       /* device memory mapped for staging at creation (capped at the budget; 0 = on
                                      demand): growing the pool later stalls the request that needs it */
 } axhel_server_config_t;
@@ -277,7 +287,8 @@ typedef struct axhel_request_info {
 
 typedef struct axhel_server_stats {
     uint64_t completed, batches, max_batch_requests, pending, in_use_bytes, peak_in_use_bytes, samples;
-    double p50_ms, p99_ms; /* submit -> done latency over completed requests */
+    double p50_ms, p99_ms;    /* submit -> done latency over completed requests */
+    uint64_t pool_used_bytes; /* device bytes allocated from the staging pool now (frees land in stream order) */
 } axhel_server_stats_t;
 
 /* Starts the scheduler and completion threads on the current device. */
@@ -312,6 +323,12 @@ axhel_status_t axhel_server_drive(axhel_server_t server, const axhel_request_t* 
                                   uint64_t* const* outputs, uint32_t copies, const double* isolated_ms,
                                   double rate_per_s, double seconds, uint64_t seed, axhel_drive_result_t* out);
 const char* axhel_server_last_error(void);
+/* Failure-injection hook (new; for tests): staging of the next batch fails
+ * at its request `request` (0-based, in admission order) as a device
+ * allocation failure would, after the requests before it were staged.  The
+ * batch's requests end with AXHEL_ERR_NOMEM and every buffer already staged
+ * for them goes back to the pool. */
+axhel_status_t axhel_server_debug_fail_staging(axhel_server_t server, uint32_t request);
 
 /* ---------------------------------------------------------------------- */
 /* Element-wise (device pointers); result may alias any operand.           */

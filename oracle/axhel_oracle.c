@@ -342,6 +342,131 @@ void orc_reduce(uint64_t* r, const uint64_t* a, uint64_t n, uint64_t q, uint64_t
 }
 
 /* ---------------------------------------------------------------------- */
+/* multi-limb call sequences (checkers for full-size batches)             */
+/* ---------------------------------------------------------------------- */
+
+/* One limb of a batch job: the reference's per-limb call sequence.
+ *   kind 1: ComputeForward(in_f, out_f)                       ntt.cpp:173-186
+ *   kind 2: [ReduceMod(4,2) if in_f == 4] ComputeInverse(2, out_f)  ntt.cpp:192-204
+ *   kind 3: [ReduceMod(4,2)] ComputeInverse(2,2) -> MulMod(., vec, 2) -> ComputeForward(1, out_f)
+ *   kind 4: [ReduceMod(4,2)] ComputeInverse(2,2) -> FMAMod(., s, vec|NULL, 2) -> ComputeForward(1, out_f)
+ * The ReduceMod(4,2) ahead of the inverse is eltwise-reduce-mod.cpp:110-118. */
+static void job_limb(uint32_t kind, uint64_t* res, const uint64_t* op, const uint64_t* vec, uint64_t s,
+                     uint64_t n, uint64_t q, const uint64_t* fwd, const uint64_t* inv, const uint64_t* ninv,
+                     uint64_t in_f, uint64_t out_f)
+{
+    if (kind == 1) {
+        orc_ntt_compute_forward(res, op, n, q, fwd, in_f, out_f);
+        return;
+    }
+    const uint64_t* src = op;
+    if (in_f == 4) {
+        orc_reduce(res, op, n, q, 4, 2);
+        src = res;
+    }
+    if (kind == 2) {
+        orc_ntt_compute_inverse(res, src, n, q, inv, ninv, 2, out_f);
+        return;
+    }
+    orc_ntt_compute_inverse(res, src, n, q, inv, ninv, 2, 2);
+    if (kind == 3)
+        orc_mul(res, res, vec, n, q, 2);
+    else
+        orc_fma(res, res, s, vec, n, q, 2);
+    orc_ntt_compute_forward(res, res, n, q, fwd, 1, out_f);
+}
+
+typedef struct {
+    uint32_t kind;
+    uint64_t* res;
+    const uint64_t *op, *vec, *scalars, *qs;
+    const uint64_t* const* fwds;
+    const uint64_t* const* invs;
+    const uint64_t* const* ninvs;
+    uint64_t n, nq, in_f, out_f, begin, end;
+} job_arg;
+
+static void* job_worker(void* p)
+{
+    job_arg* a = (job_arg*)p;
+    for (uint64_t i = a->begin; i < a->end; ++i) {
+        const uint64_t k = i % a->nq;
+        job_limb(a->kind, a->res + i * a->n, a->op + i * a->n, a->vec ? a->vec + i * a->n : NULL,
+                 a->scalars ? a->scalars[k] : 0, a->n, a->qs[k], a->fwds ? a->fwds[k] : NULL,
+                 a->invs ? a->invs[k] : NULL, a->ninvs ? a->ninvs[k] : NULL, a->in_f, a->out_f);
+    }
+    return NULL;
+}
+
+static int clamp_threads(int threads, uint64_t count)
+{
+    if (threads <= 0) threads = (int)sysconf(_SC_NPROCESSORS_ONLN);
+    if (threads < 1) threads = 1;
+    if (threads > 256) threads = 256;
+    if ((uint64_t)threads > count) threads = (int)(count ? count : 1);
+    return threads;
+}
+
+void orc_job_batch(uint32_t kind, uint64_t* res, const uint64_t* op, const uint64_t* vec,
+                   const uint64_t* scalars, uint64_t n, uint64_t count, const uint64_t* qs,
+                   const uint64_t* const* fwds, const uint64_t* const* invs, const uint64_t* const* ninvs,
+                   uint64_t nq, uint64_t in_f, uint64_t out_f, int threads)
+{
+    threads = clamp_threads(threads, count);
+    pthread_t tid[256];
+    job_arg args[256];
+    for (int t = 0; t < threads; ++t) {
+        job_arg a = {kind, res, op, vec, scalars, qs, fwds, invs, ninvs, n, nq, in_f, out_f,
+                     count * t / threads, count * (t + 1) / threads};
+        args[t] = a;
+        pthread_create(&tid[t], NULL, job_worker, &args[t]);
+    }
+    for (int t = 0; t < threads; ++t) pthread_join(tid[t], NULL);
+}
+
+typedef struct {
+    uint64_t *r0, *r1, *r2;
+    const uint64_t *c0, *c1, *d0, *d1, *qs;
+    uint64_t n, nq, factor, begin, end;
+} tensor_arg;
+
+static void* tensor_worker(void* p)
+{
+    tensor_arg* a = (tensor_arg*)p;
+    const uint64_t n = a->n;
+    uint64_t* u = (uint64_t*)malloc(n * sizeof(uint64_t));
+    for (uint64_t i = a->begin; i < a->end && u; ++i) {
+        const uint64_t q = a->qs[i % a->nq], o = i * n;
+        orc_mul(a->r0 + o, a->c0 + o, a->d0 + o, n, q, a->factor);
+        orc_mul(a->r1 + o, a->c0 + o, a->d1 + o, n, q, a->factor);
+        orc_mul(u, a->c1 + o, a->d0 + o, n, q, a->factor);
+        orc_add_vv(a->r1 + o, a->r1 + o, u, n, q);
+        orc_mul(a->r2 + o, a->c1 + o, a->d1 + o, n, q, a->factor);
+        orc_reduce(a->r0 + o, a->r0 + o, n, q, 4, 1);
+        orc_reduce(a->r1 + o, a->r1 + o, n, q, 4, 1);
+        orc_reduce(a->r2 + o, a->r2 + o, n, q, 4, 1);
+    }
+    free(u);
+    return NULL;
+}
+
+void orc_tensor_batch(uint64_t* r0, uint64_t* r1, uint64_t* r2, const uint64_t* c0, const uint64_t* c1,
+                      const uint64_t* d0, const uint64_t* d1, uint64_t n, uint64_t count, const uint64_t* qs,
+                      uint64_t nq, uint64_t factor, int threads)
+{
+    threads = clamp_threads(threads, count);
+    pthread_t tid[256];
+    tensor_arg args[256];
+    for (int t = 0; t < threads; ++t) {
+        tensor_arg a = {r0, r1, r2, c0, c1, d0, d1, qs, n, nq, factor, count * t / threads,
+                        count * (t + 1) / threads};
+        args[t] = a;
+        pthread_create(&tid[t], NULL, tensor_worker, &args[t]);
+    }
+    for (int t = 0; t < threads; ++t) pthread_join(tid[t], NULL);
+}
+
+/* ---------------------------------------------------------------------- */
 /* reference test-suite generators: tests/common/{reference,parameters}.hpp */
 /* ---------------------------------------------------------------------- */
 

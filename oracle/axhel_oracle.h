@@ -63,6 +63,24 @@ void orc_fma(uint64_t* r, const uint64_t* a, uint64_t s, const uint64_t* c, uint
 void orc_reduce(uint64_t* r, const uint64_t* a, uint64_t n, uint64_t q, uint64_t in_f,
                 uint64_t out_f);
 
+/* ---- multi-limb call sequences (full-size batch checkers) ---- */
+/* One job of `count` limbs stored back to back, limb i with modulus
+ * qs[i % nq] and its tables; kind as AXHEL_JOB_FORWARD/INVERSE/CHAIN_MUL/
+ * CHAIN_FMA (1..4): the reference's per-limb call sequence for that kind
+ * (forward; [ReduceMod 4->2] inverse; [ReduceMod 4->2] inverse(2,2) ->
+ * MulMod/FMAMod(., 2) -> forward(1, out_f)).  vec / scalars may be NULL
+ * where the kind does not use them.  Limbs run on up to `threads` threads. */
+void orc_job_batch(uint32_t kind, uint64_t* res, const uint64_t* op, const uint64_t* vec,
+                   const uint64_t* scalars, uint64_t n, uint64_t count, const uint64_t* qs,
+                   const uint64_t* const* fwds, const uint64_t* const* invs, const uint64_t* const* ninvs,
+                   uint64_t nq, uint64_t in_f, uint64_t out_f, int threads);
+/* The tensor-product call sequence per limb: t0 = MulMod(c0,d0), t1 = MulMod(c0,d1),
+ * u = MulMod(c1,d0), t1 = AddMod(t1,u), t2 = MulMod(c1,d1) (factor `factor`),
+ * then ReduceMod(., 4, 1) on each result. */
+void orc_tensor_batch(uint64_t* r0, uint64_t* r1, uint64_t* r2, const uint64_t* c0, const uint64_t* c1,
+                      const uint64_t* d0, const uint64_t* d1, uint64_t n, uint64_t count, const uint64_t* qs,
+                      uint64_t nq, uint64_t factor, int threads);
+
 /* ---- reference test-suite generators (tests/common/parameters.hpp) ---- */
 uint64_t orc_pow_mod(uint64_t a, uint64_t e, uint64_t q);
 int orc_is_prime(uint64_t n);

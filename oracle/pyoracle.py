@@ -111,6 +111,11 @@ class Oracle(_Common):
         self._tables = self._fn("ntt_tables", C.c_int, u64, u64, u64, p64, p64, p64)
         self._fwd = self._fn("ntt_compute_forward", None, p64, p64, u64, u64, p64, u64, u64)
         self._inv = self._fn("ntt_compute_inverse", None, p64, p64, u64, u64, p64, p64, u64, u64)
+        PP = C.POINTER(p64)
+        self._job = self._fn("job_batch", None, C.c_uint32, p64, p64, p64, p64, u64, u64, p64, PP, PP, PP, u64,
+                             u64, u64, C.c_int)
+        self._tensor = self._fn("tensor_batch", None, p64, p64, p64, p64, p64, p64, p64, u64, u64, p64, u64, u64,
+                                C.c_int)
         self.is_prime = self._fn("is_prime", C.c_int, u64)
         self.find_ntt_prime = self._fn("find_ntt_prime", u64, u64, C.c_uint)
         self.find_ntt_prime_near = self._fn("find_ntt_prime_near", u64, u64, C.c_uint, u64, u64)
@@ -134,6 +139,32 @@ class Oracle(_Common):
         out = np.zeros_like(x) if out is None else out
         self._fwd(_ptr(out), _ptr(x), x.size, q, _ptr(fwd), in_f, out_f)
         return out
+
+    def job_batch(self, kind, x, n, count, qs, tables, in_f, out_f, vec=None, scalars=None, threads=0, out=None):
+        """The reference's per-limb call sequence of a batch job (kind 1..4 as
+        the C-ABI's AXHEL_JOB_*) over `count` limbs of degree n stored back to
+        back; limb i uses qs[i % len(qs)] and tables[i % len(qs)] = (fwd, inv,
+        ninv).  Multi-threaded over limbs (threads 0 = every core)."""
+        nq = len(qs)
+        assert len(tables) == nq and x.size == n * count
+        out = np.zeros_like(x) if out is None else out
+        PP = p64 * nq
+        fw = PP(*[_ptr(t[0]) for t in tables])
+        iv = PP(*[_ptr(t[1]) for t in tables])
+        ni = PP(*[_ptr(t[2]) for t in tables])
+        qa = np.ascontiguousarray(qs, dtype=np.uint64)
+        sc = None if scalars is None else np.ascontiguousarray(scalars, dtype=np.uint64)
+        self._job(kind, _ptr(out), _ptr(x), _ptr(vec), _ptr(sc), n, count, _ptr(qa), fw, iv, ni, nq, in_f, out_f,
+                  threads)
+        return out
+
+    def tensor_batch(self, c0, c1, d0, d1, n, count, qs, factor, threads=0):
+        """The tensor-product per-limb call sequence (three results)."""
+        outs = [np.zeros_like(c0) for _ in range(3)]
+        qa = np.ascontiguousarray(qs, dtype=np.uint64)
+        self._tensor(*[_ptr(o) for o in outs], _ptr(c0), _ptr(c1), _ptr(d0), _ptr(d1), n, count, _ptr(qa), len(qs),
+                     factor, threads)
+        return outs
 
     def inverse(self, x, q, inv, ninv, in_f=1, out_f=1, out=None):
         out = np.zeros_like(x) if out is None else out

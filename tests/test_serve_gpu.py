@@ -71,8 +71,9 @@ SPECS = [(13, 4, 4, 3), (14, 2, 2, 4), (15, 6, 6, 3), (16, 3, 3, 4), (17, 2, 2, 
          (12, 3, 3, 4)]
 
 
-@pytest.mark.parametrize("cfg", [{}, {"persistent": True}, {"small_request_words": 1 << 16}],
-                         ids=["per-phase", "persistent", "two-lanes"])
+@pytest.mark.parametrize("cfg", [{}, {"persistent": True}, {"small_request_words": 1 << 16}, {"flags": 2},
+                                 {"flags": 4, "aging_us": 500}],
+                         ids=["per-phase", "persistent", "two-lanes", "arrival-priority", "smallest-first"])
 def test_same_bits_alone_and_in_a_mix(cuda, oracle, cfg):
     reqs = make_requests(cuda, oracle, 5, SPECS)
     srv = cuda.Server(budget_bytes=8 << 30, max_inflight=2, max_batch_requests=64, **cfg)
@@ -231,4 +232,57 @@ def test_pageable_host_buffers(cuda, oracle):
         st, _ = srv.wait(rid)
         assert st == 0
         np.testing.assert_array_equal(o, expected(oracle, r))
+    srv.close()
+
+
+def test_staging_failure_frees_what_it_staged(cuda, oracle):
+    """A device allocation failure part-way through staging a batch (injected
+    on the host at its third request): every request of that batch ends with
+    AXHEL_ERR_NOMEM, the buffers staged for the first ones go back to the
+    pool, the budget returns to zero, and the server keeps serving."""
+    reqs = make_requests(cuda, oracle, 31, [(13, 2, 2, 3), (14, 2, 2, 4), (13, 3, 3, 3), (14, 2, 2, 3)])
+    srv = cuda.Server(budget_bytes=1 << 30, max_inflight=1, max_batch_requests=16)
+    srv.pause(True)
+    hs = [submit(srv, r, on_device=False) for r in reqs]
+    srv.debug_fail_staging(2)
+    srv.pause(False)
+    for rid, _ in hs:
+        st, _ = srv.wait(rid)
+        assert st == 3  # AXHEL_ERR_NOMEM
+    s = srv.stats()
+    assert s["in_use_bytes"] == 0
+    assert s["pool_used_bytes"] == 0
+    hs = [submit(srv, r, on_device=False) for r in reqs]
+    for (rid, bufs), r in zip(hs, reqs):
+        st, _ = srv.wait(rid)
+        assert st == 0
+        np.testing.assert_array_equal(result(bufs, r["x"].size, False), expected(oracle, r))
+    assert srv.stats()["pool_used_bytes"] == 0
+    srv.close()
+
+
+@pytest.mark.parametrize("aging_us", [0, 10_000_000])
+def test_smallest_first_admission_and_aging(cuda, oracle, aging_us):
+    """Smallest-first admission, one request per batch on one stream: held
+    requests run smallest first; with an aging bound of 0 every request has
+    aged, so they run in arrival order.  Results are the same either way."""
+    specs = [(15, 4, 4, 3), (13, 2, 2, 4), (16, 3, 3, 3), (13, 1, 1, 3), (14, 2, 2, 4)]
+    reqs = make_requests(cuda, oracle, 41, specs)
+    srv = cuda.Server(budget_bytes=4 << 30, max_inflight=1, max_batch_requests=1, flags=cuda.SERVER_SMALLEST_FIRST,
+                      aging_us=aging_us)
+    srv.pause(True)
+    hs = [submit(srv, r, on_device=True) for r in reqs]
+    srv.pause(False)
+    batch = []
+    for (rid, bufs), r in zip(hs, reqs):
+        st, info = srv.wait(rid)
+        assert st == 0 and info.batch_size == 1
+        batch.append(info.batch_id)
+        np.testing.assert_array_equal(result(bufs, r["x"].size, True), expected(oracle, r))
+    words = [r["n"] * r["count"] for r in reqs]
+    order = sorted(range(len(reqs)), key=lambda k: batch[k])
+    if aging_us:
+        assert [words[k] for k in order] == sorted(words)
+    else:
+        assert order == list(range(len(reqs)))
     srv.close()

@@ -60,14 +60,19 @@ def test_static_scratch_batch_matches_allocating_batch_twice(cuda, oracle):
 
 
 def test_static_scratch_refuses_batches_beyond_its_size(cuda, oracle):
-    n = 1024
+    n, jobs = 1024, 4096
     q = oracle.find_ntt_prime(n, 40)
     t = cuda.NTT(n, q, oracle.find_primitive_root(n, q))
-    d = dev_empty(8)
-    # 400k limbs need 1.6 MB of completion counters: more than the 1 MiB array.
-    # Refused on the host, before any copy or launch.
-    spec = [dict(kind=1, ntts=[t], count=400_000, result=ptr(d), operand=ptr(d), in_f=1, out_f=4)]
+    # 4096 one-limb jobs need about 1.3 MB of descriptors: more than the
+    # 1 MiB array.  Every job has its own limb of a real buffer (32 MiB), so
+    # nothing could run past an allocation even if the batch got through;
+    # it is refused on the host, before any copy or launch.
+    d = dev_empty(jobs * n)
+    spec = [dict(kind=1, ntts=[t], count=1, result=ptr(d, j * n), operand=ptr(d, j * n), in_f=1, out_f=4)
+            for j in range(jobs)]
     with pytest.raises(cuda.AxhelError) as e:
         cuda.batch_run_static(spec)
     assert e.value.status == 4  # AXHEL_ERR_UNSUPPORTED
     assert "static scratch holds 1048576 bytes" in str(e.value)
+    # the same batch through the allocating entry point runs
+    cuda.batch_run(spec)
