@@ -74,8 +74,34 @@ def _compile(src, verbose_ptxas=False):
     return obj, r.stderr
 
 
+TOOLS = os.path.join(PKG, "tools")
+
+
+def build_tools(force=False):
+    """The measuring programs of ``axhel_b200/tools`` (C++ callers of the
+    public API), linked against libaxhel.so next to them."""
+    for f in sorted(os.listdir(TOOLS)):
+        if not f.endswith(".cpp"):
+            continue
+        src = os.path.join(TOOLS, f)
+        exe = os.path.join(PKG, f[:-4])
+        if not force and os.path.exists(exe) and os.path.getmtime(exe) >= _newest([src, LIB] + headers()):
+            continue
+        cmd = ["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), src, "-L" + PKG, "-laxhel",
+               "-Wl,-rpath,$ORIGIN", "-lpthread", "-o", exe]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"tool build failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+
+
 def build(force=False, verbose_ptxas=False, quiet=False):
-    """Compile and link libaxhel.so; returns its path."""
+    """Compile and link libaxhel.so (and the tools); returns its path."""
+    lib = _build_lib(force, verbose_ptxas, quiet)
+    build_tools(force)
+    return lib
+
+
+def _build_lib(force=False, verbose_ptxas=False, quiet=False):
     os.makedirs(OBJ, exist_ok=True)
     srcs = sources()
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= _newest(srcs + headers() + [__file__]):
@@ -104,8 +130,13 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--ptxas-v", action="store_true", help="print registers / spills per kernel")
+    ap.add_argument("--debug-log", action="store_true",
+                    help="define AXHEL_DEBUG: every drop-in call logs its dispatch to stderr (AXHEL_LOG)")
     a = ap.parse_args()
-    print(build(force=a.force or a.ptxas_v, verbose_ptxas=a.ptxas_v))
+    if a.debug_log:
+        NVCC_FLAGS.append("-DAXHEL_DEBUG")
+        CXX_FLAGS.append("-DAXHEL_DEBUG")
+    print(build(force=a.force or a.ptxas_v or a.debug_log, verbose_ptxas=a.ptxas_v))
 
 
 if __name__ == "__main__":

@@ -5,13 +5,15 @@
 // synchronous (results are visible on return), result may alias the
 // operands, n == 0 is a no-op, and unsupported mod-factors leave the result
 // untouched.  Pointers may be host memory (the reference's and SEAL's usage:
-// operands are staged through per-thread device buffers) or device memory
-// (used in place, no copies).  Each host thread issues its work on its own
+// operands are copied into per-thread pinned buffers, then by DMA into
+// per-thread device buffers, and results back the same way) or device
+// memory (used in place, no copies).  Each host thread issues its work on its own
 // per-thread default stream, so const NTT objects shared between threads (as
 // SEAL's process-wide cache does) are safe to use concurrently.
 // CUDA failures throw std::runtime_error: there is no CPU fallback.
 #include <cuda_runtime.h>
 
+#include <cstdlib>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -19,6 +21,7 @@
 
 #include "../../include/axhel/axhel.hpp"
 #include "../../include/axhel/ntt/ntt-rns.hpp"
+#include "../../include/axhel/util/debug.hpp"
 #include "../../include/axhel_cuda.h"
 
 namespace unipi {
@@ -37,6 +40,9 @@ void check_cuda(cudaError_t e, const char* what)
 }
 
 inline cudaStream_t stream() { return cudaStreamPerThread; }
+
+// Default bound for staging host operands through pinned buffers.
+constexpr size_t kPinnedStagingMax = size_t(1) << 30;
 
 // Growable per-thread device staging buffers (one per operand slot).
 struct Staging {
@@ -61,13 +67,58 @@ struct Staging {
 };
 thread_local Staging t_staging;
 
+// Growable per-thread pinned host buffers: a host operand is copied into one
+// by the CPU and from there to the device by DMA (and results the other way),
+// instead of handing pageable memory to cudaMemcpyAsync, which stages it
+// through the driver's own buffers and returns only when the copy is done.
+struct Bounce {
+    uint64_t* buf[4] = {nullptr, nullptr, nullptr, nullptr};
+    size_t cap[4] = {0, 0, 0, 0};
+    ~Bounce()
+    {
+        for (auto* p : buf)
+            if (p) cudaFreeHost(p);
+    }
+    uint64_t* get(int slot, size_t words)
+    {
+        if (cap[slot] < words) {
+            if (buf[slot]) cudaFreeHost(buf[slot]);
+            buf[slot] = nullptr;
+            cap[slot] = 0;
+            check_cuda(cudaMallocHost(&buf[slot], words * sizeof(uint64_t)), "pinned staging allocation");
+            cap[slot] = words;
+        }
+        return buf[slot];
+    }
+};
+thread_local Bounce t_bounce;
+
+// Host operands up to this many bytes go through the pinned buffers; larger
+// ones through cudaMemcpyAsync on the pageable memory itself.  Environment
+// variable AXHEL_PINNED_STAGING_MAX (bytes; 0 = never), read once.
+size_t pinned_max()
+{
+    static const size_t v = [] {
+        const char* e = std::getenv("AXHEL_PINNED_STAGING_MAX");
+        return e ? (size_t)std::strtoull(e, nullptr, 10) : kPinnedStagingMax;
+    }();
+    return v;
+}
+
 // Device view of an input operand: the pointer itself if it is device
 // memory, else a staged copy.
 const uint64_t* input(const uint64_t* p, uint64_t n, int slot)
 {
     if (!p || axhel_cuda_is_device_pointer(p)) return p;
     uint64_t* d = t_staging.get(slot, n);
-    check_cuda(cudaMemcpyAsync(d, p, n * sizeof(uint64_t), cudaMemcpyHostToDevice, stream()), "host to device copy");
+    const size_t bytes = n * sizeof(uint64_t);
+    const void* src = p;
+    if (bytes <= pinned_max()) {
+        uint64_t* h = t_bounce.get(slot, n);
+        std::memcpy(h, p, bytes);
+        src = h;
+    }
+    check_cuda(cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, stream()), "host to device copy");
     return d;
 }
 
@@ -87,10 +138,13 @@ struct Output {
     }
     void finish()
     {
+        const size_t bytes = n * sizeof(uint64_t);
+        uint64_t* bounce = (host && bytes <= pinned_max()) ? t_bounce.get(3, n) : nullptr;
         if (host)
-            check_cuda(cudaMemcpyAsync(host, dev, n * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream()),
+            check_cuda(cudaMemcpyAsync(bounce ? bounce : host, dev, bytes, cudaMemcpyDeviceToHost, stream()),
                        "device to host copy");
         check_cuda(cudaStreamSynchronize(stream()), "stream synchronize");
+        if (bounce) std::memcpy(host, bounce, bytes);
     }
 };
 
@@ -104,6 +158,7 @@ void EltwiseAddMod(uint64_t* result, const uint64_t* operand1, const uint64_t* o
     Output out(result, n);
     const uint64_t* a = input(operand1, n, 0);
     const uint64_t* b = input(operand2, n, 1);
+    AXHEL_LOG("EltwiseAddMod vector-vector -> CUDA, n=" << n << (out.host ? ", host result" : ", device result"));
     check(axhel_cuda_eltwise_add_vv(out.dev, a, b, n, modulus, stream()), "EltwiseAddMod");
     out.finish();
 }
@@ -113,6 +168,7 @@ void EltwiseAddMod(uint64_t* result, const uint64_t* operand1, uint64_t operand2
     if (n == 0) return;
     Output out(result, n);
     const uint64_t* a = input(operand1, n, 0);
+    AXHEL_LOG("EltwiseAddMod vector-scalar -> CUDA, n=" << n << (out.host ? ", host result" : ", device result"));
     check(axhel_cuda_eltwise_add_vs(out.dev, a, operand2, n, modulus, stream()), "EltwiseAddMod");
     out.finish();
 }
@@ -123,6 +179,7 @@ void EltwiseSubMod(uint64_t* result, const uint64_t* operand1, const uint64_t* o
     Output out(result, n);
     const uint64_t* a = input(operand1, n, 0);
     const uint64_t* b = input(operand2, n, 1);
+    AXHEL_LOG("EltwiseSubMod vector-vector -> CUDA, n=" << n << (out.host ? ", host result" : ", device result"));
     check(axhel_cuda_eltwise_sub_vv(out.dev, a, b, n, modulus, stream()), "EltwiseSubMod");
     out.finish();
 }
@@ -132,6 +189,7 @@ void EltwiseSubMod(uint64_t* result, const uint64_t* operand1, uint64_t operand2
     if (n == 0) return;
     Output out(result, n);
     const uint64_t* a = input(operand1, n, 0);
+    AXHEL_LOG("EltwiseSubMod vector-scalar -> CUDA, n=" << n << (out.host ? ", host result" : ", device result"));
     check(axhel_cuda_eltwise_sub_vs(out.dev, a, operand2, n, modulus, stream()), "EltwiseSubMod");
     out.finish();
 }
@@ -143,6 +201,7 @@ void EltwiseMulMod(uint64_t* result, const uint64_t* operand1, const uint64_t* o
     Output out(result, n);
     const uint64_t* a = input(operand1, n, 0);
     const uint64_t* b = input(operand2, n, 1);
+    AXHEL_LOG("EltwiseMulMod -> CUDA, mod_factor=" << mod_factor << ", n=" << n);
     check(axhel_cuda_eltwise_mul(out.dev, a, b, n, modulus, mod_factor, stream()), "EltwiseMulMod");
     out.finish();
 }
@@ -154,6 +213,7 @@ void EltwiseFMAMod(uint64_t* res, const uint64_t* op1, uint64_t op2, const uint6
     Output out(res, n);
     const uint64_t* a = input(op1, n, 0);
     const uint64_t* c = input(op3, n, 1);
+    AXHEL_LOG("EltwiseFMAMod -> CUDA, mod_factor=" << mod_factor << ", n=" << n << (c ? ", addend" : ""));
     check(axhel_cuda_eltwise_fma(out.dev, a, op2, c, n, mod, mod_factor, stream()), "EltwiseFMAMod");
     out.finish();
 }
@@ -169,6 +229,8 @@ void EltwiseReduceMod(uint64_t* res, const uint64_t* op, uint64_t n, uint64_t mo
                          in_mod_factor == mod;
     if (!matched) return;  // eltwise-reduce-mod.cpp:32-128: an unmatched pair writes nothing
     const uint64_t* a = input(op, n, 0);
+    AXHEL_LOG("EltwiseReduceMod -> CUDA, in_factor=" << in_mod_factor << ", out_factor=" << out_mod_factor
+                                                      << ", n=" << n);
     check(axhel_cuda_eltwise_reduce(out.dev, a, n, mod, in_mod_factor, out_mod_factor, stream()), "EltwiseReduceMod");
     out.finish();
 }
@@ -215,6 +277,8 @@ void NTT::ComputeForward(uint64_t* result, const uint64_t* operand, uint64_t inp
     const uint64_t n = impl_->degree;
     Output out(result, n);
     const uint64_t* a = input(operand, n, 0);
+    AXHEL_LOG("NTT::ComputeForward -> CUDA, N=" << n << ", out_factor=" << output_mod_factor
+                                                 << (out.host ? ", host operands" : ", device operands"));
     check(axhel_cuda_ntt_forward(impl_->handle, out.dev, a, input_mod_factor, output_mod_factor, stream()),
           "ComputeForward");
     out.finish();
@@ -226,6 +290,8 @@ void NTT::ComputeInverse(uint64_t* result, const uint64_t* operand, uint64_t inp
     const uint64_t n = impl_->degree;
     Output out(result, n);
     const uint64_t* a = input(operand, n, 0);
+    AXHEL_LOG("NTT::ComputeInverse -> CUDA, N=" << n << ", out_factor=" << output_mod_factor
+                                                 << (out.host ? ", host operands" : ", device operands"));
     check(axhel_cuda_ntt_inverse(impl_->handle, out.dev, a, input_mod_factor, output_mod_factor, stream()),
           "ComputeInverse");
     out.finish();

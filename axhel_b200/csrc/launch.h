@@ -13,8 +13,9 @@ int sm_count();
 void count_launch();
 
 // Brackets one launch with CUDA events on its stream while profiling is on
-// (axhel_cuda_profile_enable); a no-op otherwise.  `fmt` names the kernel
-// configuration in the report.
+// (axhel_cuda_profile_enable), and with an NVTX range named like the kernel
+// configuration when the environment variable AXHEL_NVTX is set (non-zero);
+// a no-op otherwise.  `fmt` names the kernel configuration.
 class ProfScope {
 public:
     ProfScope(cudaStream_t s, const char* fmt, ...) __attribute__((format(printf, 3, 4)));
@@ -25,7 +26,11 @@ public:
 private:
     cudaStream_t s_;
     bool on_;
+    bool nvtx_;
 };
+
+// Whether AXHEL_NVTX asks for NVTX ranges (read once).
+bool nvtx_enabled();
 
 void barrett_params(uint64_t q, uint64_t* mu, uint32_t* shift);
 

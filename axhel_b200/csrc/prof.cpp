@@ -1,14 +1,17 @@
-// Launch accounting and the optional per-kernel event timer.
+// Launch accounting, the optional per-kernel event timer and NVTX ranges.
 //
 // When enabled (axhel_cuda_profile_enable), every kernel launch of this
 // library is bracketed by two CUDA events recorded on the launching stream;
 // axhel_cuda_profile_report aggregates launches and device time per kernel
 // configuration.  Off by default: then a launch costs one relaxed atomic add.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <string>
@@ -34,14 +37,26 @@ thread_local bool t_has_open = false;
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
-ProfScope::ProfScope(cudaStream_t s, const char* fmt, ...) : s_(s), on_(g_prof.load(std::memory_order_relaxed))
+bool nvtx_enabled()
 {
-    if (!on_) return;
+    static const bool on = [] {
+        const char* e = std::getenv("AXHEL_NVTX");
+        return e && *e && std::strcmp(e, "0") != 0;
+    }();
+    return on;
+}
+
+ProfScope::ProfScope(cudaStream_t s, const char* fmt, ...)
+    : s_(s), on_(g_prof.load(std::memory_order_relaxed)), nvtx_(nvtx_enabled())
+{
+    if (!on_ && !nvtx_) return;
     char name[128];
     va_list ap;
     va_start(ap, fmt);
     std::vsnprintf(name, sizeof name, fmt, ap);
     va_end(ap);
+    if (nvtx_) nvtxRangePushA(name);
+    if (!on_) return;
     t_open.name = name;
     cudaEventCreate(&t_open.a);
     cudaEventCreate(&t_open.b);
@@ -51,6 +66,7 @@ ProfScope::ProfScope(cudaStream_t s, const char* fmt, ...) : s_(s), on_(g_prof.l
 
 ProfScope::~ProfScope()
 {
+    if (nvtx_) nvtxRangePop();
     if (!on_ || !t_has_open) return;
     cudaEventRecord(t_open.b, s_);
     std::lock_guard<std::mutex> lk(g_prof_mu);

@@ -233,6 +233,53 @@ def cmd_run(args):
     return 0
 
 
+def write_summary(path, records, backend):
+    """Writes summary.csv rows for timed scenarios given as records with the
+    scenario keys and `raw_ns` (per sample, `batch` calls each) -- e.g. a CPU
+    backend timed by wall clock -- with the same statistics and columns as
+    `run` (times in nanoseconds per call)."""
+    with open(path, "w", newline="") as f:
+        w = csv.writer(f)
+        w.writerow(["backend"] + KEYS + METRICS)
+        f3 = lambda x: f"{x:.3f}"
+        for rec in records:
+            per_call = [x / rec["batch"] for x in rec["raw_ns"]]
+            st = statistics(per_call)
+            degree = int(rec["poly_degree"])
+            w.writerow([backend] + [rec[k] for k in KEYS] + [
+                st["samples_total"], st["samples_kept"], st["outliers_removed"], f3(st["raw_min"]),
+                f3(st["raw_max"]), f3(st["q1"]), f3(st["q3"]), f3(st["iqr"]), f3(st["lower_fence"]),
+                f3(st["upper_fence"]), f3(st["min"]), f3(st["max"]), f3(st["mean"]), f3(st["median"]),
+                f3(st["stddev"]), f3(st["cv_percent"]), f3(st["mean"] / degree), f3(st["median"] / degree), 0])
+
+
+def speedup_table(path):
+    """Markdown table of a compare output: per kernel and degree, the median
+    over modulus widths of the CPU / GPU median-time ratio."""
+    with open(path, newline="") as f:
+        rows = list(csv.DictReader(f))
+    by = {}
+    for r in rows:
+        by.setdefault((r["kernel"], int(r["poly_degree"])), []).append(
+            (float(r["speedup_median_cpu_over_gpu"]), float(r["cpu_median_ns"]), float(r["gpu_median_ns"])))
+    degrees = sorted({d for _, d in by})
+    kernels = [k for k in KERNELS if any((k, d) in by for d in degrees)]
+    med = lambda v: sorted(v)[len(v) // 2]
+    lines = ["| kernel | " + " | ".join(f"N={d}" for d in degrees) + " |",
+             "|---|" + "---|" * len(degrees)]
+    for k in kernels:
+        cells = []
+        for d in degrees:
+            v = by.get((k, d))
+            if not v:
+                cells.append("")
+                continue
+            cells.append(f"{med([x[0] for x in v]):.2f}x ({med([x[1] for x in v]) / 1e3:.1f} / "
+                         f"{med([x[2] for x in v]) / 1e3:.1f} us)")
+        lines.append(f"| {k} | " + " | ".join(cells) + " |")
+    return "\n".join(lines)
+
+
 def load_summary(path):
     with open(path, newline="") as f:
         rows = list(csv.DictReader(f))
@@ -246,7 +293,9 @@ def cmd_compare(args):
     common = sorted(set(cpu) & set(gpu), key=lambda k: (k[0], int(k[1]), int(k[2])))
     if not common:
         raise SystemExit("no scenario appears in both summaries")
-    ghz = args.cpu_ghz
+    ghz = 1.0 if args.cpu_unit == "ns" else args.cpu_ghz
+    if ghz is None:
+        raise SystemExit("--cpu-ghz is required for a CPU summary in cycles")
     Path(args.output).parent.mkdir(parents=True, exist_ok=True)
     with open(args.output, "w", newline="") as f:
         w = csv.writer(f)
@@ -280,7 +329,9 @@ def main(argv=None):
     c.add_argument("cpu_summary")
     c.add_argument("gpu_summary")
     c.add_argument("output")
-    c.add_argument("--cpu-ghz", type=float, required=True, help="clock converting the CPU summary's cycles to ns")
+    c.add_argument("--cpu-ghz", type=float, default=None, help="clock converting the CPU summary's cycles to ns")
+    c.add_argument("--cpu-unit", choices=["cycles", "ns"], default="cycles",
+                   help="unit of the CPU summary's *_cycles columns (ns: a wall-clock summary)")
     a = ap.parse_args(argv)
     return cmd_run(a) if a.cmd == "run" else cmd_compare(a)
 

@@ -388,6 +388,13 @@ def run_ours(args):
         serve["workload"] = ("INTT->MulMod/FMAMod->NTT requests, N in 2^13..2^17, L in 2..40, 24 templates, "
                              "Poisson arrivals at 50/70/90 % of capacity, HBM budget 60 GB; headline figures at 70 %")
 
+    dropin = None
+    if rank == 0 and not args.no_dropin:
+        try:
+            dropin = dropin_host(with_reference=world == 1 and not args.no_cpu)
+        except Exception as e:  # the timer is a separate program; report why it did not run
+            dropin = {"unavailable": str(e)[:300]}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -418,6 +425,7 @@ def run_ours(args):
             "e2e": e2e,
             "serve": serve,
             "configs": others,
+            "dropin_host": dropin,
             "tables": {"contexts": len(mods), "degree": N, "device_ms": tables_ms,
                        "reference_cpu_ms": cpu["tables_ms"] if cpu and "tables_ms" in cpu else None,
                        "note": "cold start: twiddle tables of the 24 moduli, device generation (one launch, "
@@ -464,6 +472,64 @@ def headline_digest_check(capi, ntts, xp, y, sh, want):
         return {"same_bits": None}
     return {"same_bits": f == want["headline"]["forward_lazy_sha256"] and b == want["headline"]["round_trip_sha256"],
             "checked": "forward lazy outputs and round-trip outputs of all 768 limbs"}
+
+
+def dropin_cases():
+    """(logn, q, psi) per degree 2^12..2^17: a 50-bit NTT prime of each."""
+    from axhel_b200 import params
+
+    out = []
+    for logn in range(12, 18):
+        n = 1 << logn
+        q = params.ntt_prime_near(n, 50, 1, 4)
+        out.append((logn, q, params.primitive_root(n, q)))
+    return out
+
+
+def dropin_timer(exe, threads, seconds, cases):
+    """Runs a build of axhel_b200/tools/dropin_bench.cpp: {(op, logn): us per call}."""
+    args = [exe, str(threads), str(seconds)] + [f"{l}:{q}:{p}" for l, q, p in cases]
+    r = subprocess.run(args, capture_output=True, text=True, timeout=600)
+    if r.returncode != 0:
+        raise RuntimeError(f"{os.path.basename(exe)} failed: {r.stderr[-400:]}")
+    out = {}
+    for line in r.stdout.splitlines():
+        d = json.loads(line)
+        out[(d["op"], d["logn"])] = d
+    return out
+
+
+def dropin_host(with_reference, threads_list=(1, 8), seconds=0.2):
+    """SEAL's call pattern through the C++ drop-in: host (pageable) pointers,
+    one limb per call, in place, threads sharing one cached NTT object --
+    ComputeForward(p,p,4,4), ComputeInverse(p,p,2,1), EltwiseMulMod(p,p,b,N,q,4)
+    and the N-point plain round trip (two forwards, MulMod, AddMod with a
+    scalar, inverse) -- against the same program linked to the reference
+    native backend (oracle/_ref/dropin_bench_ref).  Mean microseconds per call
+    seen by a thread; the crossover is the smallest degree from which the GPU
+    call is faster than the reference's."""
+    cases = dropin_cases()
+    ours_exe = os.path.join(ROOT, "axhel_b200", "dropin_bench")
+    ref_exe = os.path.join(ROOT, "oracle", "_ref", "dropin_bench_ref")
+    out = {"unit": "us per call (mean per thread)", "pattern": "host pageable buffers, one limb per call, in place, "
+           "threads share one const NTT per degree; 50-bit primes", "rows": []}
+    crossover = {}
+    for threads in threads_list:
+        ours = dropin_timer(ours_exe, threads, seconds, cases)
+        ref = dropin_timer(ref_exe, threads, seconds, cases) if with_reference and os.path.exists(ref_exe) else {}
+        for (op, logn), d in sorted(ours.items(), key=lambda kv: (kv[0][0], kv[0][1])):
+            row = {"op": op, "logn": logn, "threads": threads, "us": d["us_per_call"],
+                   "calls_per_s": d["calls_per_s"]}
+            if (op, logn) in ref:
+                r = ref[(op, logn)]
+                row.update({"reference_us": r["us_per_call"], "reference_calls_per_s": r["calls_per_s"],
+                            "speedup": r["us_per_call"] / d["us_per_call"]})
+                key = f"{op}@{threads}t"
+                if row["speedup"] > 1 and key not in crossover:
+                    crossover[key] = 1 << logn
+            out["rows"].append(row)
+    out["crossover_degree"] = crossover
+    return out
 
 
 def plain_per_limb(capi, ntts, x, y, sh, limbs):
@@ -559,6 +625,45 @@ def end_to_end(capi, ntts, data, dev, steps, chunks=8):
             "pipeline": f"{chunks} chunks over 3 streams, steps back to back"}
 
 
+def run_kernel_table(args):
+    """The per-kernel comparison table: every public kernel over the reference
+    benchmark's scenario matrix (degrees 2048..32768 x widths 20..62), timed
+    on the GPU by axhel_b200.harness (device time per call) and, as the CPU
+    baseline, the reference native backend (oracle/_ref/kernel_timer_ref,
+    wall time per call on one host thread); both summaries in the reference's
+    summary.csv columns, joined into speedup.csv, plus a markdown digest."""
+    from pathlib import Path
+
+    import torch
+
+    from axhel_b200 import harness, params
+
+    out = Path(args.kernel_table)
+    out.mkdir(parents=True, exist_ok=True)
+    reps, warm = 30, 5
+    torch.cuda.set_device(0)
+    harness.main(["run", "--output", str(out / "b200"), "--repetitions", str(reps), "--warmup", str(warm),
+                  "--no-raw"])
+    exe = os.path.join(ROOT, "oracle", "_ref", "kernel_timer_ref")
+    cases = []
+    for d in harness.DEGREES:
+        for b in harness.BITS:
+            q = harness.largest_ntt_prime(d, b)
+            cases.append(f"{d}:{b}:{q}:{params.primitive_root(d, q)}")
+    r = subprocess.run([exe, str(reps), str(warm), "1"] + cases, capture_output=True, text=True, timeout=1800)
+    if r.returncode != 0:
+        raise RuntimeError(f"kernel_timer_ref failed: {r.stderr[-400:]}")
+    (out / "reference").mkdir(exist_ok=True)
+    recs = [json.loads(l) for l in r.stdout.splitlines() if l.strip()]
+    harness.write_summary(out / "reference" / "summary.csv", recs, "reference-native-1thread")
+    harness.main(["compare", str(out / "reference" / "summary.csv"), str(out / "b200" / "summary.csv"),
+                  str(out / "speedup.csv"), "--cpu-unit", "ns"])
+    table = harness.speedup_table(out / "speedup.csv")
+    (out / "speedup.md").write_text(table + "\n")
+    print(table, flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -569,9 +674,15 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop measurement")
     ap.add_argument("--no-others", action="store_true", help="skip the tensor-product and uneven-batch workloads")
+    ap.add_argument("--no-dropin", action="store_true", help="skip the C++ drop-in per-call timings")
     ap.add_argument("--profile-step", action="store_true",
                     help="warm up, run one step and exit (the command profiled by ncu)")
+    ap.add_argument("--kernel-table", metavar="DIR", default=None,
+                    help="write the per-kernel GPU vs reference table (summary.csv both sides, speedup.csv) to DIR "
+                         "and exit")
     args = ap.parse_args()
+    if args.kernel_table:
+        return run_kernel_table(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

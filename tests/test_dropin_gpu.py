@@ -18,7 +18,8 @@ def cuda_include():
     pytest.skip("CUDA headers not found")
 
 
-def test_cpp_dropin(tmp_path, cuda):
+@pytest.mark.parametrize("pinned_max", [None, "0"], ids=["pinned-staging", "pageable-staging"])
+def test_cpp_dropin(tmp_path, cuda, pinned_max):
     exe = tmp_path / "test_dropin"
     lib_dir = os.path.join(ROOT, "axhel_b200")
     orc = tmp_path / "axhel_oracle.o"
@@ -28,6 +29,9 @@ def test_cpp_dropin(tmp_path, cuda):
            "-Wl,-rpath," + lib_dir, "-L/usr/local/cuda/lib64", "-lcudart", "-Wl,-rpath,/usr/local/cuda/lib64",
            "-lpthread", "-o", str(exe)]
     subprocess.run(cmd, check=True, capture_output=True, text=True)
-    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    env = dict(os.environ)
+    if pinned_max is not None:  # host operands handed to cudaMemcpyAsync as they are
+        env["AXHEL_PINNED_STAGING_MAX"] = pinned_max
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600, env=env)
     assert r.returncode == 0, r.stderr[-4000:]
     assert "all checks passed" in r.stdout

@@ -59,3 +59,25 @@ def test_small_run_writes_every_kernel(tmp_path, cuda):
         assert r["backend"] == "B200" and int(r["samples_total"]) == 7
         assert 0 < float(r["median_cycles"]) < 1e7  # ns per call
     assert (tmp_path / "metadata.txt").read_text().count("unit=nanoseconds") == 1
+
+
+def test_wall_clock_summary_joins_in_nanoseconds(tmp_path):
+    """A CPU backend timed by wall clock (records of raw ns samples) gets the
+    same summary columns and statistics, and joins without a clock rate."""
+    recs = [dict(kernel="ntt_forward", poly_degree=4096, qi_bits=50, modulus=1125899906826241, mod_factor=0,
+                 input_mod_factor=1, output_mod_factor=1, batch=2, raw_ns=[20000.0, 21000.0, 20500.0, 90000.0]),
+            dict(kernel="add_vv", poly_degree=4096, qi_bits=50, modulus=1125899906826241, mod_factor=0,
+                 input_mod_factor=0, output_mod_factor=0, batch=1, raw_ns=[3000.0, 3100.0, 2900.0])]
+    harness.write_summary(tmp_path / "cpu.csv", recs, "reference-native-1thread")
+    rows = {r["kernel"]: r for r in csv.DictReader(open(tmp_path / "cpu.csv"))}
+    assert list(next(iter(rows.values())).keys()) == ["backend"] + harness.KEYS + harness.METRICS
+    assert int(rows["ntt_forward"]["outliers_removed"]) == 1
+    assert float(rows["ntt_forward"]["median_cycles"]) == pytest.approx(10250.0)
+    gpu = {**recs[0], "raw_ns": [2050.0] * 4, "batch": 1}
+    harness.write_summary(tmp_path / "gpu.csv", [gpu], "B200")
+    assert harness.main(["compare", str(tmp_path / "cpu.csv"), str(tmp_path / "gpu.csv"), str(tmp_path / "s.csv"),
+                         "--cpu-unit", "ns"]) == 0
+    out = list(csv.DictReader(open(tmp_path / "s.csv")))
+    assert len(out) == 1 and float(out[0]["speedup_median_cpu_over_gpu"]) == pytest.approx(5.0)
+    md = harness.speedup_table(tmp_path / "s.csv")
+    assert "| ntt_forward | 5.00x" in md

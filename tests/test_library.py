@@ -136,3 +136,23 @@ def test_batch_split_table_and_override(tmp_path):
     for logn, row in ((16, 4), (16, 12), (12, 8), (9, 5), (18, 9)):
         with pytest.raises(capi.AxhelError):
             capi.batch_split_set(logn, row)
+
+
+def test_debug_log_build_compiles(tmp_path):
+    """The AXHEL_DEBUG build of the drop-in (AXHEL_LOG lines on every call,
+    axhel/util/debug.hpp) compiles; the default build compiles them out."""
+    cuda_inc = "/usr/local/cuda/include"
+    if not os.path.exists(os.path.join(cuda_inc, "cuda_runtime.h")):
+        pytest.skip("CUDA headers not found")
+    src = os.path.join(ROOT, "axhel_b200", "csrc", "dropin.cpp")
+    for defs in (["-DAXHEL_DEBUG"], []):
+        subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-Wall", "-Werror", *defs,
+                        "-I" + os.path.join(ROOT, "include"), "-I" + cuda_inc, src], check=True)
+    probe = tmp_path / "log.cpp"
+    probe.write_text('#include <axhel/util/debug.hpp>\n#include <sstream>\n'
+                     'int main() { AXHEL_LOG("x=" << 1); return 0; }\n')
+    exe = tmp_path / "log"
+    subprocess.run(["g++", "-std=c++17", "-DAXHEL_DEBUG", "-I" + os.path.join(ROOT, "include"), str(probe), "-o",
+                    str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, check=True)
+    assert r.stderr == "[AXHEL] x=1\n"
