@@ -67,14 +67,15 @@ class ServerStats(C.Structure):
     _fields_ = [("completed", C.c_uint64), ("batches", C.c_uint64), ("max_batch_requests", C.c_uint64),
                 ("pending", C.c_uint64), ("in_use_bytes", C.c_uint64), ("peak_in_use_bytes", C.c_uint64),
                 ("samples", C.c_uint64), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
-                ("pool_used_bytes", C.c_uint64)]
+                ("pool_used_bytes", C.c_uint64), ("host_us_per_batch", C.c_double)]
 
 
 class DriveResult(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("skipped", C.c_uint64),
                 ("failed", C.c_uint64), ("wall_s", C.c_double), ("jobs_per_s", C.c_double),
                 ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("p50_slowdown", C.c_double),
-                ("p99_slowdown", C.c_double), ("isolated_p99_ms", C.c_double)]
+                ("p99_slowdown", C.c_double), ("isolated_p99_ms", C.c_double), ("p50_queue_ms", C.c_double),
+                ("p99_queue_ms", C.c_double), ("p99_large_ms", C.c_double), ("p99_rest_ms", C.c_double)]
 
 
 class AxhelError(RuntimeError):

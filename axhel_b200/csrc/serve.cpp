@@ -121,6 +121,7 @@ struct axhel_server {
     std::string fatal;
     std::vector<cudaEvent_t> event_pool;  // reused completion events
     std::atomic<int> debug_fail_at{-1};   // failure injection: staging of the next batch fails at this request
+    double host_us_total = 0;             // scheduler time spent in launch(), all batches
 
     cudaEvent_t get_event()
     {
@@ -369,8 +370,11 @@ void axhel_server::scheduler()
         lk.unlock();
         Inflight f;
         f.id = bid;
+        const auto h0 = Clock::now();
         const axhel_status_t rc = launch(slots[si], si, take, f);
+        const double host_us = std::chrono::duration<double, std::micro>(Clock::now() - h0).count();
         lk.lock();
+        host_us_total += host_us;
         if (rc) {
             for (Req* q : take) {
                 q->status = rc;
@@ -626,6 +630,7 @@ axhel_status_t axhel_server_stats(axhel_server_t s, axhel_server_stats_t* out, i
     uint64_t used = 0;  // a 64-bit attribute value
     out->pool_used_bytes =
         cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess ? (uint64_t)used : 0;
+    out->host_us_per_batch = s->batches ? s->host_us_total / (double)s->batches : 0.0;
     if (reset_latencies) s->lat_ms.clear();
     return AXHEL_OK;
 }
@@ -684,7 +689,15 @@ axhel_status_t axhel_server_drive(axhel_server_t server, const axhel_request_t* 
     std::deque<Live> live;
     std::condition_variable lv;
     bool done = false;
-    std::vector<double> lat, slow, iso;
+    std::vector<double> lat, slow, iso, queue, lat_large, lat_rest;
+    // templates in the top quarter of isolated latency
+    std::vector<char> large(n_templates, 0);
+    if (isolated_ms) {
+        std::vector<double> v(isolated_ms, isolated_ms + n_templates);
+        std::sort(v.begin(), v.end());
+        const double cut = v[(size_t)(0.75 * (n_templates - 1) + 0.5)];
+        for (uint32_t t = 0; t < n_templates; ++t) large[t] = isolated_ms[t] >= cut;
+    }
     uint64_t failed = 0;
     // collector: waits for requests in submission order, frees their copies
     std::thread collector([&] {
@@ -704,6 +717,8 @@ axhel_status_t axhel_server_drive(axhel_server_t server, const axhel_request_t* 
                 ++failed;
             } else {
                 lat.push_back(info.latency_ms);
+                queue.push_back(info.queue_ms);
+                (large[l.t] ? lat_large : lat_rest).push_back(info.latency_ms);
                 if (isolated_ms) {
                     slow.push_back(info.latency_ms / isolated_ms[l.t]);
                     iso.push_back(isolated_ms[l.t]);
@@ -775,6 +790,10 @@ axhel_status_t axhel_server_drive(axhel_server_t server, const axhel_request_t* 
     out->p50_slowdown = pct(slow, 0.5);
     out->p99_slowdown = pct(slow, 0.99);
     out->isolated_p99_ms = pct(iso, 0.99);
+    out->p50_queue_ms = pct(queue, 0.5);
+    out->p99_queue_ms = pct(queue, 0.99);
+    out->p99_large_ms = pct(lat_large, 0.99);
+    out->p99_rest_ms = pct(lat_rest, 0.99);
     return rc;
 }
 

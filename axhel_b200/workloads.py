@@ -388,6 +388,8 @@ def serving(loads=(0.5, 0.7, 0.9), seconds=4.0, budget=60 << 30, inflight=4, see
                         "p50_ms": d["p50_ms"], "p99_ms": d["p99_ms"], "isolated_p99_ms": d["isolated_p99_ms"],
                         "p99_over_isolated_p99": d["p99_ms"] / d["isolated_p99_ms"] if d["isolated_p99_ms"] else None,
                         "p50_slowdown": d["p50_slowdown"], "p99_slowdown": d["p99_slowdown"],
+                        "p50_queue_ms": d["p50_queue_ms"], "p99_queue_ms": d["p99_queue_ms"],
+                        "p99_large_ms": d["p99_large_ms"], "p99_rest_ms": d["p99_rest_ms"],
                         "requests": d["completed"], "skipped_no_buffer": d["skipped"], "failed": d["failed"]})
     st = srv.stats()
     srv.close()
@@ -398,6 +400,7 @@ def serving(loads=(0.5, 0.7, 0.9), seconds=4.0, budget=60 << 30, inflight=4, see
            "small_request_words": small_words, "policy": policy_name(flags, aging_us),
            "capacity_jobs_per_s": cap, "isolated_median_ms": statistics.median(iso), "loads": results,
            "batches": st["batches"], "max_batch_requests": st["max_batch_requests"],
+           "host_us_per_batch": st["host_us_per_batch"],
            "peak_in_use_bytes": st["peak_in_use_bytes"], "budget_bytes": budget, "max_inflight": inflight}
     if plain:
         out["plain_sequential_jobs_per_s"] = plain_sequential(rp)
@@ -502,6 +505,12 @@ def kernel_case(family):
         outs = [torch.empty_like(ins[0]) for _ in range(3)]
         for _ in range(2):
             capi.tensor_product(*[o.data_ptr() for o in outs], *[x.data_ptr() for x in ins], n, cnt, qs, 1)
+    elif family == "peak":  # the register-only butterfly probe, forward then inverse (two launches each)
+        n = 1 << 16
+        q, psi = params.rns_moduli(n, 1, 50, 50)[0]
+        t = capi.NTT(n, q, psi)
+        for inv in (False, True):
+            capi.butterfly_peak(t, inv)
     elif family == "tables":  # 3 x 24 fresh contexts of N = 2^16
         for lo, hi in ((30, 40), (41, 51), (52, 62)):
             capi.NTT.create_many([(1 << 16, q, psi) for q, psi in params.rns_moduli(1 << 16, 24, lo, hi)])
@@ -535,7 +544,7 @@ def main():
     ap.add_argument("what", choices=["tensor", "uneven", "serve", "eltwise", "case"])
     ap.add_argument("family", nargs="?", default="eltwise",
                     help="case: eltwise | eltwise_unaligned | tensor | tables | chain | batch | batch_phased | "
-                         "batch_eltwise")
+                         "batch_eltwise | peak")
     ap.add_argument("--seconds", type=float, default=4.0)
     ap.add_argument("--device", action="store_true", help="device-resident request operands")
     ap.add_argument("--persistent", action="store_true", help="one persistent launch per batch")

@@ -289,6 +289,7 @@ typedef struct axhel_server_stats {
     uint64_t completed, batches, max_batch_requests, pending, in_use_bytes, peak_in_use_bytes, samples;
     double p50_ms, p99_ms;    /* submit -> done latency over completed requests */
     uint64_t pool_used_bytes; /* device bytes allocated from the staging pool now (frees land in stream order) */
+    double host_us_per_batch; /* mean scheduler time per batch: staging, descriptors, launches */
 } axhel_server_stats_t;
 
 /* Starts the scheduler and completion threads on the current device. */
@@ -318,6 +319,9 @@ typedef struct axhel_drive_result {
     uint64_t submitted, completed, skipped, failed;
     double wall_s, jobs_per_s;
     double p50_ms, p99_ms, p50_slowdown, p99_slowdown, isolated_p99_ms;
+    double p50_queue_ms, p99_queue_ms; /* submit -> admitted into a batch */
+    double p99_large_ms;               /* p99 latency of the templates in the top quarter of isolated latency */
+    double p99_rest_ms;                /* p99 latency of the other templates */
 } axhel_drive_result_t;
 axhel_status_t axhel_server_drive(axhel_server_t server, const axhel_request_t* templates, uint32_t n_templates,
                                   uint64_t* const* outputs, uint32_t copies, const double* isolated_ms,
