@@ -40,13 +40,14 @@ class Job(C.Structure):
 SERVER_PERSISTENT = 1
 SERVER_ARRIVAL_PRIORITY = 2
 SERVER_SMALLEST_FIRST = 4
+SERVER_LARGE_FIRST = 8
 
 
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_batch_words", C.c_uint64),
                 ("small_request_words", C.c_uint64), ("max_inflight", C.c_uint32),
                 ("max_batch_requests", C.c_uint32), ("flags", C.c_uint32), ("aging_us", C.c_uint32),
-                ("reserve_bytes", C.c_uint64)]
+                ("reserve_bytes", C.c_uint64), ("batch_size_ratio", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class Request(C.Structure):
@@ -133,6 +134,8 @@ def _declare(L):
     d("axhel_cuda_plan_set", st_t, C.c_int, u32, u32, vp, vp, vp)
     d("axhel_cuda_plan_get", st_t, C.c_int, u32, u64, vp, vp, vp, vp)
     d("axhel_cuda_plan_load", st_t, C.c_char_p, C.POINTER(u32))
+    d("axhel_cuda_plan_set_prefetch", st_t, C.c_int, u32, u32)
+    d("axhel_cuda_plan_get_prefetch", st_t, C.c_int, u32, u64, C.POINTER(u32))
     d("axhel_cuda_batch_split_set", st_t, u32, u32)
     d("axhel_cuda_batch_split_get", st_t, u32, C.POINTER(u32))
     d("axhel_cuda_is_device_pointer", C.c_int, vp)
@@ -284,10 +287,10 @@ class Server:
     """The continuous-batching serving loop (axhel_server_*)."""
 
     def __init__(self, budget_bytes, max_inflight=2, max_batch_requests=256, max_batch_words=0, persistent=False,
-                 small_request_words=0, reserve_bytes=0, flags=0, aging_us=0):
+                 small_request_words=0, reserve_bytes=0, flags=0, aging_us=0, batch_size_ratio=0):
         flags |= SERVER_PERSISTENT if persistent else 0
         cfg = ServerConfig(budget_bytes, max_batch_words, small_request_words, max_inflight, max_batch_requests,
-                           flags, aging_us, reserve_bytes)
+                           flags, aging_us, reserve_bytes, batch_size_ratio, 0)
         self.h = vp()
         _scheck(lib().axhel_server_create(C.byref(cfg), C.byref(self.h)), "server_create")
         self._keep = {}
@@ -484,21 +487,27 @@ def tensor_product(r0, r1, r2, c0, c1, d0, d1, n, count, moduli, factor=1, strea
 
 
 def plan_set(inverse, logn, passes):
-    """passes: list of (lg, lr, tg); [] restores the default."""
+    """passes: list of (lg, lr, tg) or (lg, lr, tg, prefetch); [] restores the default."""
     n = len(passes)
     lg = (u32 * 3)(*[p[0] for p in passes])
     lr = (u32 * 3)(*[p[1] for p in passes])
     tg = (u32 * 3)(*[p[2] for p in passes])
     check(lib().axhel_cuda_plan_set(int(inverse), logn, n, C.cast(lg, vp), C.cast(lr, vp), C.cast(tg, vp)),
           "plan_set")
+    mask = sum(1 << i for i, p in enumerate(passes) if len(p) > 3 and p[3])
+    if n and mask:
+        check(lib().axhel_cuda_plan_set_prefetch(int(inverse), logn, mask), "plan_set_prefetch")
 
 
 def plan_get(inverse, logn, count):
+    """[(lg, lr, tg, prefetch)] of the plan used for `count` limbs."""
     npass = u32()
     lg, lr, tg = (u32 * 3)(), (u32 * 3)(), (u32 * 3)()
     check(lib().axhel_cuda_plan_get(int(inverse), logn, count, C.byref(npass), C.cast(lg, vp), C.cast(lr, vp),
                                     C.cast(tg, vp)), "plan_get")
-    return [(lg[i], lr[i], tg[i]) for i in range(npass.value)]
+    mask = u32()
+    check(lib().axhel_cuda_plan_get_prefetch(int(inverse), logn, count, C.byref(mask)), "plan_get_prefetch")
+    return [(lg[i], lr[i], tg[i], (mask.value >> i) & 1) for i in range(npass.value)]
 
 
 def batch_split_set(logn, row_stages):

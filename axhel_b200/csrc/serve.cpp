@@ -250,7 +250,11 @@ axhel_status_t axhel_server::launch(Slot& s, int slot_index, std::vector<Req*>& 
     cudaError_t e = cudaMemcpyAsync(desc, s.host_img, img.size(), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
         e = per_phase ? axhel_impl::batch_launch_classes(classes, st, &s.lanes) : axhel_impl::batch_launch_args(args, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(s.err_host, args.error, sizeof(int), cudaMemcpyDeviceToHost, st);
+    // only the persistent kernel's dependency waits can set the error word
+    if (e == cudaSuccess && !per_phase)
+        e = cudaMemcpyAsync(s.err_host, args.error, sizeof(int), cudaMemcpyDeviceToHost, st);
+    else if (per_phase)
+        *s.err_host = AXHEL_OK;
     // results back smallest first; each request completes at its own event
     std::vector<Req*> order(take);
     std::stable_sort(order.begin(), order.end(), [](const Req* a, const Req* b) { return a->words < b->words; });
@@ -323,8 +327,9 @@ void axhel_server::scheduler()
     for (;;) {
         cv_sched.wait(lk, [&] { return stop || (!paused && (runnable(0) || runnable(1))); });
         if (stop) break;
-        // the small-request lane first, then the other
-        const int lane = runnable(0) ? 0 : 1;
+        // the high-priority lane first, then the other
+        const int first = (cfg.flags & AXHEL_SERVER_LARGE_FIRST) ? 1 : 0;
+        const int lane = runnable(first) ? first : 1 - first;
         std::deque<Req*>& queue = pending[lane];
         order_queue(queue);
         // admit in queue order while the budget allows
@@ -339,6 +344,10 @@ void axhel_server::scheduler()
             }
             if (in_use + bytes + q->need > cfg.hbm_budget_bytes) break;
             if (cfg.max_batch_words && !take.empty() && words + q->words > cfg.max_batch_words) break;
+            if (cfg.batch_size_ratio && !take.empty()) {
+                const uint64_t a = take.front()->words, b = q->words;
+                if (std::max(a, b) > (uint64_t)cfg.batch_size_ratio * std::min(a, b)) break;
+            }
             bytes += q->need;
             words += q->words;
             queue.pop_front();
@@ -474,7 +483,8 @@ axhel_status_t axhel_server_create(const axhel_server_config_t* cfg, axhel_serve
         // with two lanes, lane 0 (small requests) gets the highest priority:
         // its CTAs are dispatched ahead of the large lane's as SMs free up
         sl.lane = s->lanes == 2 ? (int)(i / cfg->max_inflight) : 1;
-        int prio = sl.lane == 0 ? prio_high : prio_low;
+        const bool large_first = cfg->flags & AXHEL_SERVER_LARGE_FIRST;
+        int prio = (sl.lane == 0) != large_first ? prio_high : prio_low;
         if (cfg->flags & AXHEL_SERVER_ARRIVAL_PRIORITY) {
             // the lane's k-th slot at the k-th highest priority (the rest at
             // the lowest): the order in which the scheduler fills them

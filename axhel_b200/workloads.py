@@ -335,16 +335,20 @@ def _pct(v, p):
 
 def serving(loads=(0.5, 0.7, 0.9), seconds=4.0, budget=60 << 30, inflight=4, seed=5, n_templates=32,
             device=False, max_batch_words=0, persistent=False, plain=True, small_words=0, reserve=8 << 30,
-            max_batch_requests=256, flags=0, aging_us=0):
+            max_batch_requests=256, flags=0, aging_us=0, batch_size_ratio=0, small_pct=None):
     """Isolated latency of every template (alone on an idle server), capacity
     (a burst), then Poisson arrivals at each load fraction of capacity
     (host-staged requests: `reserve` bytes of the staging pool mapped up
     front): p50/p99 latency, p99 of each request's slowdown against its own isolated
     latency, and jobs/s; then the plain sequential GPU path."""
     rp = RequestPool(n_templates=n_templates, seed=seed, device=device)
+    if small_pct is not None:  # two lanes split at this percentile of the templates' sizes
+        sizes = sorted(t["n"] * t["L"] for t in rp.t)
+        small_words = sizes[min(len(sizes) - 1, int(small_pct / 100 * (len(sizes) - 1)))]
     srv = capi.Server(budget_bytes=budget, max_inflight=inflight, max_batch_requests=max_batch_requests,
                       max_batch_words=max_batch_words, persistent=persistent, small_request_words=small_words,
-                      reserve_bytes=0 if device else reserve, flags=flags, aging_us=aging_us)
+                      reserve_bytes=0 if device else reserve, flags=flags, aging_us=aging_us,
+                      batch_size_ratio=batch_size_ratio)
     rng = np.random.default_rng(seed)
 
     iso = []
@@ -398,6 +402,7 @@ def serving(loads=(0.5, 0.7, 0.9), seconds=4.0, budget=60 << 30, inflight=4, see
            "operands": "device-resident" if device else "host pinned, staged per request",
            "launch": "persistent" if persistent else "per-phase class launches", "max_batch_words": max_batch_words,
            "small_request_words": small_words, "policy": policy_name(flags, aging_us),
+           "batch_size_ratio": batch_size_ratio, "max_batch_requests_cfg": max_batch_requests,
            "capacity_jobs_per_s": cap, "isolated_median_ms": statistics.median(iso), "loads": results,
            "batches": st["batches"], "max_batch_requests": st["max_batch_requests"],
            "host_us_per_batch": st["host_us_per_batch"],
@@ -414,6 +419,8 @@ def policy_name(flags, aging_us=0):
         parts.append("arrival-priority streams")
     if flags & capi.SERVER_SMALLEST_FIRST:
         parts.append(f"smallest-first admission (aging {aging_us} us)")
+    if flags & capi.SERVER_LARGE_FIRST:
+        parts.append("large-request lane at high priority")
     return ", ".join(parts) or "arrival-order admission, equal-priority streams"
 
 
@@ -555,6 +562,10 @@ def main():
     ap.add_argument("--arrival-priority", action="store_true", help="batches in flight prioritised by launch order")
     ap.add_argument("--smallest-first", action="store_true", help="admit the smallest pending requests first")
     ap.add_argument("--aging-us", type=int, default=0, help="smallest-first: pending time after which arrival wins")
+    ap.add_argument("--large-first", action="store_true", help="two lanes, the large-request lane at high priority")
+    ap.add_argument("--small-pct", type=float, default=None,
+                    help="two lanes split at this percentile of the templates' sizes")
+    ap.add_argument("--size-ratio", type=int, default=0, help="batches only of requests within this size factor")
     ap.add_argument("--loads", default="0.5,0.7,0.9")
     ap.add_argument("--templates", type=int, default=24, help="request templates (the bench uses 24)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain sequential comparison")
@@ -569,11 +580,12 @@ def main():
         out = uneven_batch()
     else:
         flags = (capi.SERVER_ARRIVAL_PRIORITY if a.arrival_priority else 0) | \
-            (capi.SERVER_SMALLEST_FIRST if a.smallest_first else 0)
+            (capi.SERVER_SMALLEST_FIRST if a.smallest_first else 0) | (capi.SERVER_LARGE_FIRST if a.large_first else 0)
         out = serving(loads=tuple(float(x) for x in a.loads.split(",")), seconds=a.seconds, device=a.device,
                       persistent=a.persistent, max_batch_words=a.max_batch_words, inflight=a.inflight,
                       small_words=a.small_words, max_batch_requests=a.max_batch_requests, flags=flags,
-                      aging_us=a.aging_us, n_templates=a.templates, plain=not a.no_plain)
+                      aging_us=a.aging_us, n_templates=a.templates, plain=not a.no_plain,
+                      batch_size_ratio=a.size_ratio, small_pct=a.small_pct)
     print(json.dumps(out), flush=True)
 
 

@@ -247,6 +247,10 @@ typedef struct axhel_server* axhel_server_t;
  * a request pending longer than aging_us goes ahead of them in arrival
  * order, so large requests are not starved. */
 #define AXHEL_SERVER_SMALLEST_FIRST 4u
+/* With two lanes (small_request_words > 0), the lane of the LARGER requests
+ * gets the high stream priority instead of the small one: the largest
+ * requests, which set the latency tail, pass the small ones on the SMs. */
+#define AXHEL_SERVER_LARGE_FIRST 8u
 
 typedef struct axhel_server_config {
     uint64_t hbm_budget_bytes;    /* device bytes the server may hold for staged operands */
@@ -258,6 +262,9 @@ typedef struct axhel_server_config {
     uint32_t aging_us;            /* AXHEL_SERVER_SMALLEST_FIRST: pending time after which arrival order wins */
     uint64_t reserve_bytes;       /* device memory mapped for staging at creation (capped at the budget; 0 = on
                                      demand): growing the pool later stalls the request that needs it */
+    uint32_t batch_size_ratio;    /* a batch only takes requests within this factor of the size of its first one
+                                     (0 = any size): small requests do not wait inside a large one's batch */
+    uint32_t reserved;
 } axhel_server_config_t;
 
 /* One request: a job of the batch engine (AXHEL_JOB_*).  input / output /
@@ -384,6 +391,14 @@ axhel_status_t axhel_cuda_plan_set(int inverse, uint32_t log_degree, uint32_t np
 /* Reads the plan used for (inverse, log2 N, count limbs); arrays of >= 3. */
 axhel_status_t axhel_cuda_plan_get(int inverse, uint32_t log_degree, uint64_t count, uint32_t* npass, uint32_t* lg,
                                    uint32_t* lr, uint32_t* tg);
+/* Marks passes of the plan forced by axhel_cuda_plan_set for (inverse, log2 N)
+ * to run with the prefetching pass kernel (bit i = pass i): a grid of
+ * resident CTAs walks the tiles, and each thread's asynchronous copies bring
+ * its next tile's operands into shared memory while it transforms the
+ * current one.  Same results bit for bit.  Used by the autotuner. */
+axhel_status_t axhel_cuda_plan_set_prefetch(int inverse, uint32_t log_degree, uint32_t mask);
+/* Reads the prefetch mask of the plan used for (inverse, log2 N, count limbs). */
+axhel_status_t axhel_cuda_plan_get_prefetch(int inverse, uint32_t log_degree, uint64_t count, uint32_t* mask);
 /* Loads an autotuner table (text, one plan per line); NULL = the table shipped
  * beside the library.  Returns the number of plans loaded via *loaded. */
 axhel_status_t axhel_cuda_plan_load(const char* path, uint32_t* loaded);
