@@ -6,7 +6,7 @@ depth LR in {3, 4, 5} and tile width TG on the GPU (CUDA events, median of
 several launches of the batched C-ABI call) and writes the fastest to
 ``axhel_b200/ntt_plans.txt``, which the library loads at first use:
 
-    <inverse> <logn> <limb-bucket> <npass> (<lg> <lr> <tg>)... [<prefetch mask>]
+    <inverse> <logn> <limb-bucket> <npass> (<lg> <lr> <tg>)...
 
 limb-bucket = floor(log2(limbs)).  For the uneven-batch engine (fixed
 1024-residue tiles) it times, per degree, every split of a job's stages into
@@ -63,15 +63,7 @@ def candidates(logn, inverse):
                             if (tga << (a - lra)) < 64 or (tgb << (b - lrb)) < 64:
                                 continue
                             out.append([row, col] if inverse else [col, row])
-    # the same splits with every pass on the prefetching kernel, where it exists
-    out += [[(lg, lr, tg, 1) for lg, lr, tg in plan] for plan in out if all(pf_eligible(*c) for c in plan)]
     return out
-
-
-def pf_eligible(lg, lr, tg):
-    """The prefetching pass kernel is compiled for 5..10 stages at register
-    depth 3 or 4, and needs three tiles of shared memory."""
-    return 5 <= lg <= 10 and lr in (3, 4) and 3 * tg * (1 << lg) * 8 <= 227 * 1024
 
 
 def time_plan(capi, torch, ntts, x, y, count, inverse, reps=5):
@@ -124,9 +116,8 @@ def tune(lognums, buckets, limbs_cap_bytes=1 << 30, verbose=True):
                 if best is None:
                     continue
                 ms, plan = best
-                flat = " ".join(f"{c[0]} {c[1]} {c[2]}" for c in plan)
-                mask = sum(1 << i for i, c in enumerate(plan) if len(c) > 3 and c[3])
-                lines.append(f"{int(inverse)} {logn} {bucket} {len(plan)} {flat}" + (f" {mask}" if mask else ""))
+                flat = " ".join(f"{lg} {lr} {tg}" for lg, lr, tg in plan)
+                lines.append(f"{int(inverse)} {logn} {bucket} {len(plan)} {flat}")
                 if verbose:
                     rate = count / (ms / 1e3)
                     print(f"inv={int(inverse)} logn={logn} limbs={count}: {plan} {ms:.4f} ms "
@@ -216,8 +207,7 @@ def main():
     merged = sorted(keep + lines, key=lambda l: (l.startswith("B"), l))
     with open(a.out, "w") as f:
         f.write("# NTT pass plans chosen by axhel_b200/autotune.py on one B200\n")
-        f.write("# inverse logn limb-bucket npass (lg lr tg)... [prefetch mask]  |  B logn contiguous-pass-stages "
-                "(batch engine)\n")
+        f.write("# inverse logn limb-bucket npass (lg lr tg)...  |  B logn contiguous-pass-stages (batch engine)\n")
         f.write("\n".join(merged) + "\n")
     print(f"wrote {a.out} ({len(lines)} lines tuned, {len(keep)} kept, {time.time() - t:.0f} s)")
 

@@ -134,8 +134,6 @@ def _declare(L):
     d("axhel_cuda_plan_set", st_t, C.c_int, u32, u32, vp, vp, vp)
     d("axhel_cuda_plan_get", st_t, C.c_int, u32, u64, vp, vp, vp, vp)
     d("axhel_cuda_plan_load", st_t, C.c_char_p, C.POINTER(u32))
-    d("axhel_cuda_plan_set_prefetch", st_t, C.c_int, u32, u32)
-    d("axhel_cuda_plan_get_prefetch", st_t, C.c_int, u32, u64, C.POINTER(u32))
     d("axhel_cuda_batch_split_set", st_t, u32, u32)
     d("axhel_cuda_batch_split_get", st_t, u32, C.POINTER(u32))
     d("axhel_cuda_is_device_pointer", C.c_int, vp)
@@ -487,27 +485,21 @@ def tensor_product(r0, r1, r2, c0, c1, d0, d1, n, count, moduli, factor=1, strea
 
 
 def plan_set(inverse, logn, passes):
-    """passes: list of (lg, lr, tg) or (lg, lr, tg, prefetch); [] restores the default."""
+    """passes: list of (lg, lr, tg); [] restores the default."""
     n = len(passes)
     lg = (u32 * 3)(*[p[0] for p in passes])
     lr = (u32 * 3)(*[p[1] for p in passes])
     tg = (u32 * 3)(*[p[2] for p in passes])
     check(lib().axhel_cuda_plan_set(int(inverse), logn, n, C.cast(lg, vp), C.cast(lr, vp), C.cast(tg, vp)),
           "plan_set")
-    mask = sum(1 << i for i, p in enumerate(passes) if len(p) > 3 and p[3])
-    if n and mask:
-        check(lib().axhel_cuda_plan_set_prefetch(int(inverse), logn, mask), "plan_set_prefetch")
 
 
 def plan_get(inverse, logn, count):
-    """[(lg, lr, tg, prefetch)] of the plan used for `count` limbs."""
     npass = u32()
     lg, lr, tg = (u32 * 3)(), (u32 * 3)(), (u32 * 3)()
     check(lib().axhel_cuda_plan_get(int(inverse), logn, count, C.byref(npass), C.cast(lg, vp), C.cast(lr, vp),
                                     C.cast(tg, vp)), "plan_get")
-    mask = u32()
-    check(lib().axhel_cuda_plan_get_prefetch(int(inverse), logn, count, C.byref(mask)), "plan_get_prefetch")
-    return [(lg[i], lr[i], tg[i], (mask.value >> i) & 1) for i in range(npass.value)]
+    return [(lg[i], lr[i], tg[i]) for i in range(npass.value)]
 
 
 def batch_split_set(logn, row_stages):

@@ -471,7 +471,6 @@ axhel_status_t chain(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* result,
     // thread (LR = 4) it needs 128 registers; 8 (LR = 3) keep it at 76 and
     // measured 3 % faster at N = 2^16, 768 limbs.
     PassCfg fc = inv.pass[inv.npass - 1];
-    fc.pf = 0;  // the fused pass has no prefetching form
     if (fc.lr > 3 && fc.lg >= 4 && ((uint64_t)fc.tg << (fc.lg - 3)) <= 512) fc.lr = 3;
     c.pass.src = src;
     c.pass.dst = result;
@@ -656,28 +655,6 @@ axhel_status_t axhel_cuda_plan_get(int inverse, uint32_t logn, uint64_t count, u
         lr[i] = (uint32_t)p.pass[i].lr;
         tg[i] = (uint32_t)p.pass[i].tg;
     }
-    return AXHEL_OK;
-}
-
-axhel_status_t axhel_cuda_plan_set_prefetch(int inverse, uint32_t logn, uint32_t mask)
-{
-    NttPlan p = plan_for(inverse != 0, logn, 1);
-    if (!plan_is_override(inverse != 0, logn)) return fail(AXHEL_ERR_INVALID, "set a plan for this degree first");
-    for (int i = 0; i < p.npass; ++i) p.pass[i].pf = (mask >> i) & 1u;
-    if (!plan_valid(p, logn, inverse != 0))
-        return fail(AXHEL_ERR_UNSUPPORTED, "no prefetching kernel for a pass of this plan");
-    plan_override(inverse != 0, logn, &p);
-    return AXHEL_OK;
-}
-
-axhel_status_t axhel_cuda_plan_get_prefetch(int inverse, uint32_t logn, uint64_t count, uint32_t* mask)
-{
-    if (!mask) return fail(AXHEL_ERR_INVALID, "null output");
-    if (logn < 1 || logn > 17) return fail(AXHEL_ERR_UNSUPPORTED, "log degree out of range");
-    const NttPlan p = plan_for(inverse != 0, logn, count);
-    uint32_t m = 0;
-    for (int i = 0; i < p.npass; ++i) m |= (p.pass[i].pf ? 1u : 0u) << i;
-    *mask = m;
     return AXHEL_OK;
 }
 

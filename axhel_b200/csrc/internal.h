@@ -63,7 +63,6 @@ struct ChainArgs {
 // One pass configuration chosen by the planner / autotuner.
 struct PassCfg {
     int lg, lr, tg;
-    int pf = 0;  // 1: the prefetching kernel (a resident grid walks the tiles, next tile's operands staged by cp.async)
 };
 struct NttPlan {
     int npass;
@@ -80,7 +79,6 @@ NttPlan plan_for(bool inverse, uint32_t logn, uint64_t limbs);
 bool plan_valid(const NttPlan& p, uint32_t logn, bool inverse);
 int plan_load(const char* path);
 void plan_override(bool inverse, uint32_t logn, const NttPlan* p);  // nullptr clears
-bool plan_is_override(bool inverse, uint32_t logn);
 // Uneven-batch engine: stages of the contiguous pass of an N = 2^logn job
 // (override > table > default); the strided pass takes the rest.
 bool batch_row_valid(uint32_t logn, int row);

@@ -1,9 +1,7 @@
 // Instantiations and launchers of the NTT pass kernels (ntt_kernels.cuh).
 #include <cuda_runtime.h>
 
-#include <map>
 #include <mutex>
-#include <tuple>
 
 #include "launch.h"
 #include "ntt_kernels.cuh"
@@ -18,17 +16,11 @@ using ChainFn = void (*)(const ChainArgs);
 constexpr int kMaxLG = 13;
 constexpr int kMaxLR = 5;
 
-// Prefetching pass kernels are compiled for the group sizes of the passes
-// of N >= 2^10 transforms (a pass of 5..10 stages) and register depths 3, 4.
-constexpr int kPfMinLG = 5, kPfMaxLG = 10, kPfMaxLR = 4;
-
 struct KernelTable {
     PassFn fwd[kMaxLG + 1][kMaxLR + 1] = {};
     PassFn inv[kMaxLG + 1][kMaxLR + 1] = {};
-    PassFn fwd_pf[kMaxLG + 1][kMaxLR + 1] = {};
-    PassFn inv_pf[kMaxLG + 1][kMaxLR + 1] = {};
     ChainFn chain[kMaxLG + 1][kMaxLR + 1] = {};
-    bool smem_set[5][kMaxLG + 1][kMaxLR + 1] = {};
+    bool smem_set[3][kMaxLG + 1][kMaxLR + 1] = {};
 };
 
 template <int LG, int LR>
@@ -38,10 +30,6 @@ void add_one(KernelTable& t)
         t.fwd[LG][LR] = ntt_pass_kernel<false, LG, LR>;
         t.inv[LG][LR] = ntt_pass_kernel<true, LG, LR>;
         t.chain[LG][LR] = ntt_chain_kernel<LG, LR>;
-        if constexpr (LG >= kPfMinLG && LG <= kPfMaxLG && LR >= 3 && LR <= kPfMaxLR) {
-            t.fwd_pf[LG][LR] = ntt_pass_pf_kernel<false, LG, LR>;
-            t.inv_pf[LG][LR] = ntt_pass_pf_kernel<true, LG, LR>;
-        }
     }
 }
 
@@ -77,9 +65,7 @@ KernelTable& table()
 
 std::mutex g_attr_mu;
 
-// Exchange space of a tile; the prefetching kernel adds two staging buffers
-// of the same size.
-size_t smem_bytes(const PassCfg& c) { return (size_t)c.tg * (size_t(1) << c.lg) * sizeof(uint64_t) * (c.pf ? 3 : 1); }
+size_t smem_bytes(const PassCfg& c) { return (size_t)c.tg * (size_t(1) << c.lg) * sizeof(uint64_t); }
 
 template <class Fn>
 cudaError_t ensure_smem(Fn fn, int kind, const PassCfg& c)
@@ -115,56 +101,24 @@ bool geometry_ok(const PassCfg& c, uint32_t logn, uint32_t lgS)
 bool pass_supported(const PassCfg& c)
 {
     if (c.lg < 1 || c.lg > kMaxLG || c.lr < 1 || c.lr > kMaxLR) return false;
-    if (c.pf) return table().fwd_pf[c.lg][c.lr] != nullptr && smem_bytes(c) <= 227 * 1024;
     return table().fwd[c.lg][c.lr] != nullptr;
 }
-
-namespace {
-
-// Resident CTAs of a prefetching pass kernel on the whole device (its grid),
-// per (direction, width, depth, tile groups), computed once.
-unsigned pf_grid(PassFn fn, bool inverse, const PassCfg& c, unsigned threads)
-{
-    static std::mutex mu;
-    static std::map<std::tuple<int, int, int, int, int>, unsigned> cache;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    const auto key = std::make_tuple(dev, inverse ? 1 : 0, c.lg, c.lr, c.tg);
-    std::lock_guard<std::mutex> lk(mu);
-    auto it = cache.find(key);
-    if (it != cache.end()) return it->second;
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void*>(fn), (int)threads,
-                                                  smem_bytes(c));
-    const unsigned g = (unsigned)(per_sm < 1 ? 1 : per_sm) * (unsigned)sm_count();
-    cache.emplace(key, g);
-    return g;
-}
-
-}  // namespace
 
 cudaError_t launch_ntt_pass(bool inverse, const PassCfg& c, const PassArgs& a, cudaStream_t s)
 {
     if (!pass_supported(c)) return cudaErrorInvalidValue;
     const uint32_t lgS = inverse ? a.s0 : (a.logn - a.s0 - c.lg);
     if (!geometry_ok(c, a.logn, lgS) || (uint32_t)c.tg != a.tg) return cudaErrorInvalidValue;
-    PassFn fn = c.pf ? (inverse ? table().inv_pf[c.lg][c.lr] : table().fwd_pf[c.lg][c.lr])
-                     : (inverse ? table().inv[c.lg][c.lr] : table().fwd[c.lg][c.lr]);
-    cudaError_t e = ensure_smem(fn, (inverse ? 1 : 0) + (c.pf ? 3 : 0), c);
+    PassFn fn = inverse ? table().inv[c.lg][c.lr] : table().fwd[c.lg][c.lr];
+    cudaError_t e = ensure_smem(fn, inverse ? 1 : 0, c);
     if (e != cudaSuccess) return e;
     const uint64_t tiles = a.count * ((1ull << (a.logn - c.lg)) / c.tg);
     if (tiles == 0) return cudaSuccess;
     if (tiles > 0x7fffffffull) return cudaErrorInvalidValue;
     const unsigned threads = (unsigned)c.tg << (c.lg - c.lr);
-    unsigned grid = (unsigned)tiles;
-    if (c.pf) {
-        const unsigned g = pf_grid(fn, inverse, c, threads);
-        if (g < grid) grid = g;
-    }
     count_launch();
-    ProfScope prof(s, "ntt_%s_pass lg=%d lr=%d tg=%d%s", inverse ? "inv" : "fwd", c.lg, c.lr, c.tg,
-                   c.pf ? " pf" : "");
-    fn<<<grid, threads, smem_bytes(c), s>>>(a);
+    ProfScope prof(s, "ntt_%s_pass lg=%d lr=%d tg=%d", inverse ? "inv" : "fwd", c.lg, c.lr, c.tg);
+    fn<<<(unsigned)tiles, threads, smem_bytes(c), s>>>(a);
     return cudaGetLastError();
 }
 

@@ -390,19 +390,31 @@ __device__ __forceinline__ void run_rounds(uint64_t (&v)[1 << LR], uint64_t* smg
 
 // ------------------------------------------------------------------ kernels
 
-// The stages of one tile on operands already in registers (round 0's
-// elements of thread (gi, k)), then the store of the last round.
-template <bool INV, int LG, int LR>
-__device__ __forceinline__ void pass_tile_regs(uint64_t (&v)[1 << LR], uint64_t* dst, const ModCtx* cx,
-                                               const Tile& t, uint32_t gi, uint32_t k, uint32_t logn, uint32_t s0,
-                                               uint32_t lgtg, uint32_t flags, bool vec_ok, uint64_t* sm)
+// One tile of a pass: stages [s0, s0 + LG) of limb `limb`.  `sm` holds
+// 2^lgtg groups of 2^LG + 1 words; all threads of the CTA take part.
+template <bool INV, int LG, int LR, bool CG>
+__device__ __forceinline__ void pass_tile(const uint64_t* src, uint64_t* dst, const ModCtx* cx, uint32_t logn,
+                                          uint32_t s0, uint32_t lgtg, uint64_t limb, uint64_t tile_in_limb,
+                                          uint32_t flags, uint64_t* sm)
 {
     constexpr int R = 1 << LR;
     constexpr int NR = num_rounds<LG, LR>();
+    constexpr int LO_FIRST = round_lo<INV, LG, LR, 0>();
     constexpr int LO_LAST = round_lo<INV, LG, LR, NR - 1>();
+    const uint32_t lgS = INV ? s0 : (logn - s0 - LG);
+    const Tile t = make_tile<LG>(lgS, lgtg, limb, tile_in_limb);
     const uint64_t q = cx->q, q2 = cx->q2;
     const uint64_t n = 1ull << logn;
+    const uint64_t* lsrc = src + (limb << logn);
+    uint64_t* ldst = dst + (limb << logn);
+    const bool vec_ok = ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0;
+
+    uint32_t gi, k;
+    thread_role<LG, LR>(t, gi, k);
     const uint64_t blk = tile_blk<LG>(t, gi);
+
+    uint64_t v[R];
+    load_global<LG, LR, LO_FIRST, CG>(v, lsrc, t, gi, round_base<LR>(k, LO_FIRST), vec_ok);
     if (flags & kPreCsub2q) {
 #pragma unroll
         for (int i = 0; i < R; ++i) v[i] = csub_lazy(v[i], q2);
@@ -413,79 +425,7 @@ __device__ __forceinline__ void pass_tile_regs(uint64_t (&v)[1 << LR], uint64_t*
 #pragma unroll
         for (int i = 0; i < R; ++i) v[i] = INV ? csub_lazy(v[i], q) : csub_lazy(csub_lazy(v[i], q2), q);
     }
-    store_global<LG, LR, LO_LAST>(v, dst + (t.limb << logn), t, gi, round_base<LR>(k, LO_LAST), vec_ok);
-}
-
-// One tile of a pass: stages [s0, s0 + LG) of limb `limb`.  `sm` holds
-// 2^lgtg groups of 2^LG words; all threads of the CTA take part.
-template <bool INV, int LG, int LR, bool CG>
-__device__ __forceinline__ void pass_tile(const uint64_t* src, uint64_t* dst, const ModCtx* cx, uint32_t logn,
-                                          uint32_t s0, uint32_t lgtg, uint64_t limb, uint64_t tile_in_limb,
-                                          uint32_t flags, uint64_t* sm)
-{
-    constexpr int R = 1 << LR;
-    constexpr int LO_FIRST = round_lo<INV, LG, LR, 0>();
-    const uint32_t lgS = INV ? s0 : (logn - s0 - LG);
-    const Tile t = make_tile<LG>(lgS, lgtg, limb, tile_in_limb);
-    const bool vec_ok = ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0;
-    uint32_t gi, k;
-    thread_role<LG, LR>(t, gi, k);
-    uint64_t v[R];
-    load_global<LG, LR, LO_FIRST, CG>(v, src + (limb << logn), t, gi, round_base<LR>(k, LO_FIRST), vec_ok);
-    pass_tile_regs<INV, LG, LR>(v, dst, cx, t, gi, k, logn, s0, lgtg, flags, vec_ok, sm);
-}
-
-// ------------------------------------------------- async staging of operands
-
-// Asynchronous global -> shared copies (cp.async): 8 bytes through L1, 16
-// bytes around it; each thread waits for its own copies only.
-__device__ __forceinline__ void cp_async8(uint64_t* sdst, const uint64_t* gsrc)
-{
-    const uint32_t sa = static_cast<uint32_t>(__cvta_generic_to_shared(sdst));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async16(ulonglong2* sdst, const ulonglong2* gsrc)
-{
-    const uint32_t sa = static_cast<uint32_t>(__cvta_generic_to_shared(sdst));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-// Waits until at most the latest committed group of this thread is in flight.
-__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-
-// Thread-private staging of round 0's R operands: pair i (registers 2i,
-// 2i+1) in the 16-byte slot st[i * nthr] -- lane-consecutive slots, so
-// reading them back is conflict-free.  Same global addresses as load_global.
-template <int LG, int LR, int LO>
-__device__ __forceinline__ void stage_global(ulonglong2* st, uint32_t nthr, const uint64_t* __restrict__ limb_src,
-                                             const Tile& t, uint32_t gi, uint32_t rb, bool vec_ok)
-{
-    constexpr int R = 1 << LR;
-    if (t.strided) {
-        const uint64_t* p = limb_src + t.base + gi + ((uint64_t)rb << t.lgS);
-#pragma unroll
-        for (int i = 0; i < R; ++i)
-            cp_async8(reinterpret_cast<uint64_t*>(st + (i >> 1) * nthr) + (i & 1), p + ((uint64_t)i << (LO + t.lgS)));
-    } else if (LO == 0 && vec_ok) {
-        const ulonglong2* p = reinterpret_cast<const ulonglong2*>(limb_src + t.base + ((uint64_t)gi << LG) + rb);
-#pragma unroll
-        for (int i = 0; i < R / 2; ++i) cp_async16(st + i * nthr, p + i);
-    } else {
-        const uint64_t* p = limb_src + t.base + ((uint64_t)gi << LG) + rb;
-#pragma unroll
-        for (int i = 0; i < R; ++i) cp_async8(reinterpret_cast<uint64_t*>(st + (i >> 1) * nthr) + (i & 1), p + (i << LO));
-    }
-}
-
-template <int LR>
-__device__ __forceinline__ void read_stage(uint64_t (&v)[1 << LR], const ulonglong2* st, uint32_t nthr)
-{
-#pragma unroll
-    for (int i = 0; i < (1 << LR) / 2; ++i) {
-        const ulonglong2 w = st[i * nthr];
-        v[2 * i] = w.x;
-        v[2 * i + 1] = w.y;
-    }
+    store_global<LG, LR, LO_LAST>(v, ldst, t, gi, round_base<LR>(k, LO_LAST), vec_ok);
 }
 
 template <bool INV, int LG, int LR>
@@ -571,55 +511,6 @@ __device__ __forceinline__ void chain_tile(const uint64_t* src, uint64_t* dst, c
         for (int i = 0; i < R; ++i) v[i] = csub_lazy(csub_lazy(v[i], q2), q);
     }
     store_global<LG, LR, LO_LAST>(v, ldst, t, gi, round_base<LR>(k, LO_LAST), vec_ok);
-}
-
-// A pass over all tiles with a grid of resident CTAs: each CTA walks its
-// tiles (blockIdx.x, + gridDim.x, ...) and, while it transforms one, its
-// threads' asynchronous copies bring the next tile's round-0 operands into
-// a private double-buffered staging area (after the TG groups of exchange
-// space), so the loads' latency hides behind a whole tile of butterflies.
-// The same tile functions as ntt_pass_kernel: the same results bit for bit.
-template <bool INV, int LG, int LR>
-__global__ void __launch_bounds__(max_threads(LR)) ntt_pass_pf_kernel(const __grid_constant__ PassArgs a)
-{
-    extern __shared__ uint64_t sm[];
-    constexpr int R = 1 << LR;
-    constexpr int LO_FIRST = round_lo<INV, LG, LR, 0>();
-    const uint32_t lgtg = __ffs(a.tg) - 1;
-    const uint32_t lg_tiles = a.logn - LG - lgtg;  // log2 tiles per limb
-    const uint64_t tiles = a.count << lg_tiles;
-    const uint32_t nthr = blockDim.x;
-    const uint32_t lgS = INV ? a.s0 : (a.logn - a.s0 - LG);
-    const bool vec_ok = ((reinterpret_cast<uintptr_t>(a.src) | reinterpret_cast<uintptr_t>(a.dst)) & 15) == 0;
-    ulonglong2* stage = reinterpret_cast<ulonglong2*>(sm + ((uint64_t)a.tg << LG)) + threadIdx.x;
-    const uint32_t half = (R / 2) * nthr;  // slots per staging buffer
-    uint64_t tile = blockIdx.x;
-    if (tile >= tiles) return;
-    Tile t = make_tile<LG>(lgS, lgtg, tile >> lg_tiles, tile & ((1ull << lg_tiles) - 1));
-    uint32_t gi, k;
-    thread_role<LG, LR>(t, gi, k);  // the same for every tile of the launch
-    const uint32_t rb0 = round_base<LR>(k, LO_FIRST);
-    stage_global<LG, LR, LO_FIRST>(stage, nthr, a.src + (t.limb << a.logn), t, gi, rb0, vec_ok);
-    cp_async_commit();
-    for (uint32_t it = 0;; ++it) {
-        const uint64_t next = tile + gridDim.x;
-        Tile tn = t;
-        if (next < tiles) {  // the next tile's operands into the other buffer, read one iteration ago
-            tn = make_tile<LG>(lgS, lgtg, next >> lg_tiles, next & ((1ull << lg_tiles) - 1));
-            stage_global<LG, LR, LO_FIRST>(stage + ((it + 1) & 1) * half, nthr, a.src + (tn.limb << a.logn), tn, gi,
-                                           rb0, vec_ok);
-        }
-        cp_async_commit();
-        cp_async_wait_prev();  // this tile's copies have landed
-        uint64_t v[R];
-        read_stage<LR>(v, stage + (it & 1) * half, nthr);
-        pass_tile_regs<INV, LG, LR>(v, a.dst, a.ctx[limb_mod(t.limb, a.nctx)], t, gi, k, a.logn, a.s0, lgtg, a.flags,
-                                    vec_ok, sm);
-        if (next >= tiles) break;
-        __syncthreads();  // the exchange space is rewritten by the next tile
-        tile = next;
-        t = tn;
-    }
 }
 
 // Kernel of the fused chain pass: one CTA per tile of chain_tile above; the

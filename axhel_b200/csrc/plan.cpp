@@ -4,9 +4,8 @@
 // Priority: an explicit override (axhel_cuda_plan_set) > the autotuner table
 // (loaded from ntt_plans.txt beside the library, or axhel_cuda_plan_load) >
 // the built-in default.  Table lines:
-//   <inverse 0|1> <logn> <limb-bucket> <npass> (<lg> <lr> <tg>){npass} [<prefetch mask>]
-// where limb-bucket = floor(log2(limbs)) clamped to [0, 15] and bit i of the
-// optional mask runs pass i with the prefetching kernel.  A lookup takes
+//   <inverse 0|1> <logn> <limb-bucket> <npass> (<lg> <lr> <tg>){npass}
+// where limb-bucket = floor(log2(limbs)) clamped to [0, 15].  A lookup takes
 // the nearest bucket at or below the requested one, else the nearest above.
 // Lines `B <logn> <row stages>` give the uneven-batch engine's split of an
 // N = 2^logn job into its strided and contiguous passes.
@@ -102,15 +101,13 @@ int load_table_locked(const char* path)
             }
             continue;
         }
-        int inv, logn, bucket, npass, v[10] = {0};
-        int got = std::sscanf(line, "%d %d %d %d %d %d %d %d %d %d %d %d %d %d", &inv, &logn, &bucket, &npass,
-                              &v[0], &v[1], &v[2], &v[3], &v[4], &v[5], &v[6], &v[7], &v[8], &v[9]);
+        int inv, logn, bucket, npass, v[9] = {0};
+        int got = std::sscanf(line, "%d %d %d %d %d %d %d %d %d %d %d %d %d", &inv, &logn, &bucket, &npass, &v[0],
+                              &v[1], &v[2], &v[3], &v[4], &v[5], &v[6], &v[7], &v[8]);
         if (got < 4 || npass < 1 || npass > 3 || got < 4 + 3 * npass) continue;
-        const int mask = got > 4 + 3 * npass ? v[3 * npass] : 0;
         NttPlan p{};
         p.npass = npass;
-        for (int i = 0; i < npass; ++i)
-            p.pass[i] = PassCfg{v[3 * i], v[3 * i + 1], v[3 * i + 2], (mask >> i) & 1};
+        for (int i = 0; i < npass; ++i) p.pass[i] = PassCfg{v[3 * i], v[3 * i + 1], v[3 * i + 2]};
         if (!plan_valid(p, (uint32_t)logn, inv != 0)) continue;
         g_table[std::make_tuple(inv ? 1 : 0, (uint32_t)logn, bucket)] = p;
         ++n;
@@ -149,7 +146,7 @@ bool plan_valid(const NttPlan& p, uint32_t logn, bool inverse)
         if ((uint64_t)c.tg > (1ull << (logn - c.lg))) return false;
         const uint32_t lgS = inverse ? s0 : logn - s0 - (uint32_t)c.lg;
         if (lgS > 0 && (uint64_t)c.tg > (1ull << lgS)) return false;
-        if ((size_t)c.tg * ((size_t(1) << c.lg) + 1) * 8 * (c.pf ? 3 : 1) > 227 * 1024) return false;
+        if ((size_t)c.tg * ((size_t(1) << c.lg) + 1) * 8 > 227 * 1024) return false;
         s0 += (uint32_t)c.lg;
     }
     return true;
@@ -170,12 +167,6 @@ NttPlan plan_for(bool inverse, uint32_t logn, uint64_t limbs)
         }
     }
     return default_plan(inverse, logn, limbs);
-}
-
-bool plan_is_override(bool inverse, uint32_t logn)
-{
-    std::lock_guard<std::mutex> lk(g_mu);
-    return g_override.count({inverse ? 1 : 0, logn}) != 0;
 }
 
 void plan_override(bool inverse, uint32_t logn, const NttPlan* p)

@@ -59,7 +59,7 @@ constexpr int kPending = -1, kRunning = -2;
 // stretches every such sleep by the thread's timer slack, 50 us by default,
 // which would land in each request's latency.
 void tighten_timer_slack() { prctl(PR_SET_TIMERSLACK, 1000UL, 0, 0, 0); }
-constexpr size_t kStagingBytes = 1 << 20;  // pinned descriptor staging per slot at creation
+constexpr size_t kStagingBytes = 1 << 20;  // descriptor buffers per slot at creation (pinned host, device)
 
 bool is_device(const void* p) { return p && axhel_cuda_is_device_pointer(p); }
 
@@ -87,6 +87,7 @@ struct Slot {
     int* err_host = nullptr;        // pinned word the kernel's error status is copied into
     unsigned char* host_img = nullptr;  // pinned staging of the batch descriptors
     size_t host_cap = 0;
+    unsigned char* dev_img = nullptr;   // the slot's device descriptor buffer (kStagingBytes, at creation)
     std::vector<unsigned char*> retired;  // outgrown staging, freed with the server
     bool busy = false;
 };
@@ -210,24 +211,27 @@ axhel_status_t axhel_server::launch(Slot& s, int slot_index, std::vector<Req*>& 
     std::string err;
     const bool per_phase = !(cfg.flags & AXHEL_SERVER_PERSISTENT);
     std::vector<axhel_impl::ClassLaunch> classes;
-    axhel_status_t rc = axhel_impl::batch_build(jobs.data(), jobs.size(), nullptr, img, &zo, &zb, &args, nullptr, &err,
-                                                per_phase ? &classes : nullptr);
-    if (rc) {
-        unstage(st, take, take.size());
-        return sfail(rc, err);
+    // The descriptors go to the slot's own device buffer, laid out for its
+    // address in one pass; the slot's previous batch has completed, and the
+    // copy is stream-ordered after it anyway.  A batch too large for it gets a
+    // buffer from the stream-ordered pool, returned after the batch: no
+    // cudaMalloc / cudaFree (which wait for the whole device) while other
+    // batches run.
+    void* desc = s.dev_img;
+    bool own_desc = false;
+    axhel_status_t rc = axhel_impl::batch_build(jobs.data(), jobs.size(), s.dev_img, img, &zo, &zb, &args, nullptr,
+                                                &err, per_phase ? &classes : nullptr);
+    if (rc == AXHEL_OK && img.size() > kStagingBytes) {
+        if (cudaMallocFromPoolAsync(&desc, img.size(), pool, st) != cudaSuccess) {
+            unstage(st, take, take.size());
+            return sfail(AXHEL_ERR_NOMEM, "batch descriptor buffer");
+        }
+        own_desc = true;
+        rc = axhel_impl::batch_build(jobs.data(), jobs.size(), static_cast<unsigned char*>(desc), img, &zo, &zb,
+                                     &args, nullptr, &err, per_phase ? &classes : nullptr);
     }
-    // Descriptors come from the stream-ordered pool and go back to it after
-    // the batch: no cudaMalloc / cudaFree (which wait for the whole device)
-    // while other batches run.
-    void* desc = nullptr;
-    if (cudaMallocFromPoolAsync(&desc, img.size(), pool, st) != cudaSuccess) {
-        unstage(st, take, take.size());
-        return sfail(AXHEL_ERR_NOMEM, "batch descriptor buffer");
-    }
-    rc = axhel_impl::batch_build(jobs.data(), jobs.size(), static_cast<unsigned char*>(desc), img, &zo, &zb,
-                                 &args, nullptr, &err, per_phase ? &classes : nullptr);
     if (rc) {
-        cudaFreeAsync(desc, st);
+        if (own_desc) cudaFreeAsync(desc, st);
         unstage(st, take, take.size());
         return sfail(rc, err);
     }
@@ -237,7 +241,7 @@ axhel_status_t axhel_server::launch(Slot& s, int slot_index, std::vector<Req*>& 
         unsigned char* grown = nullptr;
         const size_t cap = std::max<size_t>(img.size() * 2, s.host_cap * 2);
         if (cudaMallocHost(reinterpret_cast<void**>(&grown), cap) != cudaSuccess) {
-            cudaFreeAsync(desc, st);
+            if (own_desc) cudaFreeAsync(desc, st);
             unstage(st, take, take.size());
             return sfail(AXHEL_ERR_NOMEM, "pinned descriptor staging");
         }
@@ -269,7 +273,7 @@ axhel_status_t axhel_server::launch(Slot& s, int slot_index, std::vector<Req*>& 
         }
     }
     unstage(st, take, take.size());  // in stream order, after the copies back
-    cudaFreeAsync(desc, st);  // after the error word's copy, in stream order
+    if (own_desc) cudaFreeAsync(desc, st);  // after the error word's copy, in stream order
     if (e != cudaSuccess) return sfail(AXHEL_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
     f.reqs = order;
     f.slot = slot_index;
@@ -405,6 +409,8 @@ void axhel_server::completer()
 {
     cudaSetDevice(device);
     tighten_timer_slack();
+    std::vector<std::pair<Inflight*, cudaEvent_t>> heads;
+    std::vector<cudaError_t> state;
     std::unique_lock<std::mutex> lk(mu);
     for (;;) {
         cv_done.wait(lk, [&] { return !inflight.empty() || stop; });
@@ -412,17 +418,27 @@ void axhel_server::completer()
             if (stop) break;
             continue;
         }
-        // Poll every request of every batch in flight: batches of the two
-        // lanes finish out of launch order, and a request completes as soon
-        // as its own result has landed.
-        bool progress = false;
-        for (auto it = inflight.begin(); it != inflight.end();) {
-            Inflight& f = *it;
+        // Poll the oldest pending result of every batch in flight (batches of
+        // the two lanes finish out of launch order, and a request completes
+        // as soon as its own result has landed), querying the events without
+        // the lock so that the scheduler keeps admitting meanwhile.  Only this
+        // thread removes batches, and appending to the deque keeps references
+        // to its elements valid.
+        heads.clear();
+        for (Inflight& f : inflight) heads.emplace_back(&f, f.done.empty() ? nullptr : f.done.front());
+        lk.unlock();
+        state.assign(heads.size(), cudaErrorNotReady);
+        for (size_t i = 0; i < heads.size(); ++i)
+            if (heads[i].second) state[i] = cudaEventQuery(heads[i].second);
+        lk.lock();
+        bool progress = false, emptied = false;
+        for (size_t i = 0; i < heads.size(); ++i) {
+            cudaError_t e = state[i];
+            if (e == cudaErrorNotReady) continue;
+            Inflight& f = *heads[i].first;
             Slot& sl = slots[f.slot];
             while (!f.reqs.empty()) {
-                cudaEvent_t ev = f.done.empty() ? nullptr : f.done.front();
-                const cudaError_t e = ev ? cudaEventQuery(ev) : cudaErrorNotReady;
-                if (e == cudaErrorNotReady) break;
+                cudaEvent_t ev = f.done.front();
                 Req* q = f.reqs.front();
                 q->status = (e == cudaSuccess) ? *sl.err_host : AXHEL_ERR_CUDA;
                 q->t_done = Clock::now();
@@ -435,20 +451,24 @@ void axhel_server::completer()
                 f.done.erase(f.done.begin());
                 f.reqs.erase(f.reqs.begin());
                 progress = true;
+                if (f.reqs.empty()) break;
+                e = cudaEventQuery(f.done.front());  // the batch's next result, often landed too
+                if (e == cudaErrorNotReady) break;
             }
             if (f.reqs.empty()) {
                 for (cudaEvent_t ev : f.done) event_pool.push_back(ev);
+                f.done.clear();
                 sl.busy = false;
-                it = inflight.erase(it);
-            } else {
-                ++it;
+                emptied = true;
             }
         }
+        if (emptied)
+            for (auto it = inflight.begin(); it != inflight.end();) it = it->reqs.empty() ? inflight.erase(it) : it + 1;
         if (progress) {
             cv_wait.notify_all();
             cv_sched.notify_all();
         } else {
-            cv_done.wait_for(lk, std::chrono::microseconds(20));
+            cv_done.wait_for(lk, std::chrono::microseconds(10));
         }
     }
 }
@@ -498,6 +518,7 @@ axhel_status_t axhel_server_create(const axhel_server_config_t* cfg, axhel_serve
         // allocated now rather than on a slot's first batch
         if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&sl.host_img), kStagingBytes);
         if (e == cudaSuccess) sl.host_cap = kStagingBytes;
+        if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&sl.dev_img), kStagingBytes);
     }
     if (e == cudaSuccess && cfg->reserve_bytes) {
         // map the pool's memory now: growing it later takes tens of
@@ -514,6 +535,7 @@ axhel_status_t axhel_server_create(const axhel_server_config_t* cfg, axhel_serve
             axhel_impl::lanes_destroy(&sl.lanes);
             if (sl.err_host) cudaFreeHost(sl.err_host);
             if (sl.host_img) cudaFreeHost(sl.host_img);
+            if (sl.dev_img) cudaFree(sl.dev_img);
         }
         if (s->pool) cudaMemPoolDestroy(s->pool);
         return sfail(AXHEL_ERR_CUDA, std::string("server setup: ") + cudaGetErrorString(e));
@@ -662,6 +684,7 @@ axhel_status_t axhel_server_destroy(axhel_server_t s)
         axhel_impl::lanes_destroy(&sl.lanes);
         cudaFreeHost(sl.err_host);
         if (sl.host_img) cudaFreeHost(sl.host_img);
+        if (sl.dev_img) cudaFree(sl.dev_img);
         for (unsigned char* r : sl.retired) cudaFreeHost(r);
     }
     for (cudaEvent_t ev : s->event_pool) cudaEventDestroy(ev);

@@ -391,14 +391,6 @@ axhel_status_t axhel_cuda_plan_set(int inverse, uint32_t log_degree, uint32_t np
 /* Reads the plan used for (inverse, log2 N, count limbs); arrays of >= 3. */
 axhel_status_t axhel_cuda_plan_get(int inverse, uint32_t log_degree, uint64_t count, uint32_t* npass, uint32_t* lg,
                                    uint32_t* lr, uint32_t* tg);
-/* Marks passes of the plan forced by axhel_cuda_plan_set for (inverse, log2 N)
- * to run with the prefetching pass kernel (bit i = pass i): a grid of
- * resident CTAs walks the tiles, and each thread's asynchronous copies bring
- * its next tile's operands into shared memory while it transforms the
- * current one.  Same results bit for bit.  Used by the autotuner. */
-axhel_status_t axhel_cuda_plan_set_prefetch(int inverse, uint32_t log_degree, uint32_t mask);
-/* Reads the prefetch mask of the plan used for (inverse, log2 N, count limbs). */
-axhel_status_t axhel_cuda_plan_get_prefetch(int inverse, uint32_t log_degree, uint64_t count, uint32_t* mask);
 /* Loads an autotuner table (text, one plan per line); NULL = the table shipped
  * beside the library.  Returns the number of plans loaded via *loaded. */
 axhel_status_t axhel_cuda_plan_load(const char* path, uint32_t* loaded);

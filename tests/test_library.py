@@ -76,7 +76,7 @@ def test_default_plans_are_valid():
             for count in (1, 24, 768):
                 plan = capi.plan_get(inverse, logn, count)
                 assert sum(p[0] for p in plan) == logn
-                for lg, lr, tg, pf in plan:
+                for lg, lr, tg in plan:
                     assert 1 <= lr <= lg and tg >= 1 and (tg & (tg - 1)) == 0
                     assert (tg << (lg - lr)) <= (256 if lr >= 5 else 512)
                 if inverse:
@@ -90,22 +90,16 @@ def test_plan_override_and_table(tmp_path):
     from axhel_b200 import capi
 
     capi.plan_set(False, 16, [(8, 4, 16), (8, 4, 4)])
-    assert capi.plan_get(False, 16, 768) == [(8, 4, 16, 0), (8, 4, 4, 0)]
-    capi.plan_set(False, 16, [(8, 3, 8, 1), (8, 4, 4)])  # first pass on the prefetching kernel
-    assert capi.plan_get(False, 16, 768) == [(8, 3, 8, 1), (8, 4, 4, 0)]
-    with pytest.raises(capi.AxhelError):
-        capi.plan_set(False, 16, [(8, 5, 16, 1), (8, 4, 4)])  # no prefetching kernel at depth 5
+    assert capi.plan_get(False, 16, 768) == [(8, 4, 16), (8, 4, 4)]
     with pytest.raises(capi.AxhelError):
         capi.plan_set(False, 16, [(8, 4, 16), (7, 4, 4)])  # stages do not sum to 16
     with pytest.raises(capi.AxhelError):
         capi.plan_set(False, 16, [(8, 3, 64), (8, 4, 4)])  # 64 x 32 threads > 512
     capi.plan_set(False, 16, [])
     t = tmp_path / "plans.txt"
-    t.write_text("# inverse logn bucket npass lg lr tg ... [prefetch mask]\n0 15 3 2 8 4 8 7 4 16\n"
-                 "0 15 3 2 8 4 8 9 4 1\n1 15 3 2 7 4 16 8 3 8 2\n")
-    assert capi.plan_load(str(t)) == 2  # the second line does not sum to 15
-    assert capi.plan_get(False, 15, 8) == [(8, 4, 8, 0), (7, 4, 16, 0)]
-    assert capi.plan_get(True, 15, 8) == [(7, 4, 16, 0), (8, 3, 8, 1)]
+    t.write_text("# inverse logn bucket npass lg lr tg ...\n0 15 3 2 8 4 8 7 4 16\n0 15 3 2 8 4 8 9 4 1\n")
+    assert capi.plan_load(str(t)) == 1  # the second line does not sum to 15
+    assert capi.plan_get(False, 15, 8) == [(8, 4, 8), (7, 4, 16)]
 
 
 def test_params_primes_match_reference_generator(oracle):

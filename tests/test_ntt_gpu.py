@@ -221,8 +221,6 @@ def plan_candidates(logn, inverse):
                     col = (a, lr, min(tga, 1 << b))
                     row = (b, lr, min(tgb, 1 << a))
                     out.append([row, col] if inverse else [col, row])
-                    if lr <= 4 and 5 <= a <= 10 and 5 <= b <= 10:  # the prefetching kernel on both passes
-                        out.append([(*c, 1) for c in ([row, col] if inverse else [col, row])])
     return out
 
 
