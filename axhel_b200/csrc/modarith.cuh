@@ -60,29 +60,25 @@ __device__ __forceinline__ uint64_t mul_hi64(uint64_t a, uint64_t b)
     return r;
 }
 
-// (v * w + e * nq) mod 2^64; nq = 2^64 - q turns the Shoup subtraction
-// v*w - e*q into one accumulation chain.  The two low-word products are
-// 32x32->64 multiply-adds with a 64-bit accumulator (v0*w0 + e0*n0), the four
-// cross products only feed the high word (32-bit multiply-adds): measured
-// 2.6 % more butterflies/s on the register-only probe than low/high halves
-// with a carry chain (9.36 vs 9.12 x 10^11).
+// (v * w + e * nq) mod 2^64 with 32-bit multiply-adds; nq = 2^64 - q turns
+// the Shoup subtraction v*w - e*q into one accumulation chain.
 __device__ __forceinline__ uint64_t mul_lo_acc(uint64_t v, uint64_t w, uint64_t e, uint64_t nq)
 {
     uint64_t r;
     asm("{\n\t"
         ".reg .u32 v0, v1, w0, w1, e0, e1, n0, n1, r0, r1;\n\t"
-        ".reg .u64 t;\n\t"
         "mov.b64 {v0, v1}, %1;\n\t"
         "mov.b64 {w0, w1}, %2;\n\t"
         "mov.b64 {e0, e1}, %3;\n\t"
         "mov.b64 {n0, n1}, %4;\n\t"
-        "mul.wide.u32 t, v0, w0;\n\t"
-        "mad.wide.u32 t, e0, n0, t;\n\t"
-        "mov.b64 {r0, r1}, t;\n\t"
+        "mul.lo.u32 r0, v0, w0;\n\t"
+        "mul.hi.u32 r1, v0, w0;\n\t"
         "mad.lo.u32 r1, v0, w1, r1;\n\t"
         "mad.lo.u32 r1, v1, w0, r1;\n\t"
         "mad.lo.u32 r1, e0, n1, r1;\n\t"
         "mad.lo.u32 r1, e1, n0, r1;\n\t"
+        "mad.lo.cc.u32 r0, e0, n0, r0;\n\t"
+        "madc.hi.u32 r1, e0, n0, r1;\n\t"
         "mov.b64 %0, {r0, r1};\n\t"
         "}"
         : "=l"(r)

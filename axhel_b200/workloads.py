@@ -401,7 +401,11 @@ def serving(loads=(0.5, 0.7, 0.9), seconds=4.0, budget=60 << 30, inflight=4, see
     out = {"workload": "INTT->MulMod/FMAMod->NTT requests, N in 2^13..2^17, L in 2..40, Poisson arrivals",
            "operands": "device-resident" if device else "host pinned, staged per request",
            "launch": "persistent" if persistent else "per-phase class launches", "max_batch_words": max_batch_words,
-           "small_request_words": small_words, "policy": policy_name(flags, aging_us),
+           "small_request_words": small_words,
+           "policy": policy_name(flags, aging_us) + (
+               f"; two lanes split at {small_words} residues, the {'large' if flags & capi.SERVER_LARGE_FIRST else 'small'}"
+               " one at high stream priority" if small_words else "") + (
+               f"; {max_batch_requests} request(s) per batch" if max_batch_requests < 8 else ""),
            "batch_size_ratio": batch_size_ratio, "max_batch_requests_cfg": max_batch_requests,
            "capacity_jobs_per_s": cap, "isolated_median_ms": statistics.median(iso), "loads": results,
            "batches": st["batches"], "max_batch_requests": st["max_batch_requests"],
@@ -421,7 +425,7 @@ def policy_name(flags, aging_us=0):
         parts.append(f"smallest-first admission (aging {aging_us} us)")
     if flags & capi.SERVER_LARGE_FIRST:
         parts.append("large-request lane at high priority")
-    return ", ".join(parts) or "arrival-order admission, equal-priority streams"
+    return ", ".join(parts) or "arrival-order admission"
 
 
 def plain_sequential(rp, limit=16):

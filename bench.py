@@ -40,10 +40,16 @@ SEED = 0x415848454C
 METRIC = "batched NTT+INTT limb-transforms/s at N=2^16"
 UNIT = "limb-transforms/s"
 HBM_FALLBACK = 6650.0
-# serving loop configuration of the bench line (batches in flight, AXHEL_SERVER_* flags, aging bound)
-SERVE_INFLIGHT = 4
-SERVE_FLAGS = 0
-SERVE_AGING_US = 0
+# Serving-loop configuration of the bench line per operand placement.  Host-
+# staged requests: batches of whatever is queued, 4 in flight (their copies
+# share the PCIe link).  Device-resident requests: one request per batch, and
+# two lanes split at the 75th percentile of the request sizes, the small lane
+# at high stream priority (so small requests are not queued behind a large
+# one's kernels).
+SERVE_CONFIG = {
+    "host_staged": dict(inflight=4, max_batch_requests=256),
+    "device_resident": dict(inflight=4, max_batch_requests=1, small_pct=75),
+}
 
 
 def peaks():
@@ -373,13 +379,15 @@ def run_ours(args):
         serve = {}
         for mode, device in (("host_staged", False), ("device_resident", True)):
             r = workloads.serving(loads=(0.5, 0.7, 0.9), seconds=3.0, n_templates=24, device=device, plain=True,
-                                  small_words=0, inflight=SERVE_INFLIGHT, flags=SERVE_FLAGS, aging_us=SERVE_AGING_US)
+                                  **SERVE_CONFIG[mode])
             m = {"capacity_jobs_per_s": r["capacity_jobs_per_s"], "isolated_median_ms": r["isolated_median_ms"],
-                 "plain_sequential_jobs_per_s": r["plain_sequential_jobs_per_s"], "policy": r["policy"]}
+                 "plain_sequential_jobs_per_s": r["plain_sequential_jobs_per_s"], "policy": r["policy"],
+                 "config": {k: r[k] for k in ("max_inflight", "max_batch_requests_cfg", "small_request_words")}}
             for l in r["loads"]:
                 m[f"load_{int(round(100 * l['load']))}"] = {
                     k: l[k] for k in ("jobs_per_s", "p50_ms", "p99_ms", "isolated_p99_ms", "p99_over_isolated_p99",
-                                      "p50_slowdown", "p99_slowdown", "requests")}
+                                      "p50_slowdown", "p99_slowdown", "p99_queue_ms", "p99_large_ms", "p99_rest_ms",
+                                      "requests")}
             l70 = m["load_70"]
             m.update({"jobs_per_s_at_70pct": l70["jobs_per_s"], "p50_ms": l70["p50_ms"], "p99_ms": l70["p99_ms"],
                       "isolated_p99_ms": l70["isolated_p99_ms"], "p99_over_isolated_p99": l70["p99_over_isolated_p99"],
