@@ -42,13 +42,11 @@ UNIT = "limb-transforms/s"
 HBM_FALLBACK = 6650.0
 # Serving-loop configuration of the bench line per operand placement.  Host-
 # staged requests: batches of whatever is queued, 4 in flight (their copies
-# share the PCIe link).  Device-resident requests: one request per batch, and
-# two lanes split at the 75th percentile of the request sizes, the small lane
-# at high stream priority (so small requests are not queued behind a large
-# one's kernels).
+# share the PCIe link).  Device-resident requests: one request per batch, 8 in
+# flight, so a small request never waits inside a large one's batch.
 SERVE_CONFIG = {
     "host_staged": dict(inflight=4, max_batch_requests=256),
-    "device_resident": dict(inflight=4, max_batch_requests=1, small_pct=75),
+    "device_resident": dict(inflight=8, max_batch_requests=1),
 }
 
 
