@@ -221,101 +221,70 @@ __device__ __forceinline__ uint32_t find_entry(const BatchArgs& a, uint64_t tile
     return lo;
 }
 
-// Whether the phase p-1 tiles that tile `tile` of entry `e` needs are all
-// published (acquire at device scope when they are).
-__device__ __forceinline__ bool dep_ready(const BatchArgs& a, uint64_t tile, const BatchEntry& e)
-{
-    if (e.phase == 0) return true;
-    const BatchJob& j = a.jobs[e.job];
-    const uint64_t limb = (tile - e.tile_begin) >> (j.logn - kBatchTileLog);
-    cuda::atomic_ref<unsigned int, cuda::thread_scope_device> dep(
-        a.done[j.done_off + (uint64_t)(e.phase - 1) * j.count + limb]);
-    return dep.load(cuda::memory_order_acquire) >= j.tiles_per_limb[e.phase - 1] + j.wait_extra;
-}
-
-// Bounded wait for tile `tile`'s dependencies (2 s of %globaltimer and 2^24
-// polls); false (and the error word set) when it gave up.
-__device__ __forceinline__ bool dep_wait(const BatchArgs& a, uint64_t tile, const BatchEntry& e)
-{
-    const uint64_t t0 = global_ns();
-    uint32_t polls = 0;
-    while (!dep_ready(a, tile, e)) {
-        if (++polls > (1u << 24) || global_ns() - t0 > a.wait_ns) {
-            atomicExch(a.error, AXHEL_ERR_TIMEOUT);
-            return false;
-        }
-        __nanosleep(100);
-    }
-    return true;
-}
-
-// The persistent kernel: CTAs take tiles from one counter in phase-major
-// order.  While the CTA transforms tile i, one thread of its second warp
-// claims tile i+1, finds its entry and checks its dependencies once without
-// waiting; so the next tile is known, and usually ready, when tile i ends,
-// and only a tile whose dependencies were still running when it was claimed
-// waits (after tile i is published: the two may be the same limb's
-// consecutive phases).
 __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks) batch_kernel(const __grid_constant__ BatchArgs a)
 {
     __shared__ uint64_t sm[kBatchTileWords + 128];
     __shared__ unsigned long long s_tile[2];
-    __shared__ uint32_t s_entry[2];
-    __shared__ int s_ready[2];
+    __shared__ uint32_t s_entry;
     __shared__ int s_abort;
-    if (threadIdx.x == kBatchPublisher) {
-        const unsigned long long t = atomicAdd(a.next_tile, 1ull);
-        s_tile[0] = t;
-        s_entry[0] = 0;
+    uint32_t entry = 0;  // thread 0: entry of the CTA's latest tile
+    if (threadIdx.x == 0) {
+        s_tile[0] = atomicAdd(a.next_tile, 1ull);
         s_abort = 0;
-        if (t < a.total_tiles) {
-            const uint32_t e = find_entry(a, t, 0);
-            s_entry[0] = e;
-            if (!dep_wait(a, t, a.entries[e])) s_abort = 1;
-        }
     }
     __syncthreads();
     for (uint32_t it = 0;; ++it) {
-        const uint32_t b = it & 1;
-        const uint64_t tile = s_tile[b];
-        if (tile >= a.total_tiles || s_abort) break;
-        const uint32_t cur = s_entry[b];
-        if (threadIdx.x == kBatchPublisher) {  // the next tile, looked up while this one runs
-            const unsigned long long nxt = atomicAdd(a.next_tile, 1ull);
-            s_tile[b ^ 1] = nxt;
-            if (nxt < a.total_tiles) {
-                const uint32_t e = find_entry(a, nxt, cur);
-                s_entry[b ^ 1] = e;
-                s_ready[b ^ 1] = dep_ready(a, nxt, a.entries[e]);
+        const uint64_t tile = s_tile[it & 1];
+        if (tile >= a.total_tiles) break;
+        unsigned long long nxt = 0;  // the next tile, claimed now, announced after this one
+        if (threadIdx.x == 0) {
+            nxt = atomicAdd(a.next_tile, 1ull);
+            entry = find_entry(a, tile, entry);
+            s_entry = entry;
+            const BatchEntry e = a.entries[entry];
+            if (e.phase > 0) {
+                const BatchJob& j = a.jobs[e.job];
+                const uint64_t limb = (tile - e.tile_begin) >> (j.logn - kBatchTileLog);
+                cuda::atomic_ref<unsigned int, cuda::thread_scope_device> dep(
+                    a.done[j.done_off + (uint64_t)(e.phase - 1) * j.count + limb]);
+                const unsigned need = j.tiles_per_limb[e.phase - 1] + j.wait_extra;
+                const uint64_t t0 = global_ns();
+                uint32_t polls = 0;
+                while (dep.load(cuda::memory_order_acquire) < need) {
+                    // bounded in wall time and in polls
+                    if (++polls > (1u << 24) || global_ns() - t0 > a.wait_ns) {
+                        atomicExch(a.error, AXHEL_ERR_TIMEOUT);
+                        s_abort = 1;
+                        break;
+                    }
+                    __nanosleep(100);
+                }
             }
         }
-        {
-            const ClassEntry& c = a.tile_args[cur];
-            const uint64_t lt = tile - c.tile0;
-            const uint32_t lgt = c.logn - kBatchTileLog;  // tiles per limb: a power of two
-            run_any_tile(c, lt >> lgt, lt & ((1ull << lgt) - 1), sm);
-        }
-        __syncthreads();  // the tile's stores, and the next tile's lookup, are done
-        // Read by every thread before anything writes these slots again: the
-        // next iteration's lookup writes the other slot.
-        const bool wait_next = s_tile[b ^ 1] < a.total_tiles && !s_ready[b ^ 1];
+        __syncthreads();
+        if (s_abort) break;
+        const uint32_t cur = s_entry;
+        const ClassEntry& c = a.tile_args[cur];
+        const uint64_t lt = tile - c.tile0;
+        const uint32_t lgt = c.logn - kBatchTileLog;  // tiles per limb: a power of two
+        const uint64_t limb = lt >> lgt;
+        run_any_tile(c, limb, lt & ((1ull << lgt) - 1), sm);
+        if (threadIdx.x == 0) s_tile[(it + 1) & 1] = nxt;
+        __syncthreads();
+        // The finished tile is published by a thread of another warp than the
+        // claiming thread 0, so its release fence overlaps the next tile's
+        // lookup and dependency check instead of preceding them.
         if (threadIdx.x == kBatchPublisher) {
-            // publish this tile: release at device scope, cumulative over the
-            // stores the barrier ordered before it (its indices re-read from
-            // shared memory rather than kept live across the tile)
-            const BatchEntry e = a.entries[s_entry[b]];
+            const BatchEntry e = a.entries[cur];
             const BatchJob& j = a.jobs[e.job];
             if (e.phase + 1 < j.nphase) {
-                const uint64_t limb = (s_tile[b] - e.tile_begin) >> (j.logn - kBatchTileLog);
+                // release at device scope, cumulative over the stores the
+                // barrier ordered before it
                 cuda::atomic_ref<unsigned int, cuda::thread_scope_device> done(
                     a.done[j.done_off + (uint64_t)e.phase * j.count + limb]);
                 done.fetch_add(1u, cuda::memory_order_release);
             }
-            // then, if the next tile was not ready when claimed, wait for it
-            if (wait_next && !dep_wait(a, s_tile[b ^ 1], a.entries[s_entry[b ^ 1]])) s_abort = 1;
         }
-        // the wait's acquire (and an abort) ordered before the next tile's reads
-        if (wait_next) __syncthreads();
     }
 }
 

@@ -215,9 +215,8 @@ __device__ __forceinline__ void load_global(uint64_t (&v)[1 << LR], const uint64
     constexpr int R = 1 << LR;
     if (t.strided) {
         const uint64_t* p = limb_src + t.base + gi + ((uint64_t)rb << t.lgS);
-        const uint64_t step = 1ull << (LO + t.lgS);
 #pragma unroll
-        for (int i = 0; i < R; ++i, p += step) v[i] = ld64<CG>(p);
+        for (int i = 0; i < R; ++i) v[i] = ld64<CG>(p + ((uint64_t)i << (LO + t.lgS)));
     } else if (LO == 0 && vec_ok) {
         const ulonglong2* p = reinterpret_cast<const ulonglong2*>(limb_src + t.base + ((uint64_t)gi << LG) + rb);
 #pragma unroll
@@ -240,9 +239,8 @@ __device__ __forceinline__ void store_global(const uint64_t (&v)[1 << LR], uint6
     constexpr int R = 1 << LR;
     if (t.strided) {
         uint64_t* p = limb_dst + t.base + gi + ((uint64_t)rb << t.lgS);
-        const uint64_t step = 1ull << (LO + t.lgS);
 #pragma unroll
-        for (int i = 0; i < R; ++i, p += step) *p = v[i];
+        for (int i = 0; i < R; ++i) p[(uint64_t)i << (LO + t.lgS)] = v[i];
     } else if (LO == 0 && vec_ok) {
         ulonglong2* p = reinterpret_cast<ulonglong2*>(limb_dst + t.base + ((uint64_t)gi << LG) + rb);
 #pragma unroll
@@ -273,9 +271,7 @@ __device__ __forceinline__ void fwd_stages(uint64_t (&v)[1 << LR], uint32_t rbas
         const uint32_t t = s0 + (LG - 1 - b);
         // the twiddles of this stage are consecutive: rbase's register bits
         // are zero, so (rbase | j << (b+1)) >> (b+1) = (rbase >> (b+1)) + j
-        // a table index is below N <= 2^17: 32-bit index arithmetic
-        const ulonglong2* tws =
-            tw + ((1u << t) + ((uint32_t)blk << (LG - 1 - b)) + (rbase >> (b + 1)));
+        const ulonglong2* tws = tw + (1ull << t) + (blk << (LG - 1 - b)) + (rbase >> (b + 1));
 #pragma unroll
         for (int j = 0; j < (R >> (rb + 1)); ++j) {
             const ulonglong2 w = __ldg(tws + j);
@@ -313,9 +309,7 @@ __device__ __forceinline__ void inv_stages(uint64_t (&v)[1 << LR], uint32_t rbas
                 }
         } else {
             const uint32_t s = s0 + b;
-            const uint32_t n32 = (uint32_t)n;  // a table index is below N <= 2^17
-            const ulonglong2* tws =
-                tw + (1u + n32 - (n32 >> s) + ((uint32_t)blk << (LG - b - 1)) + (rbase >> (b + 1)));
+            const ulonglong2* tws = tw + (1 + n - (n >> s)) + (blk << (LG - b - 1)) + (rbase >> (b + 1));
 #pragma unroll
             for (int j = 0; j < (R >> (rb + 1)); ++j) {
                 const ulonglong2 w = __ldg(tws + j);
