@@ -112,6 +112,7 @@ def _declare(L):
     d("axhel_cuda_ntt_create", st_t, u64, u64, u64, C.POINTER(vp))
     d("axhel_cuda_ntt_create_many", st_t, u64, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64), C.POINTER(vp))
     d("axhel_cuda_ntt_create_external", st_t, u64, u64, vp, vp, vp, C.POINTER(vp))
+    d("axhel_cuda_ntt_refresh_external", st_t, vp, vp, vp, vp, vp)
     d("axhel_cuda_ntt_retain", st_t, vp)
     d("axhel_cuda_ntt_release", st_t, vp)
     d("axhel_cuda_ntt_degree", u64, vp)

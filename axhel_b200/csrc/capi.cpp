@@ -329,7 +329,29 @@ axhel_status_t axhel_cuda_ntt_create_external(uint64_t degree, uint64_t modulus,
     c->logn = logn;
     cudaGetDevice(&c->device);
     if ((st = upload(c.get(), fwd, inv, ninv))) return st;
+    c->external = true;
     *out = c.release();
+    return AXHEL_OK;
+}
+
+axhel_status_t axhel_cuda_ntt_refresh_external(axhel_ntt_t h, const uint64_t* fwd, const uint64_t* inv,
+                                               const uint64_t* ninv, void* stream)
+{
+    if (!h || !h->external) return fail(AXHEL_ERR_INVALID, "not a handle made from external tables");
+    if (inv && !ninv) return fail(AXHEL_ERR_INVALID, "the inverse table needs its N^-1 pair");
+    const size_t tab = h->n * 16;
+    unsigned char* base = static_cast<unsigned char*>(h->mem);
+    cudaStream_t s = S(stream);
+    // Pageable sources: each copy has read its source when the call returns.
+    cudaError_t e = cudaSuccess;
+    if (fwd) e = cudaMemcpyAsync(base + kHeader, fwd, tab, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && inv) {
+        const ModCtx hd = make_header(h, base, inv[2 * (h->n - 1)], ninv[0], ninv[1]);
+        e = cudaMemcpyAsync(base + kHeader + tab, inv, tab, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(base, &hd, sizeof hd, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the header copy reads this stack frame
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "refresh external tables");
     return AXHEL_OK;
 }
 

@@ -242,6 +242,12 @@ public:
     uint64_t degree{0};
     uint64_t modulus{0};
     axhel_ntt_t handle{nullptr};
+    // External tables, borrowed as the reference does (ntt.hpp:34-37): read
+    // again before every transform, so a caller that updates them in place
+    // gets the results the reference would give.
+    const NTTMultiplyOperand* ext_fwd{nullptr};
+    const NTTMultiplyOperand* ext_inv{nullptr};
+    NTTMultiplyOperand ext_ninv{0, 0};
     ~Impl() { axhel_cuda_ntt_release(handle); }
 };
 
@@ -263,6 +269,9 @@ NTT::NTT(uint64_t degree, uint64_t modulus, const NTTMultiplyOperand* root_power
     check(axhel_cuda_ntt_create_external(degree, modulus, reinterpret_cast<const uint64_t*>(root_powers),
                                          reinterpret_cast<const uint64_t*>(inv_root_powers), ninv, &impl_->handle),
           "NTT external tables");
+    impl_->ext_fwd = root_powers;
+    impl_->ext_inv = inv_root_powers;
+    impl_->ext_ninv = inv_degree_modulo;
 }
 
 NTT::~NTT() = default;
@@ -275,6 +284,10 @@ void NTT::ComputeForward(uint64_t* result, const uint64_t* operand, uint64_t inp
                          uint64_t output_mod_factor) const
 {
     const uint64_t n = impl_->degree;
+    if (impl_->ext_fwd)
+        check(axhel_cuda_ntt_refresh_external(impl_->handle, reinterpret_cast<const uint64_t*>(impl_->ext_fwd),
+                                              nullptr, nullptr, stream()),
+              "NTT external tables");
     Output out(result, n);
     const uint64_t* a = input(operand, n, 0);
     AXHEL_LOG("NTT::ComputeForward -> CUDA, N=" << n << ", out_factor=" << output_mod_factor
@@ -288,6 +301,12 @@ void NTT::ComputeInverse(uint64_t* result, const uint64_t* operand, uint64_t inp
                          uint64_t output_mod_factor) const
 {
     const uint64_t n = impl_->degree;
+    if (impl_->ext_inv) {
+        const uint64_t ninv[2] = {impl_->ext_ninv.operand, impl_->ext_ninv.quotient};
+        check(axhel_cuda_ntt_refresh_external(impl_->handle, nullptr,
+                                              reinterpret_cast<const uint64_t*>(impl_->ext_inv), ninv, stream()),
+              "NTT external tables");
+    }
     Output out(result, n);
     const uint64_t* a = input(operand, n, 0);
     AXHEL_LOG("NTT::ComputeInverse -> CUDA, N=" << n << ", out_factor=" << output_mod_factor

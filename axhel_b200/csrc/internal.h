@@ -99,5 +99,6 @@ struct axhel_ntt_ctx {
     bool cached = false;
     void* mem = nullptr;                       // device allocation
     bool shared_mem = false;                   // mem lies in one block with the contexts created beside it
+    bool external = false;                     // tables supplied by the caller (axhel_cuda_ntt_create_external)
     const axhel_impl::ModCtx* dctx = nullptr;  // device address of the ModCtx header
 };

@@ -75,10 +75,22 @@ axhel_status_t axhel_cuda_ntt_create_many(uint64_t count, const uint64_t* degree
  * (ntt.hpp:37, ntt.cpp:124-133).  root_powers / inv_root_powers are HOST
  * arrays of `degree` {operand, quotient} pairs (2*degree words, the layout of
  * NTTMultiplyOperand, ntt.hpp:14-18); inv_degree is one pair.  They are
- * copied to the device at creation (the reference borrows them instead). */
+ * copied to the device at creation; axhel_cuda_ntt_refresh_external re-reads
+ * them (the reference borrows them and reads them at every transform). */
 axhel_status_t axhel_cuda_ntt_create_external(uint64_t degree, uint64_t modulus, const uint64_t* root_powers,
                                               const uint64_t* inv_root_powers, const uint64_t* inv_degree,
                                               axhel_ntt_t* out);
+
+/* The reference's external-table NTT borrows the caller's tables and reads
+ * them at every transform (ntt.hpp:34-37); this re-reads them from the
+ * caller's HOST arrays into the handle's device copy, in stream order, so
+ * that a transform issued after it sees the tables as they are now.  Either
+ * table may be NULL (not re-read); the inverse table needs inv_degree.  Only
+ * for handles made by axhel_cuda_ntt_create_external.  The C++ drop-in calls
+ * it before every transform of such an NTT. */
+axhel_status_t axhel_cuda_ntt_refresh_external(axhel_ntt_t ntt, const uint64_t* root_powers,
+                                               const uint64_t* inv_root_powers, const uint64_t* inv_degree,
+                                               void* stream);
 
 axhel_status_t axhel_cuda_ntt_retain(axhel_ntt_t ntt);
 axhel_status_t axhel_cuda_ntt_release(axhel_ntt_t ntt);

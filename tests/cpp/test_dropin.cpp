@@ -9,6 +9,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -86,6 +87,35 @@ static void test_external_tables()
     CHECK(y == x, "external tables inverse via copy");
     NTT moved = std::move(copy);
     CHECK(moved.Degree() == 8 && copy.Degree() == 0, "move leaves an empty object");
+}
+
+// The external tables are borrowed (ntt.hpp:34-37): tables the caller
+// rewrites in place after construction are the ones the next transform uses.
+static void test_external_tables_borrowed()
+{
+    const uint64_t n = 4096, q = orc_find_ntt_prime(n, 50);
+    const uint64_t psi1 = orc_find_primitive_root(n, q);
+    const uint64_t psi2 = orc_pow_mod(psi1, 3, q);  // another primitive 2n-th root (3 is odd)
+    Tables t1 = tables(n, q, psi1), t2 = tables(n, q, psi2);
+    std::vector<uint64_t> fwd = t1.fwd, inv = t1.inv;  // the caller's tables
+    NTT ntt(n, q, reinterpret_cast<const NTTMultiplyOperand*>(fwd.data()),
+            reinterpret_cast<const NTTMultiplyOperand*>(inv.data()), NTTMultiplyOperand{t1.ninv[0], t1.ninv[1]});
+    uint64_t st[313];
+    orc_mt64_seed(st, kSeed ^ 0xB0220);
+    const Vec x = rand_vec(st, n, q);
+    Vec y(n), e(n);
+    ntt.ComputeForward(y.data(), x.data(), 1, 4);
+    orc_ntt_compute_forward(e.data(), x.data(), n, q, t1.fwd.data(), 1, 4);
+    CHECK(y == e, "borrowed tables: forward with the first tables");
+    std::copy(t2.fwd.begin(), t2.fwd.end(), fwd.begin());  // rewritten in place, same storage
+    std::copy(t2.inv.begin(), t2.inv.end(), inv.begin());
+    ntt.ComputeForward(y.data(), x.data(), 1, 4);
+    orc_ntt_compute_forward(e.data(), x.data(), n, q, t2.fwd.data(), 1, 4);
+    CHECK(y == e, "borrowed tables: forward sees the rewritten table");
+    const Vec z = rand_vec(st, n, 2 * q);
+    ntt.ComputeInverse(y.data(), z.data(), 2, 2);
+    orc_ntt_compute_inverse(e.data(), z.data(), n, q, t2.inv.data(), t1.ninv, 2, 2);
+    CHECK(y == e, "borrowed tables: inverse sees the rewritten table");
 }
 
 static void test_transforms_vs_oracle()
@@ -305,6 +335,7 @@ int main()
 {
     test_known_vector();
     test_external_tables();
+    test_external_tables_borrowed();
     test_transforms_vs_oracle();
     test_lazy_round_trip_seal_style();
     test_eltwise_host_pointers();
