@@ -306,3 +306,30 @@ def test_polymul_matches_schoolbook(cuda, oracle, n):
         cuda.mul(ptr(prod), ptr(A), ptr(B), n, q, 1)  # dyadic product in the NTT domain
         t.inverse(ptr(prod), ptr(prod), 1, 1)
         np.testing.assert_array_equal(host(prod, n), want, err_msg=f"normalized, q bits {bits}")
+
+
+def test_refresh_external_tables(cuda, oracle):
+    """axhel_cuda_ntt_refresh_external: a handle made from external tables
+    re-reads them (the reference borrows them); other handles refuse."""
+    import ctypes as C
+
+    n = 1024
+    q, psi1 = ntt_params(oracle, n, 50)
+    psi2 = oracle.pow_mod(psi1, 3, q)
+    f1, i1, n1 = oracle.tables(n, q, psi1)
+    f2, i2, n2 = oracle.tables(n, q, psi2)
+    t = cuda.NTT(n, q, tables=(f1, i1, n1))
+    x = oracle.random_vector(oracle.rng(SEED ^ 0xEF), n, q)
+    d, o = dev(x), dev_empty(n)
+    t.forward(ptr(o), ptr(d), 1, 4)
+    np.testing.assert_array_equal(host(o, n), oracle.forward(x, q, f1, 1, 4))
+    P = lambda a: a.ctypes.data_as(C.c_void_p)
+    L = cuda.lib()
+    assert L.axhel_cuda_ntt_refresh_external(t.h, P(f2), P(i2), P(n2), None) == 0
+    t.forward(ptr(o), ptr(d), 1, 4)
+    np.testing.assert_array_equal(host(o, n), oracle.forward(x, q, f2, 1, 4))
+    t.inverse(ptr(o), ptr(d), 1, 1)
+    np.testing.assert_array_equal(host(o, n), oracle.inverse(x, q, i2, n2, 1, 1))
+    auto = cuda.NTT(n, q, psi1)
+    assert L.axhel_cuda_ntt_refresh_external(auto.h, P(f2), None, None, None) == 1  # not an external-table handle
+    assert L.axhel_cuda_ntt_refresh_external(t.h, None, P(i2), None, None) == 1  # inverse table without N^-1
