@@ -264,33 +264,6 @@ __device__ __forceinline__ void fwd_stages(uint64_t (&v)[1 << LR], uint32_t rbas
     constexpr int hi = LG - RD * LR;
     constexpr int nb = hi < LR ? hi : LR;
     constexpr int lo = round_lo<false, LG, LR, RD>();
-    if constexpr (LR == 3 && nb == 3) {
-        // all seven twiddles of the round loaded before its first stage
-        ulonglong2 w[7];
-#pragma unroll
-        for (int bb = 0, k = 0; bb < nb; ++bb) {
-            const int b = hi - 1 - bb;
-            const int rb = b - lo;
-            const uint32_t t = s0 + (LG - 1 - b);
-            const ulonglong2* tws = tw + (1ull << t) + (blk << (LG - 1 - b)) + (rbase >> (b + 1));
-#pragma unroll
-            for (int j = 0; j < (R >> (rb + 1)); ++j) w[k++] = __ldg(tws + j);
-        }
-#pragma unroll
-        for (int bb = 0, k = 0; bb < nb; ++bb) {
-            const int b = hi - 1 - bb;
-            const int rb = b - lo;
-#pragma unroll
-            for (int j = 0; j < (R >> (rb + 1)); ++j, ++k) {
-#pragma unroll
-                for (int l = 0; l < (1 << rb); ++l) {
-                    const int i0 = (j << (rb + 1)) | l;
-                    fwd_butterfly(v[i0], v[i0 | (1 << rb)], w[k].x, w[k].y, q, q2);
-                }
-            }
-        }
-        return;
-    }
 #pragma unroll
     for (int bb = 0; bb < nb; ++bb) {
         const int b = hi - 1 - bb;  // in-group bit = butterfly span
@@ -322,33 +295,6 @@ __device__ __forceinline__ void inv_stages(uint64_t (&v)[1 << LR], uint32_t rbas
     constexpr int b0 = RD * LR;
     constexpr int b1 = (b0 + LR < LG) ? b0 + LR : LG;
     constexpr int lo = round_lo<true, LG, LR, RD>();
-    if constexpr (LR == 3 && b1 - b0 == 3) {
-        if (!(last && b1 == LG)) {
-            // all seven twiddles of the round loaded before its first stage
-            ulonglong2 w[7];
-#pragma unroll
-            for (int b = b0, k = 0; b < b1; ++b) {
-                const int rb = b - lo;
-                const uint32_t s = s0 + b;
-                const ulonglong2* tws = tw + (1 + n - (n >> s)) + (blk << (LG - b - 1)) + (rbase >> (b + 1));
-#pragma unroll
-                for (int j = 0; j < (R >> (rb + 1)); ++j) w[k++] = __ldg(tws + j);
-            }
-#pragma unroll
-            for (int b = b0, k = 0; b < b1; ++b) {
-                const int rb = b - lo;
-#pragma unroll
-                for (int j = 0; j < (R >> (rb + 1)); ++j, ++k) {
-#pragma unroll
-                    for (int l = 0; l < (1 << rb); ++l) {
-                        const int i0 = (j << (rb + 1)) | l;
-                        inv_butterfly(v[i0], v[i0 | (1 << rb)], w[k].x, w[k].y, q, q2);
-                    }
-                }
-            }
-            return;
-        }
-    }
 #pragma unroll
     for (int b = b0; b < b1; ++b) {
         const int rb = b - lo;
