@@ -72,11 +72,13 @@ SPECS = [(13, 4, 4, 3), (14, 2, 2, 4), (15, 6, 6, 3), (16, 3, 3, 4), (17, 2, 2, 
 
 
 @pytest.mark.parametrize("cfg", [{}, {"persistent": True}, {"small_request_words": 1 << 16}, {"flags": 2},
-                                 {"flags": 4, "aging_us": 500}],
-                         ids=["per-phase", "persistent", "two-lanes", "arrival-priority", "smallest-first"])
+                                 {"flags": 4, "aging_us": 500}, {"max_batch_requests": 1, "max_inflight": 8},
+                                 {"small_request_words": 1 << 16, "flags": 8}, {"batch_size_ratio": 2}],
+                         ids=["per-phase", "persistent", "two-lanes", "arrival-priority", "smallest-first",
+                              "one-per-batch", "large-first", "size-ratio"])
 def test_same_bits_alone_and_in_a_mix(cuda, oracle, cfg):
     reqs = make_requests(cuda, oracle, 5, SPECS)
-    srv = cuda.Server(budget_bytes=8 << 30, max_inflight=2, max_batch_requests=64, **cfg)
+    srv = cuda.Server(**{"budget_bytes": 8 << 30, "max_inflight": 2, "max_batch_requests": 64, **cfg})
     alone = []
     for k, r in enumerate(reqs):  # one at a time on an idle server
         rid, bufs = submit(srv, r, on_device=k % 2 == 0)
@@ -99,7 +101,10 @@ def test_same_bits_alone_and_in_a_mix(cuda, oracle, cfg):
         assert st == 0
         sizes.append(info.batch_size)
         np.testing.assert_array_equal(result(bufs, reqs[k]["x"].size, on_dev), alone[k], err_msg=f"mix {k}")
-    assert max(sizes) > 1, "concurrent requests were batched together"
+    if cfg.get("max_batch_requests", 64) > 1:
+        assert max(sizes) > 1, "concurrent requests were batched together"
+    else:
+        assert max(sizes) == 1
     stats = srv.stats()
     assert stats["completed"] == 3 * len(reqs) and stats["p99_ms"] >= stats["p50_ms"] > 0
     srv.close()
