@@ -87,8 +87,8 @@ def build_tools(force=False):
         exe = os.path.join(PKG, f[:-4])
         if not force and os.path.exists(exe) and os.path.getmtime(exe) >= _newest([src, LIB] + headers()):
             continue
-        cmd = ["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), src, "-L" + PKG, "-laxhel",
-               "-Wl,-rpath,$ORIGIN", "-lpthread", "-o", exe]
+        cmd = ["g++", "-O2", "-std=c++17", "-DAXHEL_RNS", "-I" + os.path.join(ROOT, "include"), src, "-L" + PKG,
+               "-laxhel", "-Wl,-rpath,$ORIGIN", "-lpthread", "-o", exe]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"tool build failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")

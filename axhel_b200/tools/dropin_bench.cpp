@@ -18,7 +18,16 @@
 //
 // One JSON line per (operation, degree): mean microseconds per call seen by
 // each thread, and calls per second over all threads.
+//
+// Built against this library (AXHEL_RNS defined), it also times a whole RNS
+// polynomial of L = 24 limbs -- the loop SEAL runs over a ciphertext's moduli
+// (ntt_negacyclic_harvey over coeff_modulus) -- as 24 per-limb
+// ComputeForward calls and as one ComputeForwardRNS call
+// (axhel/ntt/ntt-rns.hpp, not in the reference API), both on host memory.
 #include <axhel/axhel.hpp>
+#ifdef AXHEL_RNS
+#include <axhel/ntt/ntt-rns.hpp>
+#endif
 
 #include <atomic>
 #include <chrono>
@@ -165,6 +174,24 @@ int main(int argc, char** argv)
                  ax::EltwiseAddMod(s.c.data(), s.c.data(), scalar, n, c.q);
                  ntt.ComputeInverse(s.c.data(), s.c.data(), 1, 1);
              }));
+#ifdef AXHEL_RNS
+        // an RNS polynomial of 24 limbs (the same modulus stands in for the
+        // 24 distinct ones of a ciphertext: the cost does not depend on it)
+        constexpr size_t L = 24;
+        const std::vector<ax::NTT> limbs(L, ntt);
+        auto setup_poly = [&](int t) {
+            Bufs s;
+            s.x.resize(n * L);
+            fill(s.x, 2 * c.q, 41 + t);
+            return s;
+        };
+        emit("rns24_per_limb_calls", c, threads, run(threads, seconds, setup_poly, [&](Bufs& s) {
+                 for (size_t i = 0; i < L; ++i) limbs[i].ComputeForward(s.x.data() + i * n, s.x.data() + i * n, 4, 4);
+             }));
+        emit("rns24_one_call", c, threads, run(threads, seconds, setup_poly, [&](Bufs& s) {
+                 ax::ComputeForwardRNS(limbs.data(), L, s.x.data(), s.x.data(), L, 4, 4);
+             }));
+#endif
     }
     return 0;
 }

@@ -526,10 +526,16 @@ def dropin_host(with_reference, threads_list=(1, 8), seconds=0.2):
         for (op, logn), d in sorted(ours.items(), key=lambda kv: (kv[0][0], kv[0][1])):
             row = {"op": op, "logn": logn, "threads": threads, "us": d["us_per_call"],
                    "calls_per_s": d["calls_per_s"]}
-            if (op, logn) in ref:
+            if op.startswith("rns24") and ("forward_4_4", logn) in ref:
+                # the reference's cost of the same polynomial: 24 per-limb calls
+                r = ref[("forward_4_4", logn)]
+                row.update({"reference_us": 24 * r["us_per_call"],
+                            "speedup": 24 * r["us_per_call"] / d["us_per_call"]})
+            elif (op, logn) in ref:
                 r = ref[(op, logn)]
                 row.update({"reference_us": r["us_per_call"], "reference_calls_per_s": r["calls_per_s"],
                             "speedup": r["us_per_call"] / d["us_per_call"]})
+            if "speedup" in row:
                 key = f"{op}@{threads}t"
                 if row["speedup"] > 1 and key not in crossover:
                     crossover[key] = 1 << logn
