@@ -124,6 +124,7 @@ def _declare(L):
     d("axhel_cuda_ntt_inverse_batch", st_t, C.POINTER(vp), u64, vp, vp, u64, u64, u64, vp)
     d("axhel_cuda_ntt_chain_mul_batch", st_t, C.POINTER(vp), u64, vp, vp, vp, u64, u64, u64, vp)
     d("axhel_cuda_ntt_chain_fma_batch", st_t, C.POINTER(vp), u64, vp, vp, vp, vp, u64, u64, u64, vp)
+    d("axhel_cuda_ntt_product_batch", st_t, C.POINTER(vp), u64, vp, vp, vp, u64, u64, u64, vp)
     d("axhel_cuda_eltwise_add_vv", st_t, vp, vp, vp, u64, u64, vp)
     d("axhel_cuda_eltwise_add_vs", st_t, vp, vp, u64, u64, u64, vp)
     d("axhel_cuda_eltwise_sub_vv", st_t, vp, vp, vp, u64, u64, vp)
@@ -449,6 +450,13 @@ def inverse_batch(ntts, dst, src, count, in_f=1, out_f=1, stream=0):
 def chain_mul_batch(ntts, dst, src, multiplicand, count, in_f=2, out_f=1, stream=0):
     check(lib().axhel_cuda_ntt_chain_mul_batch(_handles(ntts), len(ntts), dst, src, multiplicand, count, in_f, out_f,
                                                stream), "ntt_chain_mul_batch")
+
+
+def product_batch(ntts, dst, src, multiplicand, count, in_f=4, out_f=1, stream=0):
+    """Fused NTT -> MulMod(., multiplicand, 4) -> INTT over a batch."""
+    hs = _handles(ntts)
+    check(lib().axhel_cuda_ntt_product_batch(hs, len(ntts), dst, src, multiplicand, count, in_f, out_f, stream),
+          "ntt_product_batch")
 
 
 def chain_fma_batch(ntts, dst, src, scalars, addend, count, in_f=2, out_f=1, stream=0):

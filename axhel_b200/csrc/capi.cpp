@@ -523,9 +523,82 @@ axhel_status_t chain(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* result,
     return AXHEL_OK;
 }
 
+// NTT -> MulMod -> INTT over a batch: the forward's passes up to its last
+// (contiguous) one, that pass fused with the dyadic product and the
+// inverse's first pass, then the inverse's remaining passes.  The forward
+// runs the inverse plan's passes in reverse order, so its last pass is the
+// inverse's first (the same groups).
+axhel_status_t product(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* result, const uint64_t* operand,
+                       const uint64_t* vec, uint64_t count, uint64_t out_f, void* stream)
+{
+    ChainArgs c{};
+    uint64_t n;
+    axhel_status_t st = collect(ntts, n_ntts, c.pass, &n);
+    if (st) return st;
+    if (count == 0) return AXHEL_OK;
+    if (!result || !operand || !vec) return fail(AXHEL_ERR_INVALID, "null data pointer");
+    if (vec == result) return fail(AXHEL_ERR_INVALID, "the multiplicand must not be the result buffer");
+    c.pass.count = count;
+    const uint32_t logn = c.pass.logn;
+    const NttPlan inv = plan_for(true, logn, count);
+    cudaStream_t s = S(stream);
+    // forward passes before the fused one: the inverse plan's passes npass-1 .. 1
+    uint32_t f0 = 0;
+    const uint64_t* src = operand;
+    for (int i = inv.npass - 1; i >= 1; --i) {
+        PassArgs a = c.pass;
+        a.src = src;
+        a.dst = result;
+        a.s0 = f0;
+        a.tg = (uint32_t)inv.pass[i].tg;
+        a.flags = 0;
+        cudaError_t e = launch_ntt_pass(false, inv.pass[i], a, s);
+        if (e != cudaSuccess) return cuda_fail(e, "product forward pass");
+        f0 += (uint32_t)inv.pass[i].lg;
+        src = result;
+    }
+    // fused: forward last pass -> MulMod -> inverse first pass (register depth 3:
+    // the pass holds both transforms' rounds and the multiplicand)
+    PassCfg fc = inv.pass[0];
+    if (fc.lr > 3 && fc.lg >= 4 && ((uint64_t)fc.tg << (fc.lg - 3)) <= 512) fc.lr = 3;
+    if (fc.lr > 3) return fail(AXHEL_ERR_UNSUPPORTED, "no fused product pass for this plan");
+    c.pass.src = src;
+    c.pass.dst = result;
+    c.pass.s0 = 0;
+    c.pass.tg = (uint32_t)fc.tg;
+    c.pass.flags = inv.npass == 1 ? ((uint32_t)kLastPass | (out_f != 2 ? (uint32_t)kPostNorm : 0u)) : 0u;
+    c.operand = vec;
+    c.op = kChainMul;
+    c.op_factor = 4;
+    cudaError_t e = launch_product_pass(fc, c, s);
+    if (e != cudaSuccess) return cuda_fail(e, "product fused pass");
+    // the inverse's remaining passes
+    uint32_t i0 = (uint32_t)fc.lg;
+    for (int i = 1; i < inv.npass; ++i) {
+        PassArgs a = c.pass;
+        a.src = result;
+        a.dst = result;
+        a.s0 = i0;
+        a.tg = (uint32_t)inv.pass[i].tg;
+        a.flags = (i == inv.npass - 1) ? ((uint32_t)kLastPass | (out_f != 2 ? (uint32_t)kPostNorm : 0u)) : 0u;
+        e = launch_ntt_pass(true, inv.pass[i], a, s);
+        if (e != cudaSuccess) return cuda_fail(e, "product inverse pass");
+        i0 += (uint32_t)inv.pass[i].lg;
+    }
+    return AXHEL_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+axhel_status_t axhel_cuda_ntt_product_batch(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* result,
+                                            const uint64_t* operand, const uint64_t* multiplicand, uint64_t count,
+                                            uint64_t input_mod_factor, uint64_t output_mod_factor, void* stream)
+{
+    (void)input_mod_factor;  // the forward accepts [0, 4q) whatever the factor (ntt.cpp:173-186)
+    return product(ntts, n_ntts, result, operand, multiplicand, count, output_mod_factor, stream);
+}
 
 axhel_status_t axhel_cuda_ntt_forward(axhel_ntt_t h, uint64_t* r, const uint64_t* x, uint64_t in_f, uint64_t out_f,
                                       void* stream)

@@ -72,6 +72,9 @@ struct NttPlan {
 // Kernel launchers (ntt.cu / eltwise.cu).  All return cudaError_t of launch.
 cudaError_t launch_ntt_pass(bool inverse, const PassCfg& cfg, const PassArgs& a, cudaStream_t s);
 cudaError_t launch_chain_pass(const PassCfg& inv_cfg, const ChainArgs& a, cudaStream_t s);
+// The fused row pass of an NTT -> MulMod -> INTT product (contiguous groups;
+// register depth at most 3).
+cudaError_t launch_product_pass(const PassCfg& cfg, const ChainArgs& a, cudaStream_t s);
 bool pass_supported(const PassCfg& cfg);
 
 // Planner (plan.cpp): default plan for (dir, logN, limbs); autotuned table if loaded.

@@ -20,7 +20,8 @@ struct KernelTable {
     PassFn fwd[kMaxLG + 1][kMaxLR + 1] = {};
     PassFn inv[kMaxLG + 1][kMaxLR + 1] = {};
     ChainFn chain[kMaxLG + 1][kMaxLR + 1] = {};
-    bool smem_set[3][kMaxLG + 1][kMaxLR + 1] = {};
+    ChainFn product[kMaxLG + 1][kMaxLR + 1] = {};
+    bool smem_set[4][kMaxLG + 1][kMaxLR + 1] = {};
 };
 
 template <int LG, int LR>
@@ -30,6 +31,7 @@ void add_one(KernelTable& t)
         t.fwd[LG][LR] = ntt_pass_kernel<false, LG, LR>;
         t.inv[LG][LR] = ntt_pass_kernel<true, LG, LR>;
         t.chain[LG][LR] = ntt_chain_kernel<LG, LR>;
+        if constexpr (LR <= 3) t.product[LG][LR] = ntt_product_kernel<LG, LR>;
     }
 }
 
@@ -118,6 +120,24 @@ cudaError_t launch_ntt_pass(bool inverse, const PassCfg& c, const PassArgs& a, c
     const unsigned threads = (unsigned)c.tg << (c.lg - c.lr);
     count_launch();
     ProfScope prof(s, "ntt_%s_pass lg=%d lr=%d tg=%d", inverse ? "inv" : "fwd", c.lg, c.lr, c.tg);
+    fn<<<(unsigned)tiles, threads, smem_bytes(c), s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_product_pass(const PassCfg& c, const ChainArgs& a, cudaStream_t s)
+{
+    if (!pass_supported(c) || c.lr > 3) return cudaErrorInvalidValue;
+    if (!geometry_ok(c, a.pass.logn, 0) || (uint32_t)c.tg != a.pass.tg) return cudaErrorInvalidValue;
+    ChainFn fn = table().product[c.lg][c.lr];
+    if (!fn) return cudaErrorInvalidValue;
+    cudaError_t e = ensure_smem(fn, 3, c);
+    if (e != cudaSuccess) return e;
+    const uint64_t tiles = a.pass.count * ((1ull << (a.pass.logn - c.lg)) / c.tg);
+    if (tiles == 0) return cudaSuccess;
+    if (tiles > 0x7fffffffull) return cudaErrorInvalidValue;
+    const unsigned threads = (unsigned)c.tg << (c.lg - c.lr);
+    count_launch();
+    ProfScope prof(s, "ntt_product_pass lg=%d lr=%d tg=%d", c.lg, c.lr, c.tg);
     fn<<<(unsigned)tiles, threads, smem_bytes(c), s>>>(a);
     return cudaGetLastError();
 }

@@ -513,6 +513,72 @@ __device__ __forceinline__ void chain_tile(const uint64_t* src, uint64_t* dst, c
     store_global<LG, LR, LO_LAST>(v, ldst, t, gi, round_base<LR>(k, LO_LAST), vec_ok);
 }
 
+// Fused row pass of an NTT -> MulMod -> INTT product (the polynomial product
+// in evaluation form, SEAL's multiply_plain): the forward's last pass (stages
+// logn-LG .. logn-1) and the inverse's first pass (stages 0 .. LG-1) act on
+// the same contiguous groups of 2^LG words, and the forward's last round
+// holds the same register bits as the inverse's first round (the low LR
+// bits), so the dyadic product runs in registers between them.  The product
+// is EltwiseMulModNative<4> (axhel/eltwise/eltwise-mul-mod.cpp:18-63) of the
+// forward's lazy output and the multiplicand, both in [0, 4q).  With LG ==
+// logn (one pass each way) the tile also holds the inverse's N^-1 stage.
+template <int LG, int LR>
+__device__ __forceinline__ void product_tile(const uint64_t* src, uint64_t* dst, const uint64_t* operand,
+                                             const ModCtx* cx, uint32_t logn, uint32_t lgtg, uint64_t limb,
+                                             uint64_t tile_in_limb, uint32_t flags, uint64_t* sm)
+{
+    constexpr int R = 1 << LR;
+    constexpr int NR = num_rounds<LG, LR>();
+    constexpr int LO_FIRST = round_lo<false, LG, LR, 0>();
+    constexpr int LO_MID = round_lo<false, LG, LR, NR - 1>();
+    constexpr int LO_LAST = round_lo<true, LG, LR, NR - 1>();
+    static_assert(LO_MID == round_lo<true, LG, LR, 0>(), "forward last round and inverse first round differ");
+    const Tile t = make_tile<LG>(0, lgtg, limb, tile_in_limb);
+    const uint64_t q = cx->q, q2 = cx->q2;
+    const uint64_t n = 1ull << logn;
+    const bool vec_ok = ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst) |
+                          reinterpret_cast<uintptr_t>(operand)) & 15) == 0;
+    uint32_t gi, k;
+    thread_role<LG, LR>(t, gi, k);
+    const uint64_t blk = tile_blk<LG>(t, gi);
+    uint64_t* smg = sm + (gi << LG);
+    const uint32_t hmask = group_mask<LG, LR>(t.strided, lgtg, gi);
+    const uint32_t lsh = lane_shift(t.strided, lgtg);
+
+    uint64_t v[R];
+    load_global<LG, LR, LO_FIRST, false>(v, src + (limb << logn), t, gi, round_base<LR>(k, LO_FIRST), vec_ok);
+    run_rounds<false, LG, LR>(v, smg, k, hmask, lsh, blk, logn - LG, n, cx, q, q2, false);
+    {
+        uint64_t m[R];
+        load_global<LG, LR, LO_MID, false>(m, operand + (limb << logn), t, gi, round_base<LR>(k, LO_MID), vec_ok);
+        const uint64_t mu = cx->mu;
+        const uint32_t shift = cx->shift;
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+            v[i] = barrett_mul(reduce_input<4>(v[i], q), reduce_input<4>(m[i], q), q, mu, shift);
+    }
+    run_rounds<true, LG, LR>(v, smg, k, hmask, lsh, blk, 0, n, cx, q, q2, (flags & kLastPass) != 0);
+    if (flags & kPostNorm) {
+#pragma unroll
+        for (int i = 0; i < R; ++i) v[i] = csub_lazy(v[i], q);
+    }
+    store_global<LG, LR, LO_LAST>(v, dst + (limb << logn), t, gi, round_base<LR>(k, LO_LAST), vec_ok);
+}
+
+// Kernel of the fused product pass: one CTA per tile of product_tile above.
+template <int LG, int LR>
+__global__ void __launch_bounds__(max_threads(LR)) ntt_product_kernel(const __grid_constant__ ChainArgs c)
+{
+    extern __shared__ uint64_t sm[];
+    const PassArgs& a = c.pass;
+    const uint32_t lgtg = __ffs(a.tg) - 1;
+    const uint32_t lg_tiles = a.logn - LG - lgtg;
+    const uint64_t tile = blockIdx.x;
+    const uint64_t limb = tile >> lg_tiles;
+    product_tile<LG, LR>(a.src, a.dst, c.operand, a.ctx[limb_mod(limb, a.nctx)], a.logn, lgtg, limb,
+                         tile & ((1ull << lg_tiles) - 1), a.flags, sm);
+}
+
 // Kernel of the fused chain pass: one CTA per tile of chain_tile above; the
 // modulus context and the FMA scalar follow the limb.
 template <int LG, int LR>

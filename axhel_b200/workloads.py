@@ -2,6 +2,7 @@
 
     python -m axhel_b200.workloads tensor   # fused tensor-product chain vs per-limb calls
     python -m axhel_b200.workloads uneven   # 512 uneven polynomials in one launch vs per-limb calls
+    python -m axhel_b200.workloads product  # fused NTT -> MulMod -> INTT vs three batched calls
     python -m axhel_b200.workloads serve    # Poisson arrivals at 50/70/90 % of capacity
     python -m axhel_b200.workloads eltwise  # streaming eltwise kernels, GB/s at 2^24 elements
     python -m axhel_b200.workloads case F   # a small case of kernel family F, for a profiler
@@ -141,6 +142,55 @@ def tensor_chain(pairs=64, L=16, logn=15, reps=5, seed=3, keep=False):
     if keep:
         out["results"] = (r0, r1, r2)
     return out
+
+
+# ------------------------------------------------------------------ product
+
+def product_chain(logn=16, limbs=24, polys=32, reps=10, seed=5):
+    """The polynomial product in evaluation form over the headline's shape
+    (24 primes of 50-59 bits, 32 polynomials): per limb ComputeForward(x, 4, 4)
+    -> EltwiseMulMod(., m, 4) -> ComputeInverse(2, 1), as the fused product
+    (one pass fused at the transforms' common contiguous pass) and as three
+    batched calls (forward batch, one element-wise MulMod job, inverse batch)."""
+    import torch
+
+    n = 1 << logn
+    mods = params.rns_moduli(n, limbs, 50, 59)
+    ntts = capi.NTT.create_many([(n, q, psi) for q, psi in mods])
+    count = limbs * polys
+    rng = np.random.default_rng(seed)
+    bounds = [4 * mods[i % limbs][0] for i in range(count)]
+    x = _dev(uniform_rows(rng, bounds, n))
+    m = _dev(uniform_rows(rng, bounds, n))
+    y, z = torch.empty_like(x), torch.empty_like(x)
+    mul = capi.Batch([dict(kind=capi.JOB_MUL, ntts=ntts, count=count, result=z.data_ptr(), operand=z.data_ptr(),
+                           vector=m.data_ptr(), in_f=4, out_f=1)])
+
+    def fused():
+        capi.product_batch(ntts, y.data_ptr(), x.data_ptr(), m.data_ptr(), count, 4, 1)
+
+    def separate():
+        capi.forward_batch(ntts, z.data_ptr(), x.data_ptr(), count, 4, 4)
+        mul.launch(phased=True)
+        capi.inverse_batch(ntts, z.data_ptr(), z.data_ptr(), count, 2, 1)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = _events()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    ms_f, ms_s = timed(fused), timed(separate)
+    same = torch.equal(y, z)
+    mul.close()
+    return {"workload": f"NTT -> MulMod -> INTT, N=2^{logn}, {count} limbs ({limbs} primes of 50-59 bits)",
+            "fused_ms": ms_f, "separate_calls_ms": ms_s, "speedup": ms_s / ms_f,
+            "fused_rate": 2 * count / (ms_f / 1e3), "unit": UNIT, "same_bits": same}
 
 
 # ------------------------------------------------------------------ uneven
@@ -552,7 +602,7 @@ def kernel_case(family):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["tensor", "uneven", "serve", "eltwise", "case"])
+    ap.add_argument("what", choices=["tensor", "uneven", "serve", "eltwise", "case", "product"])
     ap.add_argument("family", nargs="?", default="eltwise",
                     help="case: eltwise | eltwise_unaligned | tensor | tables | chain | batch | batch_phased | "
                          "batch_eltwise | peak")
@@ -582,6 +632,8 @@ def main():
         out = kernel_case(a.family)
     elif a.what == "uneven":
         out = uneven_batch()
+    elif a.what == "product":
+        out = product_chain()
     else:
         flags = (capi.SERVER_ARRIVAL_PRIORITY if a.arrival_priority else 0) | \
             (capi.SERVER_SMALLEST_FIRST if a.smallest_first else 0) | (capi.SERVER_LARGE_FIRST if a.large_first else 0)

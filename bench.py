@@ -352,6 +352,7 @@ def run_ours(args):
             u_ok = all(digest_of(j["y"]) == w["sha256"] for j, w in zip(u["jobs"], want["uneven"]["jobs"]))
         u.pop("jobs", None)
         torch.cuda.empty_cache()
+        pr = workloads.product_chain()
         others = {
             "tensor_product": {"workload": t["workload"], "ms": t["fused_ms"], "GBps": t["fused_GBps"],
                                "per_limb_calls_ms": t["per_limb_calls_ms"], "speedup": t["speedup"],
@@ -360,6 +361,10 @@ def run_ours(args):
                              "persistent_rate": u["one_launch_rate"], "phased_rate": u["phased_rate"],
                              "per_limb_rate": u["per_limb_rate"], "unit": u["unit"], "same_bits": u_ok,
                              "same_as_per_limb_calls": u["same_bits"]},
+            "ntt_mulmod_intt": {"workload": pr["workload"], "fused_ms": pr["fused_ms"],
+                                "separate_calls_ms": pr["separate_calls_ms"], "speedup": pr["speedup"],
+                                "fused_rate": pr["fused_rate"], "unit": pr["unit"],
+                                "same_as_separate_calls": pr["same_bits"]},
             "headline": headline_digest_check(capi, ntts, xp, y, sh, want),
             "same_bits_means": "every output word equal to the oracle's (SHA-256 against "
                                "tests/golden/config_digests.json)",

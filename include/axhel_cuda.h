@@ -143,6 +143,19 @@ axhel_status_t axhel_cuda_ntt_chain_mul_batch(const axhel_ntt_t* ntts, uint64_t 
                                               const uint64_t* operand, const uint64_t* multiplicand, uint64_t count,
                                               uint64_t input_mod_factor, uint64_t output_mod_factor, void* stream);
 
+/* Fused NTT -> MulMod -> INTT over a batch (new; the polynomial product in
+ * evaluation form, SEAL's multiply_plain): one kernel chain replaces
+ *   ComputeForward(x, x, in_f, 4); EltwiseMulMod(x, x, m, N, q, 4);
+ *   ComputeInverse(x, x, 2, out_f)
+ * per limb (ntt.cpp:173-204, eltwise-mul-mod.cpp:18-94): the forward's last
+ * pass, the dyadic product and the inverse's first pass run as one pass.
+ * Inputs in [0, 4q); `multiplicand` (device, the layout of operand, values
+ * in [0, 4q), in the forward's bit-reversed order) must not be `result`.
+ * Output natural order, [0, 2q) for out_f == 2, else [0, q). */
+axhel_status_t axhel_cuda_ntt_product_batch(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* result,
+                                            const uint64_t* operand, const uint64_t* multiplicand, uint64_t count,
+                                            uint64_t input_mod_factor, uint64_t output_mod_factor, void* stream);
+
 /* Fused INTT -> FMAMod -> NTT (new):
  *   ComputeInverse(x, x, in_f, 2); EltwiseFMAMod(x, x, scalars[i % n_ntts], addend_or_null, N, q, 2);
  *   ComputeForward(x, x, 1, out_f)

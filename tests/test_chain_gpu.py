@@ -77,3 +77,35 @@ def test_tensor_product_matches_call_sequence(cuda, oracle, factor):
         np.testing.assert_array_equal(r0[s], oracle.reduce(t0, q, 4, 1))
         np.testing.assert_array_equal(r1[s], oracle.reduce(t1, q, 4, 1))
         np.testing.assert_array_equal(r2[s], oracle.reduce(t2, q, 4, 1))
+
+
+@pytest.mark.parametrize("n", [8, 64, 1024, 4096, 16384, 65536, 131072])
+def test_product_matches_call_sequence(cuda, oracle, n):
+    """The fused NTT -> MulMod -> INTT product equals, limb by limb, the
+    reference call sequence ComputeForward(x, 4, 4) -> EltwiseMulMod(., m, 4)
+    -> ComputeInverse(2, out_f): lazy and normalized outputs, in place and out
+    of place."""
+    L, count = 3, 5
+    ms = moduli(oracle, n, L, 45)
+    ntts = [cuda.NTT(n, q, psi) for q, psi in ms]
+    tabs = [oracle.tables(n, q, psi) for q, psi in ms]
+    st = oracle.rng(SEED ^ 0x9D0C ^ n)
+    x = np.concatenate([oracle.random_vector(st, n, 4 * ms[i % L][0]) for i in range(count)])
+    m = np.concatenate([oracle.random_vector(st, n, 4 * ms[i % L][0]) for i in range(count)])
+    for out_f in (2, 1):
+        exp = []
+        for i in range(count):
+            q = ms[i % L][0]
+            fwd, inv, ninv = tabs[i % L]
+            seg = slice(i * n, (i + 1) * n)
+            y = oracle.forward(x[seg], q, fwd, 4, 4)
+            y = oracle.mul(y, m[seg], q, 4)
+            exp.append(oracle.inverse(y, q, inv, ninv, 2, out_f))
+        exp = np.concatenate(exp)
+        d, o, dm = dev(x), dev_empty(x.size), dev(m)
+        cuda.product_batch(ntts, ptr(o), ptr(d), ptr(dm), count, 4, out_f)
+        np.testing.assert_array_equal(host(o), exp, err_msg=f"out of place, out_f={out_f}")
+        cuda.product_batch(ntts, ptr(d), ptr(d), ptr(dm), count, 4, out_f)
+        np.testing.assert_array_equal(host(d), exp, err_msg=f"in place, out_f={out_f}")
+    with pytest.raises(cuda.AxhelError):  # the multiplicand may not be the result
+        cuda.product_batch(ntts, ptr(dm), ptr(d), ptr(dm), count, 4, 1)

@@ -306,6 +306,12 @@ def test_polymul_matches_schoolbook(cuda, oracle, n):
         cuda.mul(ptr(prod), ptr(A), ptr(B), n, q, 1)  # dyadic product in the NTT domain
         t.inverse(ptr(prod), ptr(prod), 1, 1)
         np.testing.assert_array_equal(host(prod, n), want, err_msg=f"normalized, q bits {bits}")
+        # the fused NTT -> MulMod -> INTT product, with b's lazy forward as multiplicand
+        db = dev(b)
+        t.forward(ptr(db), ptr(db), 1, 4)
+        da, out = dev(a), dev_empty(n)
+        cuda.product_batch([t], ptr(out), ptr(da), ptr(db), 1, 1, 1)
+        np.testing.assert_array_equal(host(out, n), want, err_msg=f"fused product, q bits {bits}")
 
 
 def test_refresh_external_tables(cuda, oracle):
