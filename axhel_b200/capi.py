@@ -135,6 +135,8 @@ def _declare(L):
     d("axhel_cuda_tensor_product", st_t, vp, vp, vp, vp, vp, vp, vp, u64, u64, vp, u64, u64, vp)
     d("axhel_cuda_plan_set", st_t, C.c_int, u32, u32, vp, vp, vp)
     d("axhel_cuda_plan_get", st_t, C.c_int, u32, u64, vp, vp, vp, vp)
+    d("axhel_cuda_cluster_plan_set", st_t, C.c_int, u32, u32, u32, u32, u64)
+    d("axhel_cuda_cluster_plan_get", st_t, C.c_int, u32, vp, vp, vp, vp)
     d("axhel_cuda_plan_load", st_t, C.c_char_p, C.POINTER(u32))
     d("axhel_cuda_batch_split_set", st_t, u32, u32)
     d("axhel_cuda_batch_split_get", st_t, u32, C.POINTER(u32))
@@ -509,6 +511,21 @@ def plan_get(inverse, logn, count):
     check(lib().axhel_cuda_plan_get(int(inverse), logn, count, C.byref(npass), C.cast(lg, vp), C.cast(lr, vp),
                                     C.cast(tg, vp)), "plan_get")
     return [(lg[i], lr[i], tg[i]) for i in range(npass.value)]
+
+
+def cluster_plan_set(inverse, logn, lga=0, lr=0, csize=0, max_limbs=0):
+    """Single-launch cluster form of a transform of up to `max_limbs` limbs
+    (lga = 0 restores the built-in choice; max_limbs = 0 turns it off)."""
+    check(lib().axhel_cuda_cluster_plan_set(int(inverse), logn, lga, lr, csize, max_limbs), "cluster_plan_set")
+
+
+def cluster_plan_get(inverse, logn):
+    """(lga, lr, csize, max_limbs) of the cluster form for N = 2^logn."""
+    a, b, c = u32(), u32(), u32()
+    m = u64()
+    check(lib().axhel_cuda_cluster_plan_get(int(inverse), logn, C.byref(a), C.byref(b), C.byref(c), C.byref(m)),
+          "cluster_plan_get")
+    return a.value, b.value, c.value, m.value
 
 
 def batch_split_set(logn, row_stages):

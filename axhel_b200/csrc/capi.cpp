@@ -442,7 +442,6 @@ axhel_status_t transform(bool inverse, const axhel_ntt_t* ntts, uint64_t n_ntts,
     if (count == 0) return AXHEL_OK;
     if (!result || !operand) return fail(AXHEL_ERR_INVALID, "null data pointer");
     a.count = count;
-    const NttPlan plan = plan_for(inverse, a.logn, count);
     uint32_t first = 0, last = 0;
     if (inverse) {
         if (batch_api && in_f == 4) first |= kPreCsub2q;
@@ -450,6 +449,19 @@ axhel_status_t transform(bool inverse, const axhel_ntt_t* ntts, uint64_t n_ntts,
     } else {
         if (out_f != 4) last |= kPostNorm;  // ntt.cpp:180-185
     }
+    // a few limbs: both passes in one launch, one cluster per limb (unless a
+    // pass plan was set explicitly for this degree)
+    ClusterCfg cc;
+    if (!plan_overridden(inverse, a.logn) && cluster_plan(inverse, a.logn, count, &cc)) {
+        a.src = operand;
+        a.dst = result;
+        a.s0 = 0;
+        a.tg = 0;
+        a.flags = first | last | kLastPass;
+        const cudaError_t e = launch_ntt_cluster(inverse, cc, a, S(stream));
+        return e == cudaSuccess ? AXHEL_OK : cuda_fail(e, inverse ? "inverse NTT (cluster)" : "forward NTT (cluster)");
+    }
+    const NttPlan plan = plan_for(inverse, a.logn, count);
     return run_plan(inverse, plan, a, operand, result, first, last, S(stream));
 }
 
@@ -750,6 +762,33 @@ axhel_status_t axhel_cuda_plan_get(int inverse, uint32_t logn, uint64_t count, u
         lr[i] = (uint32_t)p.pass[i].lr;
         tg[i] = (uint32_t)p.pass[i].tg;
     }
+    return AXHEL_OK;
+}
+
+axhel_status_t axhel_cuda_cluster_plan_set(int inverse, uint32_t logn, uint32_t lga, uint32_t lr, uint32_t csize,
+                                           uint64_t max_limbs)
+{
+    if (logn < 12 || logn > 17) return fail(AXHEL_ERR_UNSUPPORTED, "cluster form covers log degree 12..17");
+    if (lga == 0) {
+        cluster_plan_override(inverse != 0, logn, nullptr);
+        return AXHEL_OK;
+    }
+    const ClusterCfg c{(int)lga, (int)lr, (int)csize, max_limbs};
+    if (max_limbs && !cluster_cfg_valid(logn, c))
+        return fail(AXHEL_ERR_UNSUPPORTED, "cluster configuration not compiled or not valid for this degree");
+    cluster_plan_override(inverse != 0, logn, &c);
+    return AXHEL_OK;
+}
+
+axhel_status_t axhel_cuda_cluster_plan_get(int inverse, uint32_t logn, uint32_t* lga, uint32_t* lr, uint32_t* csize,
+                                           uint64_t* max_limbs)
+{
+    if (!lga || !lr || !csize || !max_limbs) return fail(AXHEL_ERR_INVALID, "null output");
+    const ClusterCfg c = cluster_plan_current(inverse != 0, logn);
+    *lga = (uint32_t)c.lga;
+    *lr = (uint32_t)c.lr;
+    *csize = (uint32_t)c.csize;
+    *max_limbs = c.max_limbs;
     return AXHEL_OK;
 }
 

@@ -5,14 +5,16 @@
 // synchronous (results are visible on return), result may alias the
 // operands, n == 0 is a no-op, and unsupported mod-factors leave the result
 // untouched.  Pointers may be host memory (the reference's and SEAL's usage:
-// operands are copied into per-thread pinned buffers, then by DMA into
-// per-thread device buffers, and results back the same way) or device
-// memory (used in place, no copies).  Each host thread issues its work on its own
+// operands are copied into per-thread pinned buffers; small ones are read
+// and written there by the kernels themselves through the device's mapping
+// of that memory, larger ones go by DMA to per-thread device buffers and
+// back) or device memory (used in place, no copies).  Each host thread issues its work on its own
 // per-thread default stream, so const NTT objects shared between threads (as
 // SEAL's process-wide cache does) are safe to use concurrently.
 // CUDA failures throw std::runtime_error: there is no CPU fallback.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <stdexcept>
@@ -43,6 +45,9 @@ inline cudaStream_t stream() { return cudaStreamPerThread; }
 
 // Default bound for staging host operands through pinned buffers.
 constexpr size_t kPinnedStagingMax = size_t(1) << 30;
+// Default bound for operands the kernels access in the pinned buffers
+// directly (no DMA copy).
+constexpr size_t kZeroCopyMax = size_t(128) << 10;
 
 // Growable per-thread device staging buffers (one per operand slot).
 struct Staging {
@@ -71,8 +76,11 @@ thread_local Staging t_staging;
 // by the CPU and from there to the device by DMA (and results the other way),
 // instead of handing pageable memory to cudaMemcpyAsync, which stages it
 // through the driver's own buffers and returns only when the copy is done.
+// The buffers are mapped into the device's address space (`dev` is the
+// device's view of `buf`), so a kernel can also read and write them itself.
 struct Bounce {
     uint64_t* buf[4] = {nullptr, nullptr, nullptr, nullptr};
+    uint64_t* dev[4] = {nullptr, nullptr, nullptr, nullptr};
     size_t cap[4] = {0, 0, 0, 0};
     ~Bounce()
     {
@@ -83,9 +91,19 @@ struct Bounce {
     {
         if (cap[slot] < words) {
             if (buf[slot]) cudaFreeHost(buf[slot]);
-            buf[slot] = nullptr;
+            buf[slot] = dev[slot] = nullptr;
             cap[slot] = 0;
-            check_cuda(cudaMallocHost(&buf[slot], words * sizeof(uint64_t)), "pinned staging allocation");
+            check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&buf[slot]), words * sizeof(uint64_t),
+                                     cudaHostAllocMapped | cudaHostAllocPortable),
+                       "pinned staging allocation");
+            void* d = nullptr;
+            const cudaError_t e = cudaHostGetDevicePointer(&d, buf[slot], 0);
+            if (e != cudaSuccess) {
+                cudaFreeHost(buf[slot]);
+                buf[slot] = nullptr;
+                check_cuda(e, "pinned staging mapping");
+            }
+            dev[slot] = static_cast<uint64_t*>(d);
             cap[slot] = words;
         }
         return buf[slot];
@@ -105,13 +123,31 @@ size_t pinned_max()
     return v;
 }
 
+// Host operands up to this many bytes are not copied to the device at all:
+// the kernels read them from, and write results to, the mapped pinned
+// buffers over PCIe.  For a small call that saves a DMA copy each way, whose
+// set-up costs more than moving the data.  Environment variable
+// AXHEL_ZERO_COPY_MAX (bytes; 0 = never), read once.
+size_t zero_copy_max()
+{
+    static const size_t v = [] {
+        const char* e = std::getenv("AXHEL_ZERO_COPY_MAX");
+        return e ? (size_t)std::strtoull(e, nullptr, 10) : kZeroCopyMax;
+    }();
+    return std::min(v, pinned_max());
+}
+
 // Device view of an input operand: the pointer itself if it is device
 // memory, else a staged copy.
 const uint64_t* input(const uint64_t* p, uint64_t n, int slot)
 {
     if (!p || axhel_cuda_is_device_pointer(p)) return p;
-    uint64_t* d = t_staging.get(slot, n);
     const size_t bytes = n * sizeof(uint64_t);
+    if (bytes <= zero_copy_max()) {
+        std::memcpy(t_bounce.get(slot, n), p, bytes);
+        return t_bounce.dev[slot];
+    }
+    uint64_t* d = t_staging.get(slot, n);
     const void* src = p;
     if (bytes <= pinned_max()) {
         uint64_t* h = t_bounce.get(slot, n);
@@ -122,15 +158,22 @@ const uint64_t* input(const uint64_t* p, uint64_t n, int slot)
     return d;
 }
 
-// Device destination for `result` (itself, or staging slot 3).
+// Device destination for `result`: itself, pinned slot 3 (mapped, written by
+// the kernels directly) or device staging slot 3.
 struct Output {
     uint64_t* host = nullptr;
     uint64_t* dev = nullptr;
     uint64_t n = 0;
+    bool mapped = false;
     Output(uint64_t* r, uint64_t count) : n(count)
     {
         if (axhel_cuda_is_device_pointer(r)) {
             dev = r;
+        } else if (count * sizeof(uint64_t) <= zero_copy_max()) {
+            host = r;
+            t_bounce.get(3, count);
+            dev = t_bounce.dev[3];
+            mapped = true;
         } else {
             host = r;
             dev = t_staging.get(3, count);
@@ -140,7 +183,7 @@ struct Output {
     {
         const size_t bytes = n * sizeof(uint64_t);
         uint64_t* bounce = (host && bytes <= pinned_max()) ? t_bounce.get(3, n) : nullptr;
-        if (host)
+        if (host && !mapped)
             check_cuda(cudaMemcpyAsync(bounce ? bounce : host, dev, bytes, cudaMemcpyDeviceToHost, stream()),
                        "device to host copy");
         check_cuda(cudaStreamSynchronize(stream()), "stream synchronize");

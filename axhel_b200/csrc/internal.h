@@ -77,11 +77,26 @@ cudaError_t launch_chain_pass(const PassCfg& inv_cfg, const ChainArgs& a, cudaSt
 cudaError_t launch_product_pass(const PassCfg& cfg, const ChainArgs& a, cudaStream_t s);
 bool pass_supported(const PassCfg& cfg);
 
+// Single-launch transform of a few limbs, one thread-block cluster per limb
+// (ntt_cluster.cu): first-pass stages, register stages, CTAs per cluster,
+// and the largest limb count that takes this form.
+struct ClusterCfg {
+    int lga, lr, csize;
+    uint64_t max_limbs;
+};
+bool cluster_cfg_valid(uint32_t logn, const ClusterCfg& c);
+// The cluster form for (dir, logN, limbs), if it applies.
+bool cluster_plan(bool inverse, uint32_t logn, uint64_t count, ClusterCfg* out);
+void cluster_plan_override(bool inverse, uint32_t logn, const ClusterCfg* c);  // nullptr clears
+ClusterCfg cluster_plan_current(bool inverse, uint32_t logn);
+cudaError_t launch_ntt_cluster(bool inverse, const ClusterCfg& c, const PassArgs& a, cudaStream_t s);
+
 // Planner (plan.cpp): default plan for (dir, logN, limbs); autotuned table if loaded.
 NttPlan plan_for(bool inverse, uint32_t logn, uint64_t limbs);
 bool plan_valid(const NttPlan& p, uint32_t logn, bool inverse);
 int plan_load(const char* path);
 void plan_override(bool inverse, uint32_t logn, const NttPlan* p);  // nullptr clears
+bool plan_overridden(bool inverse, uint32_t logn);
 // Uneven-batch engine: stages of the contiguous pass of an N = 2^logn job
 // (override > table > default); the strided pass takes the rest.
 bool batch_row_valid(uint32_t logn, int row);

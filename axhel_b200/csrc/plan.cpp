@@ -169,6 +169,12 @@ NttPlan plan_for(bool inverse, uint32_t logn, uint64_t limbs)
     return default_plan(inverse, logn, limbs);
 }
 
+bool plan_overridden(bool inverse, uint32_t logn)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    return g_override.count({inverse ? 1 : 0, logn}) != 0;
+}
+
 void plan_override(bool inverse, uint32_t logn, const NttPlan* p)
 {
     std::lock_guard<std::mutex> lk(g_mu);

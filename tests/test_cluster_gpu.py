@@ -1,0 +1,114 @@
+"""The single-launch cluster form of small transforms (one thread-block
+cluster per limb, the two passes exchanging the limb through distributed
+shared memory) against the oracle, for every compiled configuration."""
+import numpy as np
+import pytest
+
+from helpers import SEED, dev, dev_empty, host, ptr
+
+pytestmark = pytest.mark.gpu
+
+# (first-pass stages, second-pass stages, register stages) compiled in ntt_cluster.cu
+COMPILED = [(6, 6, 2), (6, 6, 3), (5, 7, 3), (7, 5, 3), (6, 7, 3), (7, 6, 3), (7, 7, 3), (7, 8, 3), (8, 7, 3),
+            (8, 8, 3), (8, 8, 4), (8, 9, 4), (9, 8, 4), (6, 7, 2), (7, 6, 2), (7, 7, 2), (7, 8, 2), (8, 7, 2)]
+
+
+def configs(logn):
+    """Valid (lga, lr, csize) for N = 2^logn: threads per CTA in [32, 512]
+    (256 at 32 registers per element), at most 16 CTAs, shared memory within
+    227 KiB."""
+    out = []
+    for a, b, lr in COMPILED:
+        if a + b != logn:
+            continue
+        for c in (1, 2, 3, 4):
+            lgt = logn - c - lr
+            if c > min(a, b) or lgt < 5 or (1 << lgt) > (256 if lr >= 5 else 512):
+                continue
+            if 2 * 8 * (1 << (logn - c)) > 227 * 1024:
+                continue
+            out.append((a, lr, 1 << c))
+    return out
+
+
+def moduli(oracle, n, L):
+    ntts, tabs, qs = [], [], []
+    for i in range(L):
+        q = oracle.find_ntt_prime_near(n, 52 + 3 * i, 1, 3)
+        psi = oracle.find_primitive_root(n, q)
+        ntts.append((q, psi))
+        tabs.append(oracle.tables(n, q, psi))
+        qs.append(q)
+    return ntts, tabs, qs
+
+
+@pytest.mark.parametrize("logn", [12, 13, 14, 15, 16, 17])
+def test_cluster_configs_bitexact(cuda, oracle, logn):
+    n = 1 << logn
+    L, count = 2, 3
+    params, tabs, qs = moduli(oracle, n, L)
+    ntts = [cuda.NTT(n, q, psi) for q, psi in params]
+    st = oracle.rng(SEED ^ 0xC1A5 ^ logn)
+    x = np.concatenate([oracle.random_vector(st, n, 4 * qs[i % L]) for i in range(count)])
+    ef4 = [oracle.forward(x[i * n:(i + 1) * n], qs[i % L], tabs[i % L][0], 4, 4) for i in range(count)]
+    ef1 = [oracle.forward(x[i * n:(i + 1) * n], qs[i % L], tabs[i % L][0], 4, 1) for i in range(count)]
+    # inverse inputs in [0, 4q): the batch form reduces 4 -> 2 on load
+    ei2 = [oracle.inverse(oracle.reduce(ef4[i], qs[i % L], 4, 2), qs[i % L], tabs[i % L][1], tabs[i % L][2], 2, 2)
+           for i in range(count)]
+    ei1 = [oracle.inverse(oracle.reduce(ef4[i], qs[i % L], 4, 2), qs[i % L], tabs[i % L][1], tabs[i % L][2], 2, 1)
+           for i in range(count)]
+    cfgs = configs(logn)
+    assert cfgs
+    try:
+        for lga, lr, cs in cfgs:
+            for inverse in (False, True):
+                cuda.cluster_plan_set(inverse, logn, lga, lr, cs, count)
+            tag = f"lga={lga} lr={lr} csize={cs}"
+            for k in (1, count):
+                src = dev(x[:k * n])
+                out = dev_empty(k * n)
+                cuda.forward_batch(ntts, ptr(out), ptr(src), k, 4, 4)
+                got4 = host(out)
+                np.testing.assert_array_equal(got4, np.concatenate(ef4[:k]), err_msg=f"forward 4->4 {tag} k={k}")
+                cuda.forward_batch(ntts, ptr(src), ptr(src), k, 4, 1)  # in place
+                np.testing.assert_array_equal(host(src), np.concatenate(ef1[:k]), err_msg=f"forward ->1 {tag}")
+                cuda.inverse_batch(ntts, ptr(src), ptr(out), k, 4, 2)
+                np.testing.assert_array_equal(host(src), np.concatenate(ei2[:k]), err_msg=f"inverse ->2 {tag}")
+                cuda.inverse_batch(ntts, ptr(out), ptr(out), k, 4, 1)  # in place
+                np.testing.assert_array_equal(host(out), np.concatenate(ei1[:k]), err_msg=f"inverse ->1 {tag}")
+                np.testing.assert_array_equal(
+                    host(out), np.concatenate([x[i * n:(i + 1) * n] % np.uint64(qs[i % L]) for i in range(k)]))
+    finally:
+        for inverse in (False, True):
+            cuda.cluster_plan_set(inverse, logn)
+
+
+@pytest.mark.parametrize("logn", [12, 13, 14, 15])
+def test_cluster_form_matches_pass_form(cuda, oracle, logn):
+    """The built-in choice for one limb against the two-launch pass form."""
+    n = 1 << logn
+    params, tabs, qs = moduli(oracle, n, 1)
+    ntt = cuda.NTT(n, *params[0])
+    st = oracle.rng(SEED ^ 0xC1A6 ^ logn)
+    x = oracle.random_vector(st, n, 4 * qs[0])
+    outs = []
+    try:
+        for enabled in (True, False):
+            for inverse in (False, True):
+                if enabled:
+                    cuda.cluster_plan_set(inverse, logn)
+                else:
+                    lga, lr, cs, _ = cuda.cluster_plan_get(inverse, logn)
+                    cuda.cluster_plan_set(inverse, logn, lga, lr, cs, 0)
+            a = dev(x)
+            ntt.forward(ptr(a), ptr(a), 4, 4)
+            f = host(a)
+            b = dev(oracle.reduce(f, qs[0], 4, 2))
+            ntt.inverse(ptr(b), ptr(b), 2, 1)
+            outs.append((f, host(b)))
+    finally:
+        for inverse in (False, True):
+            cuda.cluster_plan_set(inverse, logn)
+    np.testing.assert_array_equal(outs[0][0], outs[1][0])
+    np.testing.assert_array_equal(outs[0][1], outs[1][1])
+    np.testing.assert_array_equal(outs[0][0], oracle.forward(x, qs[0], tabs[0][0], 4, 4))

@@ -18,8 +18,20 @@ def cuda_include():
     pytest.skip("CUDA headers not found")
 
 
-@pytest.mark.parametrize("pinned_max", [None, "0"], ids=["pinned-staging", "pageable-staging"])
-def test_cpp_dropin(tmp_path, cuda, pinned_max):
+# Host operands take three routes: small ones are read and written by the
+# kernels in the mapped pinned buffers (the default up to 128 KiB), larger
+# ones go by DMA through the pinned buffers, or, with pinned staging off,
+# straight from the pageable memory.
+STAGING = {
+    "default": {},
+    "pinned-dma": {"AXHEL_ZERO_COPY_MAX": "0"},
+    "all-zero-copy": {"AXHEL_ZERO_COPY_MAX": str(1 << 30)},
+    "pageable-staging": {"AXHEL_PINNED_STAGING_MAX": "0"},
+}
+
+
+@pytest.mark.parametrize("staging", list(STAGING))
+def test_cpp_dropin(tmp_path, cuda, staging):
     exe = tmp_path / "test_dropin"
     lib_dir = os.path.join(ROOT, "axhel_b200")
     orc = tmp_path / "axhel_oracle.o"
@@ -30,8 +42,7 @@ def test_cpp_dropin(tmp_path, cuda, pinned_max):
            "-lpthread", "-o", str(exe)]
     subprocess.run(cmd, check=True, capture_output=True, text=True)
     env = dict(os.environ)
-    if pinned_max is not None:  # host operands handed to cudaMemcpyAsync as they are
-        env["AXHEL_PINNED_STAGING_MAX"] = pinned_max
+    env.update(STAGING[staging])
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600, env=env)
     assert r.returncode == 0, r.stderr[-4000:]
     assert "all checks passed" in r.stdout

@@ -102,6 +102,34 @@ def test_plan_override_and_table(tmp_path):
     assert capi.plan_get(False, 15, 8) == [(8, 4, 8), (7, 4, 16)]
 
 
+def test_cluster_plan_override():
+    """The single-launch cluster form's configuration: built-in choices are
+    valid, invalid ones are refused, and an override can be cleared."""
+    from axhel_b200 import capi
+
+    for inverse in (False, True):
+        for logn in range(12, 18):
+            lga, lr, cs, m = capi.cluster_plan_get(inverse, logn)
+            assert lga >= 5 and cs in (2, 4, 8, 16) and (m >= 1 or logn >= 16)
+            capi.cluster_plan_set(inverse, logn, lga, lr, cs, max(m, 1))  # valid as it stands
+            capi.cluster_plan_set(inverse, logn)
+    default = capi.cluster_plan_get(False, 12)
+    capi.cluster_plan_set(False, 12, 6, 2, 16, 5)
+    assert capi.cluster_plan_get(False, 12) == (6, 2, 16, 5)
+    with pytest.raises(capi.AxhelError):
+        capi.cluster_plan_set(False, 12, 6, 4, 8, 1)  # not compiled
+    with pytest.raises(capi.AxhelError):
+        capi.cluster_plan_set(False, 12, 6, 3, 32, 1)  # more than 16 CTAs
+    with pytest.raises(capi.AxhelError):
+        capi.cluster_plan_set(False, 16, 8, 4, 4, 1)  # 1024 threads per CTA
+    with pytest.raises(capi.AxhelError):
+        capi.cluster_plan_set(False, 11, 6, 3, 8, 1)  # degree out of range
+    capi.cluster_plan_set(False, 12, 6, 3, 8, 0)  # off
+    assert capi.cluster_plan_get(False, 12)[3] == 0
+    capi.cluster_plan_set(False, 12)
+    assert capi.cluster_plan_get(False, 12) == default
+
+
 def test_params_primes_match_reference_generator(oracle):
     from axhel_b200 import params
 
