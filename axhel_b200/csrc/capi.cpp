@@ -768,7 +768,7 @@ axhel_status_t axhel_cuda_plan_get(int inverse, uint32_t logn, uint64_t count, u
 axhel_status_t axhel_cuda_cluster_plan_set(int inverse, uint32_t logn, uint32_t lga, uint32_t lr, uint32_t csize,
                                            uint64_t max_limbs)
 {
-    if (logn < 12 || logn > 17) return fail(AXHEL_ERR_UNSUPPORTED, "cluster form covers log degree 12..17");
+    if (logn < 10 || logn > 17) return fail(AXHEL_ERR_UNSUPPORTED, "cluster form covers log degree 10..17");
     if (lga == 0) {
         cluster_plan_override(inverse != 0, logn, nullptr);
         return AXHEL_OK;

@@ -166,6 +166,7 @@ const Entry kEntries[] = {
     entry<6, 6, 2>(), entry<6, 6, 3>(), entry<5, 7, 3>(), entry<7, 5, 3>(), entry<6, 7, 3>(), entry<7, 6, 3>(),
     entry<7, 7, 3>(), entry<7, 8, 3>(), entry<8, 7, 3>(), entry<8, 8, 3>(), entry<8, 8, 4>(), entry<8, 9, 4>(),
     entry<9, 8, 4>(), entry<6, 7, 2>(), entry<7, 6, 2>(), entry<7, 7, 2>(), entry<7, 8, 2>(), entry<8, 7, 2>(),
+    entry<5, 5, 2>(), entry<5, 6, 2>(), entry<6, 5, 2>(),
 };
 constexpr int kNumEntries = sizeof(kEntries) / sizeof(kEntries[0]);
 
@@ -176,18 +177,22 @@ const Entry* find_entry(int lga, int lgb, int lr)
     return nullptr;
 }
 
-// Built-in choice per direction and log2 N (12..17): first-pass stages,
+// Built-in choice per direction and log2 N (10..17): first-pass stages,
 // register stages, cluster size, and the largest limb count that takes the
 // cluster form -- the fastest on a B200 by device time per transform
-// (CUDA-graph replay): at N = 2^12 one limb takes 3.8 / 4.6 us (forward /
-// inverse) against 6.0 / 6.5 us for the two pass launches, at 2^13 3.9 / 4.6
-// against 6.6 / 7.2, at 2^14 4.9 / 5.3 against 7.1 / 7.8, at 2^15 6.8 / 7.1
-// against 7.6 / 7.4.  From 2^16 one limb's work needs more than the 16 SMs of
-// a cluster and the pass form (all SMs) is faster, as it is from 64 / 64 /
-// 16 / 4 limbs up at 2^12..2^15.
+// (CUDA-graph replay): at N = 2^10 one limb takes 3.2 / 3.7 us (forward /
+// inverse) against 6.5 / 4.6 us for the pass form, at 2^11 3.6 / 3.8 against
+// 5.0 / 5.5, at 2^12 3.8 / 4.6 against 6.0 / 6.5 (two pass launches), at 2^13
+// 3.9 / 4.6 against 6.6 / 7.2, at 2^14 4.9 / 5.3 against 7.1 / 7.8, at 2^15
+// 6.8 / 7.1 against 7.6 / 7.4.  From 2^16 one limb's work needs more than the
+// 16 SMs of a cluster and the pass form (all SMs) is faster, as it is from
+// 16 / 4 limbs up at 2^14 / 2^15; at 2^10..2^13 the cluster form is still
+// ahead at 64 limbs, the largest count measured.
 ClusterCfg default_cfg(bool inverse, uint32_t logn)
 {
     switch (logn) {
+    case 10: return ClusterCfg{5, 2, 2, 64};
+    case 11: return ClusterCfg{6, 2, 4, 64};
     case 12: return ClusterCfg{6, 2, 8, 64};
     case 13: return inverse ? ClusterCfg{7, 2, 16, 64} : ClusterCfg{6, 2, 16, 64};
     case 14: return ClusterCfg{7, 2, 16, 16};
@@ -211,7 +216,7 @@ int entry_index(const Entry* e) { return (int)(e - kEntries); }
 
 bool cluster_cfg_valid(uint32_t logn, const ClusterCfg& c)
 {
-    if (logn < 12 || logn > 17 || c.max_limbs == 0) return false;
+    if (logn < 10 || logn > 17 || c.max_limbs == 0) return false;
     const int lgb = (int)logn - c.lga;
     if (!find_entry(c.lga, lgb, c.lr)) return false;
     if (c.csize < 2 || c.csize > 16 || (c.csize & (c.csize - 1))) return false;
@@ -224,7 +229,7 @@ bool cluster_cfg_valid(uint32_t logn, const ClusterCfg& c)
 
 bool cluster_plan(bool inverse, uint32_t logn, uint64_t count, ClusterCfg* out)
 {
-    if (logn < 12 || logn > 17) return false;
+    if (logn < 10 || logn > 17) return false;
     ClusterCfg c;
     {
         std::lock_guard<std::mutex> lk(g_mu);

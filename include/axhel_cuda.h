@@ -420,7 +420,7 @@ axhel_status_t axhel_cuda_plan_get(int inverse, uint32_t log_degree, uint64_t co
  * the reference, whose transforms run on the host): one thread-block cluster
  * of `csize` CTAs (2..16) per limb, `lga` stages in the first pass, `lr`
  * register stages; the two passes exchange the limb through the cluster's
- * shared memory instead of HBM.  Used for 2^12 <= N <= 2^17 and count <=
+ * shared memory instead of HBM.  Used for 2^10 <= N <= 2^17 and count <=
  * max_limbs; max_limbs == 0 turns it off for (direction, log2 N), lga == 0
  * restores the built-in choice.  A pass plan set by axhel_cuda_plan_set for
  * the same degree takes precedence.  Every choice computes the same bits. */

@@ -10,7 +10,8 @@ pytestmark = pytest.mark.gpu
 
 # (first-pass stages, second-pass stages, register stages) compiled in ntt_cluster.cu
 COMPILED = [(6, 6, 2), (6, 6, 3), (5, 7, 3), (7, 5, 3), (6, 7, 3), (7, 6, 3), (7, 7, 3), (7, 8, 3), (8, 7, 3),
-            (8, 8, 3), (8, 8, 4), (8, 9, 4), (9, 8, 4), (6, 7, 2), (7, 6, 2), (7, 7, 2), (7, 8, 2), (8, 7, 2)]
+            (8, 8, 3), (8, 8, 4), (8, 9, 4), (9, 8, 4), (6, 7, 2), (7, 6, 2), (7, 7, 2), (7, 8, 2), (8, 7, 2),
+            (5, 5, 2), (5, 6, 2), (6, 5, 2)]
 
 
 def configs(logn):
@@ -42,7 +43,7 @@ def moduli(oracle, n, L):
     return ntts, tabs, qs
 
 
-@pytest.mark.parametrize("logn", [12, 13, 14, 15, 16, 17])
+@pytest.mark.parametrize("logn", [10, 11, 12, 13, 14, 15, 16, 17])
 def test_cluster_configs_bitexact(cuda, oracle, logn):
     n = 1 << logn
     L, count = 2, 3

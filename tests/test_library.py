@@ -108,9 +108,9 @@ def test_cluster_plan_override():
     from axhel_b200 import capi
 
     for inverse in (False, True):
-        for logn in range(12, 18):
+        for logn in range(10, 18):
             lga, lr, cs, m = capi.cluster_plan_get(inverse, logn)
-            assert lga >= 5 and cs in (2, 4, 8, 16) and (m >= 1 or logn >= 16)
+            assert lga >= 5 and cs in (2, 4, 8, 16)
             capi.cluster_plan_set(inverse, logn, lga, lr, cs, max(m, 1))  # valid as it stands
             capi.cluster_plan_set(inverse, logn)
     default = capi.cluster_plan_get(False, 12)
@@ -123,7 +123,7 @@ def test_cluster_plan_override():
     with pytest.raises(capi.AxhelError):
         capi.cluster_plan_set(False, 16, 8, 4, 4, 1)  # 1024 threads per CTA
     with pytest.raises(capi.AxhelError):
-        capi.cluster_plan_set(False, 11, 6, 3, 8, 1)  # degree out of range
+        capi.cluster_plan_set(False, 9, 5, 2, 4, 1)  # degree out of range
     capi.cluster_plan_set(False, 12, 6, 3, 8, 0)  # off
     assert capi.cluster_plan_get(False, 12)[3] == 0
     capi.cluster_plan_set(False, 12)
