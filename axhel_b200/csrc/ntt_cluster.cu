@@ -62,12 +62,152 @@ __device__ __forceinline__ void cluster_wait()
     asm volatile("barrier.cluster.wait.aligned;" ::: "memory");
 }
 
+// ---- rounds with their twiddles loaded ahead
+//
+// A cluster holds one limb on a few SMs with a handful of warps each, so
+// every dependent load shows: a round that loads its twiddles after the
+// exchange before it waits a full L2 round trip.  These variants of the pass
+// kernels' rounds (fwd_stages / inv_stages: same butterflies, same twiddles,
+// same order) take all of a pass's twiddles from registers filled before the
+// pass starts, so their loads overlap the limb's own load (first pass) or
+// the cluster exchange (second pass).
+
+template <bool INV, int LG, int LR, int RD>
+struct RoundShape {
+    static constexpr int R = 1 << LR;
+    static constexpr int LO = round_lo<INV, LG, LR, RD>();
+    static constexpr int HI = LG - RD * LR;  // forward: stage bits HI-1 .. HI-NB
+    static constexpr int NB = HI < LR ? HI : LR;
+    static constexpr int B0 = RD * LR;  // inverse: stage bits B0 .. B1-1
+    static constexpr int B1 = (B0 + LR < LG) ? B0 + LR : LG;
+};
+
+// Twiddles of a pass held in registers: at most 2^LR - 1 per round.
+template <int NR, int LR>
+struct PassTw {
+    ulonglong2 w[NR][(1 << LR) - 1];
+    uint64_t ninv, ninv_q, sr, sr_q;  // the inverse's final stage
+};
+
+template <bool INV, int LG, int LR, int RD, bool LAST>
+__device__ __forceinline__ void load_round_tw(ulonglong2 (&w)[(1 << LR) - 1], uint32_t k, uint64_t blk, uint32_t s0,
+                                              uint64_t n, const ulonglong2* __restrict__ tw)
+{
+    using S = RoundShape<INV, LG, LR, RD>;
+    const uint32_t rbase = round_base<LR>(k, S::LO);
+    int idx = 0;
+    if constexpr (INV) {
+#pragma unroll
+        for (int b = S::B0; b < S::B1; ++b) {
+            const int rb = b - S::LO;
+            if (LAST && b == LG - 1) continue;
+            const uint32_t s = s0 + b;
+            const ulonglong2* tws = tw + (1 + n - (n >> s)) + (blk << (LG - b - 1)) + (rbase >> (b + 1));
+#pragma unroll
+            for (int j = 0; j < (S::R >> (rb + 1)); ++j) w[idx++] = __ldg(tws + j);
+        }
+    } else {
+#pragma unroll
+        for (int bb = 0; bb < S::NB; ++bb) {
+            const int b = S::HI - 1 - bb;
+            const int rb = b - S::LO;
+            const uint32_t t = s0 + (LG - 1 - b);
+            const ulonglong2* tws = tw + (1ull << t) + (blk << (LG - 1 - b)) + (rbase >> (b + 1));
+#pragma unroll
+            for (int j = 0; j < (S::R >> (rb + 1)); ++j) w[idx++] = __ldg(tws + j);
+        }
+    }
+}
+
+template <bool INV, int LG, int LR, int RD, bool LAST, int NR>
+__device__ __forceinline__ void apply_round(uint64_t (&v)[1 << LR], const PassTw<NR, LR>& pt, uint64_t q,
+                                            uint64_t q2)
+{
+    using S = RoundShape<INV, LG, LR, RD>;
+    int idx = 0;
+    if constexpr (INV) {
+#pragma unroll
+        for (int b = S::B0; b < S::B1; ++b) {
+            const int rb = b - S::LO;
+            if (LAST && b == LG - 1) {
+#pragma unroll
+                for (int j = 0; j < (S::R >> (rb + 1)); ++j)
+#pragma unroll
+                    for (int l = 0; l < (1 << rb); ++l) {
+                        const int i0 = (j << (rb + 1)) | l;
+                        inv_final_butterfly(v[i0], v[i0 | (1 << rb)], pt.ninv, pt.ninv_q, pt.sr, pt.sr_q, q, q2);
+                    }
+            } else {
+#pragma unroll
+                for (int j = 0; j < (S::R >> (rb + 1)); ++j) {
+                    const ulonglong2 w = pt.w[RD][idx++];
+#pragma unroll
+                    for (int l = 0; l < (1 << rb); ++l) {
+                        const int i0 = (j << (rb + 1)) | l;
+                        inv_butterfly(v[i0], v[i0 | (1 << rb)], w.x, w.y, q, q2);
+                    }
+                }
+            }
+        }
+    } else {
+#pragma unroll
+        for (int bb = 0; bb < S::NB; ++bb) {
+            const int rb = S::HI - 1 - bb - S::LO;
+#pragma unroll
+            for (int j = 0; j < (S::R >> (rb + 1)); ++j) {
+                const ulonglong2 w = pt.w[RD][idx++];
+#pragma unroll
+                for (int l = 0; l < (1 << rb); ++l) {
+                    const int i0 = (j << (rb + 1)) | l;
+                    fwd_butterfly(v[i0], v[i0 | (1 << rb)], w.x, w.y, q, q2);
+                }
+            }
+        }
+    }
+}
+
+template <bool INV, int LG, int LR, bool LAST, int NR, int... RD>
+__device__ __forceinline__ void load_pass_tw(std::integer_sequence<int, RD...>, PassTw<NR, LR>& pt, uint32_t k,
+                                             uint64_t blk, uint32_t s0, uint64_t n, const ModCtx* cx)
+{
+    (load_round_tw<INV, LG, LR, RD, LAST>(pt.w[RD], k, blk, s0, n, INV ? cx->inv : cx->fwd), ...);
+    if constexpr (INV && LAST) {
+        pt.ninv = cx->ninv;
+        pt.ninv_q = cx->ninv_q;
+        pt.sr = cx->sroot;
+        pt.sr_q = cx->sroot_q;
+    }
+}
+
+template <bool INV, int LG, int LR, int RD, bool LAST, int NR>
+__device__ __forceinline__ void step(uint64_t (&v)[1 << LR], const PassTw<NR, LR>& pt, uint64_t* smg, uint32_t k,
+                                     uint32_t hmask, uint32_t lsh, uint64_t q, uint64_t q2)
+{
+    if constexpr (RD > 0) exchange<INV, LG, LR, RD>(v, smg, k, hmask, lsh);
+    apply_round<INV, LG, LR, RD, LAST, NR>(v, pt, q, q2);
+}
+
+template <bool INV, int LG, int LR, bool LAST, int NR, int... RD>
+__device__ __forceinline__ void run_pass_tw(std::integer_sequence<int, RD...>, uint64_t (&v)[1 << LR],
+                                            const PassTw<NR, LR>& pt, uint64_t* smg, uint32_t k, uint32_t hmask,
+                                            uint32_t lsh, uint64_t q, uint64_t q2)
+{
+    (step<INV, LG, LR, RD, LAST, NR>(v, pt, smg, k, hmask, lsh, q, q2), ...);
+}
+
+// Prefetched twiddles fit the register budget when a pass has at most 12.
+template <int LG, int LR>
+constexpr bool prefetch_fits()
+{
+    return num_rounds<LG, LR>() * ((1 << LR) - 1) <= 12;
+}
+
 }  // namespace
 
 // One cluster of C CTAs per limb (grid = limbs * C, cluster dims C x 1 x 1);
 // blockDim = 2^(logn - c - LR); dynamic shared memory = 2 * N/C words (the
 // exchange scratch of the rounds, then the landing area of the second pass).
-template <bool INV, int LGA, int LGB, int LR>
+template <bool INV, int LGA, int LGB, int LR, bool PREFETCH>
 __global__ void __launch_bounds__(max_threads(LR)) ntt_cluster_kernel(const __grid_constant__ PassArgs a)
 {
     extern __shared__ uint64_t sm[];
@@ -90,22 +230,45 @@ __global__ void __launch_bounds__(max_threads(LR)) ntt_cluster_kernel(const __gr
     const uint64_t* lsrc = a.src + (limb << logn);
     uint64_t* ldst = a.dst + (limb << logn);
     const bool vec_ok = ((reinterpret_cast<uintptr_t>(a.src) | reinterpret_cast<uintptr_t>(a.dst)) & 15) == 0;
+    // twiddles prefetched into registers: shorter dependent chains, more
+    // registers (the launcher picks it when the grid is one wave)
+    constexpr bool PRE = PREFETCH && prefetch_fits<LGA, LR>() && prefetch_fits<LGB, LR>();
+    constexpr int NRA = num_rounds<LGA, LR>(), NRB = num_rounds<LGB, LR>();
     uint64_t v[R];
+
+    // second-pass geometry (needed early to prefetch its twiddles)
+    const Tile tB = make_tile<LGB>(INV ? (uint32_t)LGA : 0u, lgtgB, limb, rank);
+    uint32_t giB, kB;
+    thread_role<LGB, LR>(tB, giB, kB);
+    const uint64_t blkB = tile_blk<LGB>(tB, giB);
 
     // ---- first pass: stages [0, LGA)
     {
         constexpr int LO_FIRST = round_lo<INV, LGA, LR, 0>();
-        constexpr int LO_LAST = round_lo<INV, LGA, LR, num_rounds<LGA, LR>() - 1>();
+        constexpr int LO_LAST = round_lo<INV, LGA, LR, NRA - 1>();
         const Tile t = make_tile<LGA>(INV ? 0u : (uint32_t)LGB, lgtgA, limb, rank);
         uint32_t gi, k;
         thread_role<LGA, LR>(t, gi, k);
+        const uint64_t blk = tile_blk<LGA>(t, gi);
         load_global<LGA, LR, LO_FIRST>(v, lsrc, t, gi, round_base<LR>(k, LO_FIRST), vec_ok);
-        if (a.flags & kPreCsub2q) {
+        if constexpr (PRE) {
+            PassTw<NRA, LR> pt;
+            load_pass_tw<INV, LGA, LR, false>(std::make_integer_sequence<int, NRA>{}, pt, k, blk, 0, n, cx);
+            if (a.flags & kPreCsub2q) {
 #pragma unroll
-            for (int i = 0; i < R; ++i) v[i] = csub_lazy(v[i], q2);
+                for (int i = 0; i < R; ++i) v[i] = csub_lazy(v[i], q2);
+            }
+            run_pass_tw<INV, LGA, LR, false>(std::make_integer_sequence<int, NRA>{}, v, pt, scratch + (gi << LGA), k,
+                                             group_mask<LGA, LR>(t.strided, lgtgA, gi), lane_shift(t.strided, lgtgA),
+                                             q, q2);
+        } else {
+            if (a.flags & kPreCsub2q) {
+#pragma unroll
+                for (int i = 0; i < R; ++i) v[i] = csub_lazy(v[i], q2);
+            }
+            run_rounds<INV, LGA, LR>(v, scratch + (gi << LGA), k, group_mask<LGA, LR>(t.strided, lgtgA, gi),
+                                     lane_shift(t.strided, lgtgA), blk, 0, n, cx, q, q2, false);
         }
-        run_rounds<INV, LGA, LR>(v, scratch + (gi << LGA), k, group_mask<LGA, LR>(t.strided, lgtgA, gi),
-                                 lane_shift(t.strided, lgtgA), tile_blk<LGA>(t, gi), 0, n, cx, q, q2, false);
         // hand each element to its second-pass owner
         const uint32_t rb = round_base<LR>(k, LO_LAST);
         cluster_wait();
@@ -118,30 +281,35 @@ __global__ void __launch_bounds__(max_threads(LR)) ntt_cluster_kernel(const __gr
             cl.map_shared_rank(landing, owner)[off] = v[i];
         }
     }
-    // all remote stores of the cluster are visible after this barrier
-    cl.sync();
 
     // ---- second pass: stages [LGA, logn)
-    {
-        constexpr int LO_FIRST = round_lo<INV, LGB, LR, 0>();
-        constexpr int LO_LAST = round_lo<INV, LGB, LR, num_rounds<LGB, LR>() - 1>();
-        const Tile t = make_tile<LGB>(INV ? (uint32_t)LGA : 0u, lgtgB, limb, rank);
-        uint32_t gi, k;
-        thread_role<LGB, LR>(t, gi, k);
-        // the landing area is the tile itself, compacted: strided tiles as
-        // rows of 2^lgtgB columns, contiguous ones as they are
-        Tile tl = t;
-        tl.base = 0;
-        if (tl.strided) tl.lgS = lgtgB;
-        load_global<LGB, LR, LO_FIRST>(v, landing, tl, gi, round_base<LR>(k, LO_FIRST), true);
-        run_rounds<INV, LGB, LR>(v, scratch + (gi << LGB), k, group_mask<LGB, LR>(t.strided, lgtgB, gi),
-                                 lane_shift(t.strided, lgtgB), tile_blk<LGB>(t, gi), LGA, n, cx, q, q2, INV);
-        if (a.flags & kPostNorm) {
-#pragma unroll
-            for (int i = 0; i < R; ++i) v[i] = INV ? csub_lazy(v[i], q) : csub_lazy(csub_lazy(v[i], q2), q);
-        }
-        store_global<LGB, LR, LO_LAST>(v, ldst, t, gi, round_base<LR>(k, LO_LAST), vec_ok);
+    constexpr int LO_FIRST = round_lo<INV, LGB, LR, 0>();
+    constexpr int LO_LAST = round_lo<INV, LGB, LR, NRB - 1>();
+    // the landing area is the tile itself, compacted: strided tiles as rows
+    // of 2^lgtgB columns, contiguous ones as they are
+    Tile tl = tB;
+    tl.base = 0;
+    if (tl.strided) tl.lgS = lgtgB;
+    if constexpr (PRE) {
+        PassTw<NRB, LR> pt;
+        load_pass_tw<INV, LGB, LR, INV>(std::make_integer_sequence<int, NRB>{}, pt, kB, blkB, LGA, n, cx);
+        // all remote stores of the cluster are visible after this barrier
+        cl.sync();
+        load_global<LGB, LR, LO_FIRST>(v, landing, tl, giB, round_base<LR>(kB, LO_FIRST), true);
+        run_pass_tw<INV, LGB, LR, INV>(std::make_integer_sequence<int, NRB>{}, v, pt, scratch + (giB << LGB), kB,
+                                       group_mask<LGB, LR>(tB.strided, lgtgB, giB), lane_shift(tB.strided, lgtgB),
+                                       q, q2);
+    } else {
+        cl.sync();
+        load_global<LGB, LR, LO_FIRST>(v, landing, tl, giB, round_base<LR>(kB, LO_FIRST), true);
+        run_rounds<INV, LGB, LR>(v, scratch + (giB << LGB), kB, group_mask<LGB, LR>(tB.strided, lgtgB, giB),
+                                 lane_shift(tB.strided, lgtgB), blkB, LGA, n, cx, q, q2, INV);
     }
+    if (a.flags & kPostNorm) {
+#pragma unroll
+        for (int i = 0; i < R; ++i) v[i] = INV ? csub_lazy(v[i], q) : csub_lazy(csub_lazy(v[i], q2), q);
+    }
+    store_global<LGB, LR, LO_LAST>(v, ldst, tB, giB, round_base<LR>(kB, LO_LAST), vec_ok);
 }
 
 // ------------------------------------------------------------------ host side
@@ -152,13 +320,20 @@ using ClusterFn = void (*)(const PassArgs);
 
 struct Entry {
     int lga, lgb, lr;
-    ClusterFn fwd, inv;
+    ClusterFn fn[2][2];  // [inverse][prefetching twiddles]; [.][1] null where it does not fit
 };
 
 template <int A, int B, int L>
 Entry entry()
 {
-    return Entry{A, B, L, ntt_cluster_kernel<false, A, B, L>, ntt_cluster_kernel<true, A, B, L>};
+    constexpr bool pre = prefetch_fits<A, L>() && prefetch_fits<B, L>();
+    Entry e{A, B, L, {{ntt_cluster_kernel<false, A, B, L, false>, nullptr},
+                      {ntt_cluster_kernel<true, A, B, L, false>, nullptr}}};
+    if constexpr (pre) {
+        e.fn[0][1] = ntt_cluster_kernel<false, A, B, L, true>;
+        e.fn[1][1] = ntt_cluster_kernel<true, A, B, L, true>;
+    }
+    return e;
 }
 
 // The compiled (first-pass stages, second-pass stages, register stages).
@@ -180,14 +355,13 @@ const Entry* find_entry(int lga, int lgb, int lr)
 // Built-in choice per direction and log2 N (10..17): first-pass stages,
 // register stages, cluster size, and the largest limb count that takes the
 // cluster form -- the fastest on a B200 by device time per transform
-// (CUDA-graph replay): at N = 2^10 one limb takes 3.2 / 3.7 us (forward /
-// inverse) against 6.5 / 4.6 us for the pass form, at 2^11 3.6 / 3.8 against
-// 5.0 / 5.5, at 2^12 3.8 / 4.6 against 6.0 / 6.5 (two pass launches), at 2^13
-// 3.9 / 4.6 against 6.6 / 7.2, at 2^14 4.9 / 5.3 against 7.1 / 7.8, at 2^15
-// 6.8 / 7.1 against 7.6 / 7.4.  From 2^16 one limb's work needs more than the
-// 16 SMs of a cluster and the pass form (all SMs) is faster, as it is from
-// 16 / 4 limbs up at 2^14 / 2^15; at 2^10..2^13 the cluster form is still
-// ahead at 64 limbs, the largest count measured.
+// (CUDA-graph replay).  One limb, forward / inverse, against the pass form:
+// 2^10 3.0 / 3.2 us (6.7 / 4.7), 2^11 3.2 / 3.3 (5.0 / 5.6), 2^12 3.4 / 3.5
+// (6.5 / 6.6), 2^13 3.7 / 3.7 (6.7 / 7.2), 2^14 4.7 / 4.9 (7.1 / 7.7), 2^15
+// 7.0 / 7.3 (7.6 / 7.5).  From 2^16 one limb's work needs more than the 16
+// SMs of a cluster and the pass form (all SMs) is faster, as it is from 16 /
+// 4 limbs up at 2^14 / 2^15; at 2^10..2^13 the cluster form is still ahead
+// at 64 limbs, the largest count measured.
 ClusterCfg default_cfg(bool inverse, uint32_t logn)
 {
     switch (logn) {
@@ -208,7 +382,7 @@ bool g_set[2][18] = {};
 ClusterCfg g_over[2][18] = {};
 // per entry and device: shared-memory / cluster-size attributes set
 std::mutex g_attr_mu;
-uint64_t g_attr_done[2][kNumEntries] = {};
+uint64_t g_attr_done[kNumEntries][2][2] = {};
 
 int entry_index(const Entry* e) { return (int)(e - kEntries); }
 
@@ -260,19 +434,24 @@ cudaError_t launch_ntt_cluster(bool inverse, const ClusterCfg& c, const PassArgs
     if (!cluster_cfg_valid(a.logn, c)) return cudaErrorInvalidValue;
     const int lgb = (int)a.logn - c.lga;
     const Entry* e = find_entry(c.lga, lgb, c.lr);
-    ClusterFn fn = inverse ? e->inv : e->fwd;
     const int lc = __builtin_ctz(c.csize);
     const size_t smem = 2 * (sizeof(uint64_t) << (a.logn - lc));
     const uint64_t blocks = a.count * (uint64_t)c.csize;
     if (a.count == 0) return cudaSuccess;
     if (blocks > 0x7fffffffull) return cudaErrorInvalidValue;
+    // Twiddles prefetched into registers shorten each round's dependent
+    // chain but cost occupancy: worth it while the grid is one wave of at
+    // most one CTA per SM (measured faster there up to N = 2^14, slower with
+    // several clusters per SM and at 2^15).
+    const bool pre = e->fn[inverse][1] && a.logn <= 14 && blocks <= (uint64_t)sm_count();
+    ClusterFn fn = e->fn[inverse][pre];
     int dev = 0;
     cudaError_t err = cudaGetDevice(&dev);
     if (err != cudaSuccess) return err;
     if (dev >= 64) return cudaErrorInvalidDevice;
     {
         std::lock_guard<std::mutex> lk(g_attr_mu);
-        uint64_t& done = g_attr_done[inverse][entry_index(e)];
+        uint64_t& done = g_attr_done[entry_index(e)][inverse][pre];
         if (!(done >> dev & 1)) {
             err = cudaFuncSetAttribute(reinterpret_cast<const void*>(fn),
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
@@ -296,7 +475,8 @@ cudaError_t launch_ntt_cluster(bool inverse, const ClusterCfg& c, const PassArgs
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     count_launch();
-    ProfScope prof(s, "ntt_%s_cluster lga=%d lr=%d c=%d", inverse ? "inv" : "fwd", c.lga, c.lr, c.csize);
+    ProfScope prof(s, "ntt_%s_cluster lga=%d lr=%d c=%d%s", inverse ? "inv" : "fwd", c.lga, c.lr, c.csize,
+                   pre ? " prefetch" : "");
     void* args[] = {const_cast<PassArgs*>(&a)};
     err = cudaLaunchKernelExC(&cfg, reinterpret_cast<const void*>(fn), args);
     return err != cudaSuccess ? err : cudaGetLastError();

@@ -572,6 +572,14 @@ def kernel_case(family):
         t = capi.NTT(n, q, psi)
         for inv in (False, True):
             capi.butterfly_peak(t, inv)
+    elif family == "cluster":  # one limb of N = 2^12, forward and inverse: the one-launch cluster form
+        n = 1 << 12
+        q, psi = params.rns_moduli(n, 1, 50, 59)[0]
+        t = capi.NTT(n, q, psi)
+        x = _dev(rng.integers(0, q, n, dtype=np.uint64))
+        for _ in range(3):
+            capi.forward_batch([t], x.data_ptr(), x.data_ptr(), 1, 4, 4)
+            capi.inverse_batch([t], x.data_ptr(), x.data_ptr(), 1, 4, 1)
     elif family == "tables":  # 3 x 24 fresh contexts of N = 2^16
         for lo, hi in ((30, 40), (41, 51), (52, 62)):
             capi.NTT.create_many([(1 << 16, q, psi) for q, psi in params.rns_moduli(1 << 16, 24, lo, hi)])
@@ -600,12 +608,62 @@ def kernel_case(family):
     return {"case": family, "ok": True}
 
 
+def small_transform_latency(counts=(1, 4, 16, 64), reps=40):
+    """Device time per batched transform of a few limbs, N = 2^10..2^17, in
+    the one-launch cluster form (built-in choice) and in the two-launch pass
+    form: `reps` calls captured in a CUDA graph and replayed (no host launch
+    cost), best of 5 replays, microseconds per call."""
+    import torch
+
+    rows = []
+    for logn in range(10, 18):
+        n = 1 << logn
+        mods = params.rns_moduli(n, 4, 50, 59)
+        ntts = [capi.NTT(n, q, p) for q, p in mods]
+        for count in counts:
+            x = torch.randint(0, 1 << 40, (count * n,), dtype=torch.int64, device="cuda")
+            y = torch.empty_like(x)
+            for inverse in (False, True):
+                f, fa = (capi.inverse_batch, (2, 2)) if inverse else (capi.forward_batch, (4, 4))
+                row = {"logn": logn, "count": count, "direction": "inverse" if inverse else "forward"}
+                cfg = capi.cluster_plan_get(inverse, logn)
+                for form in ("cluster", "passes"):
+                    if form == "cluster" and cfg[3] < count:
+                        continue
+                    capi.cluster_plan_set(inverse, logn, *cfg[:3], 0 if form == "passes" else max(cfg[3], 1))
+                    s = torch.cuda.Stream()
+                    s.wait_stream(torch.cuda.current_stream())
+                    call = lambda st: f(ntts, y.data_ptr(), x.data_ptr(), count, fa[0], fa[1], st)
+                    with torch.cuda.stream(s):
+                        for _ in range(3):
+                            call(s.cuda_stream)
+                    torch.cuda.synchronize()
+                    g = torch.cuda.CUDAGraph()
+                    with torch.cuda.graph(g, stream=s):
+                        for _ in range(reps):
+                            call(s.cuda_stream)
+                    best = float("inf")
+                    for _ in range(5):
+                        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        e0.record()
+                        g.replay()
+                        e1.record()
+                        torch.cuda.synchronize()
+                        best = min(best, e0.elapsed_time(e1) * 1e3 / reps)
+                    del g
+                    row[f"{form}_us"] = round(best, 2)
+                capi.cluster_plan_set(inverse, logn)
+                rows.append(row)
+    return {"workload": "device time per call, a few limbs of N = 2^10..2^17 (CUDA-graph replay)",
+            "cluster_form": {str(l): capi.cluster_plan_get(False, l) for l in range(10, 18)}, "rows": rows}
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["tensor", "uneven", "serve", "eltwise", "case", "product"])
+    ap.add_argument("what", choices=["tensor", "uneven", "serve", "eltwise", "case", "product", "latency"])
     ap.add_argument("family", nargs="?", default="eltwise",
                     help="case: eltwise | eltwise_unaligned | tensor | tables | chain | batch | batch_phased | "
-                         "batch_eltwise | peak")
+                         "batch_eltwise | peak | cluster")
     ap.add_argument("--seconds", type=float, default=4.0)
     ap.add_argument("--device", action="store_true", help="device-resident request operands")
     ap.add_argument("--persistent", action="store_true", help="one persistent launch per batch")
@@ -634,6 +692,8 @@ def main():
         out = uneven_batch()
     elif a.what == "product":
         out = product_chain()
+    elif a.what == "latency":
+        out = small_transform_latency()
     else:
         flags = (capi.SERVER_ARRIVAL_PRIORITY if a.arrival_priority else 0) | \
             (capi.SERVER_SMALLEST_FIRST if a.smallest_first else 0) | (capi.SERVER_LARGE_FIRST if a.large_first else 0)

@@ -46,7 +46,10 @@ def moduli(oracle, n, L):
 @pytest.mark.parametrize("logn", [10, 11, 12, 13, 14, 15, 16, 17])
 def test_cluster_configs_bitexact(cuda, oracle, logn):
     n = 1 << logn
-    L, count = 2, 3
+    # one limb and a few run one wave of clusters (twiddles prefetched into
+    # registers up to 2^14); 160 limbs take more than one CTA per SM (the
+    # variant without prefetching)
+    L, count = 2, (160 if logn <= 14 else 3)
     params, tabs, qs = moduli(oracle, n, L)
     ntts = [cuda.NTT(n, q, psi) for q, psi in params]
     st = oracle.rng(SEED ^ 0xC1A5 ^ logn)
