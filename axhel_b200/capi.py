@@ -125,6 +125,8 @@ def _declare(L):
     d("axhel_cuda_ntt_chain_mul_batch", st_t, C.POINTER(vp), u64, vp, vp, vp, u64, u64, u64, vp)
     d("axhel_cuda_ntt_chain_fma_batch", st_t, C.POINTER(vp), u64, vp, vp, vp, vp, u64, u64, u64, vp)
     d("axhel_cuda_ntt_product_batch", st_t, C.POINTER(vp), u64, vp, vp, vp, u64, u64, u64, vp)
+    d("axhel_cuda_ntt_forward_mul_batch", st_t, C.POINTER(vp), u64, vp, vp, vp, u64, vp)
+    d("axhel_cuda_ntt_mul_inverse_batch", st_t, C.POINTER(vp), u64, vp, vp, vp, u64, u64, vp)
     d("axhel_cuda_eltwise_add_vv", st_t, vp, vp, vp, u64, u64, vp)
     d("axhel_cuda_eltwise_add_vs", st_t, vp, vp, u64, u64, u64, vp)
     d("axhel_cuda_eltwise_sub_vv", st_t, vp, vp, vp, u64, u64, vp)
@@ -447,6 +449,18 @@ def forward_batch(ntts, dst, src, count, in_f=1, out_f=1, stream=0):
 def inverse_batch(ntts, dst, src, count, in_f=1, out_f=1, stream=0):
     check(lib().axhel_cuda_ntt_inverse_batch(_handles(ntts), len(ntts), dst, src, count, in_f, out_f, stream),
           "ntt_inverse_batch")
+
+
+def forward_mul_batch(ntts, dst, src, multiplicand, count, stream=0):
+    """Forward transform of each limb, then the dyadic product with `multiplicand`."""
+    check(lib().axhel_cuda_ntt_forward_mul_batch(_handles(ntts), len(ntts), dst, src, multiplicand, count, stream),
+          "ntt_forward_mul_batch")
+
+
+def mul_inverse_batch(ntts, dst, src, multiplicand, count, out_f=1, stream=0):
+    """Dyadic product with `multiplicand`, then the inverse transform of each limb."""
+    check(lib().axhel_cuda_ntt_mul_inverse_batch(_handles(ntts), len(ntts), dst, src, multiplicand, count, out_f,
+                                                 stream), "ntt_mul_inverse_batch")
 
 
 def chain_mul_batch(ntts, dst, src, multiplicand, count, in_f=2, out_f=1, stream=0):

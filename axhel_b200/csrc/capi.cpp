@@ -431,9 +431,12 @@ axhel_status_t run_plan(bool inverse, const NttPlan& plan, PassArgs a, const uin
     return AXHEL_OK;
 }
 
+// `mul` (optional): the dyadic product with it fused into the transform --
+// ahead of an inverse (MulMod<4> on load, so inputs in [0, 4q)) or after a
+// forward (MulMod<4> of the lazy [0, 4q) output; canonical result).
 axhel_status_t transform(bool inverse, const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* result,
                          const uint64_t* operand, uint64_t count, uint64_t in_f, uint64_t out_f, bool batch_api,
-                         void* stream)
+                         void* stream, const uint64_t* mul = nullptr)
 {
     PassArgs a{};
     uint64_t n;
@@ -442,8 +445,16 @@ axhel_status_t transform(bool inverse, const axhel_ntt_t* ntts, uint64_t n_ntts,
     if (count == 0) return AXHEL_OK;
     if (!result || !operand) return fail(AXHEL_ERR_INVALID, "null data pointer");
     a.count = count;
+    a.operand = mul;
     uint32_t first = 0, last = 0;
-    if (inverse) {
+    if (mul) {
+        if (inverse) {
+            first |= kPreMul;
+            if (out_f != 2) last |= kPostNorm;
+        } else {
+            last |= kPostMul;
+        }
+    } else if (inverse) {
         if (batch_api && in_f == 4) first |= kPreCsub2q;
         if (out_f != 2) last |= kPostNorm;  // ntt.cpp:198-203
     } else {
@@ -634,6 +645,23 @@ axhel_status_t axhel_cuda_ntt_inverse_batch(const axhel_ntt_t* ntts, uint64_t n_
                                             uint64_t count, uint64_t in_f, uint64_t out_f, void* stream)
 {
     return transform(true, ntts, n_ntts, r, x, count, in_f, out_f, true, stream);
+}
+
+axhel_status_t axhel_cuda_ntt_forward_mul_batch(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* r,
+                                                const uint64_t* x, const uint64_t* m, uint64_t count, void* stream)
+{
+    if (count && !m) return fail(AXHEL_ERR_INVALID, "null multiplicand");
+    if (count && m == r) return fail(AXHEL_ERR_INVALID, "the multiplicand must not be the result buffer");
+    return transform(false, ntts, n_ntts, r, x, count, 4, 4, true, stream, m);
+}
+
+axhel_status_t axhel_cuda_ntt_mul_inverse_batch(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* r,
+                                                const uint64_t* x, const uint64_t* m, uint64_t count, uint64_t out_f,
+                                                void* stream)
+{
+    if (count && !m) return fail(AXHEL_ERR_INVALID, "null multiplicand");
+    if (count && m == r) return fail(AXHEL_ERR_INVALID, "the multiplicand must not be the result buffer");
+    return transform(true, ntts, n_ntts, r, x, count, 4, out_f, true, stream, m);
 }
 
 axhel_status_t axhel_cuda_ntt_chain_mul_batch(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* r,

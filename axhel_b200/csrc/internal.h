@@ -34,6 +34,8 @@ enum PassFlags : uint32_t {
     kPreCsub2q = 1u,     // x <- csub(x, 2q) on load (fuses EltwiseReduceMod 4->2 ahead of an inverse)
     kPostNorm = 2u,      // forward: 4->1 after the last stage; inverse: 2->1 after the final stage
     kLastPass = 4u,      // this pass holds global stage logN-1 (inverse: runs the N^-1 final stage)
+    kPreMul = 8u,        // x <- MulMod<4>(x, operand) on load (a dyadic product ahead of an inverse)
+    kPostMul = 16u,      // x <- MulMod<4>(x, operand) before the store (a dyadic product after a forward)
 };
 
 // Geometry of one pass: stages [s0, s0 + lg) of an N = 2^logn transform, on
@@ -42,6 +44,7 @@ enum PassFlags : uint32_t {
 struct PassArgs {
     const uint64_t* src;
     uint64_t* dst;
+    const uint64_t* operand;  // multiplicand of kPreMul / kPostMul, laid out like the data
     uint64_t count;
     uint32_t logn, s0, tg, flags;
     uint32_t nctx;

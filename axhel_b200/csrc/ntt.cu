@@ -19,9 +19,11 @@ constexpr int kMaxLR = 5;
 struct KernelTable {
     PassFn fwd[kMaxLG + 1][kMaxLR + 1] = {};
     PassFn inv[kMaxLG + 1][kMaxLR + 1] = {};
+    PassFn fwd_mul[kMaxLG + 1][kMaxLR + 1] = {};  // with the dyadic product (kPreMul / kPostMul)
+    PassFn inv_mul[kMaxLG + 1][kMaxLR + 1] = {};
     ChainFn chain[kMaxLG + 1][kMaxLR + 1] = {};
     ChainFn product[kMaxLG + 1][kMaxLR + 1] = {};
-    bool smem_set[4][kMaxLG + 1][kMaxLR + 1] = {};
+    bool smem_set[6][kMaxLG + 1][kMaxLR + 1] = {};
 };
 
 template <int LG, int LR>
@@ -30,6 +32,8 @@ void add_one(KernelTable& t)
     if constexpr (LR <= LG) {
         t.fwd[LG][LR] = ntt_pass_kernel<false, LG, LR>;
         t.inv[LG][LR] = ntt_pass_kernel<true, LG, LR>;
+        t.fwd_mul[LG][LR] = ntt_pass_mul_kernel<false, LG, LR>;
+        t.inv_mul[LG][LR] = ntt_pass_mul_kernel<true, LG, LR>;
         t.chain[LG][LR] = ntt_chain_kernel<LG, LR>;
         if constexpr (LR <= 3) t.product[LG][LR] = ntt_product_kernel<LG, LR>;
     }
@@ -111,15 +115,18 @@ cudaError_t launch_ntt_pass(bool inverse, const PassCfg& c, const PassArgs& a, c
     if (!pass_supported(c)) return cudaErrorInvalidValue;
     const uint32_t lgS = inverse ? a.s0 : (a.logn - a.s0 - c.lg);
     if (!geometry_ok(c, a.logn, lgS) || (uint32_t)c.tg != a.tg) return cudaErrorInvalidValue;
-    PassFn fn = inverse ? table().inv[c.lg][c.lr] : table().fwd[c.lg][c.lr];
-    cudaError_t e = ensure_smem(fn, inverse ? 1 : 0, c);
+    const bool mul = (a.flags & (kPreMul | kPostMul)) != 0;
+    PassFn fn = mul ? (inverse ? table().inv_mul[c.lg][c.lr] : table().fwd_mul[c.lg][c.lr])
+                    : (inverse ? table().inv[c.lg][c.lr] : table().fwd[c.lg][c.lr]);
+    cudaError_t e = ensure_smem(fn, (inverse ? 1 : 0) + (mul ? 4 : 0), c);
     if (e != cudaSuccess) return e;
     const uint64_t tiles = a.count * ((1ull << (a.logn - c.lg)) / c.tg);
     if (tiles == 0) return cudaSuccess;
     if (tiles > 0x7fffffffull) return cudaErrorInvalidValue;
     const unsigned threads = (unsigned)c.tg << (c.lg - c.lr);
     count_launch();
-    ProfScope prof(s, "ntt_%s_pass lg=%d lr=%d tg=%d", inverse ? "inv" : "fwd", c.lg, c.lr, c.tg);
+    ProfScope prof(s, "ntt_%s%s_pass lg=%d lr=%d tg=%d", inverse ? "inv" : "fwd", mul ? "_mul" : "", c.lg, c.lr,
+                   c.tg);
     fn<<<(unsigned)tiles, threads, smem_bytes(c), s>>>(a);
     return cudaGetLastError();
 }

@@ -251,6 +251,8 @@ __global__ void __launch_bounds__(max_threads(LR)) ntt_cluster_kernel(const __gr
         thread_role<LGA, LR>(t, gi, k);
         const uint64_t blk = tile_blk<LGA>(t, gi);
         load_global<LGA, LR, LO_FIRST>(v, lsrc, t, gi, round_base<LR>(k, LO_FIRST), vec_ok);
+        if (a.flags & kPreMul)
+            mul_operand<LGA, LR, LO_FIRST, false>(v, a.operand + (limb << logn), t, gi, k, cx, vec_ok);
         if constexpr (PRE) {
             PassTw<NRA, LR> pt;
             load_pass_tw<INV, LGA, LR, false>(std::make_integer_sequence<int, NRA>{}, pt, k, blk, 0, n, cx);
@@ -309,6 +311,8 @@ __global__ void __launch_bounds__(max_threads(LR)) ntt_cluster_kernel(const __gr
 #pragma unroll
         for (int i = 0; i < R; ++i) v[i] = INV ? csub_lazy(v[i], q) : csub_lazy(csub_lazy(v[i], q2), q);
     }
+    if (a.flags & kPostMul)
+        mul_operand<LGB, LR, LO_LAST, false>(v, a.operand + (limb << logn), tB, giB, kB, cx, vec_ok);
     store_global<LGB, LR, LO_LAST>(v, ldst, tB, giB, round_base<LR>(kB, LO_LAST), vec_ok);
 }
 

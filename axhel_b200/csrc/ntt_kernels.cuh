@@ -390,12 +390,31 @@ __device__ __forceinline__ void run_rounds(uint64_t (&v)[1 << LR], uint64_t* smg
 
 // ------------------------------------------------------------------ kernels
 
+// Dyadic product of the registers (round with register bits at LO) with the
+// multiplicand at the same positions: EltwiseMulModNative<4>
+// (eltwise-mul-mod.cpp:40-60), both operands in [0, 4q), result in [0, q).
+template <int LG, int LR, int LO, bool CG>
+__device__ __forceinline__ void mul_operand(uint64_t (&v)[1 << LR], const uint64_t* __restrict__ limb_m,
+                                            const Tile& t, uint32_t gi, uint32_t k, const ModCtx* cx, bool vec_ok)
+{
+    uint64_t m[1 << LR];
+    load_global<LG, LR, LO, CG>(m, limb_m, t, gi, round_base<LR>(k, LO),
+                                vec_ok && (reinterpret_cast<uintptr_t>(limb_m) & 15) == 0);
+    const uint64_t q = cx->q, mu = cx->mu;
+    const uint32_t shift = cx->shift;
+#pragma unroll
+    for (int i = 0; i < (1 << LR); ++i)
+        v[i] = barrett_mul(reduce_input<4>(v[i], q), reduce_input<4>(m[i], q), q, mu, shift);
+}
+
 // One tile of a pass: stages [s0, s0 + LG) of limb `limb`.  `sm` holds
-// 2^lgtg groups of 2^LG + 1 words; all threads of the CTA take part.
-template <bool INV, int LG, int LR, bool CG>
+// 2^lgtg groups of 2^LG words; all threads of the CTA take part.  With MUL,
+// flags kPreMul / kPostMul multiply by `operand` (MulMod<4>) after the load /
+// before the store.
+template <bool INV, int LG, int LR, bool CG, bool MUL = false>
 __device__ __forceinline__ void pass_tile(const uint64_t* src, uint64_t* dst, const ModCtx* cx, uint32_t logn,
                                           uint32_t s0, uint32_t lgtg, uint64_t limb, uint64_t tile_in_limb,
-                                          uint32_t flags, uint64_t* sm)
+                                          uint32_t flags, uint64_t* sm, const uint64_t* operand = nullptr)
 {
     constexpr int R = 1 << LR;
     constexpr int NR = num_rounds<LG, LR>();
@@ -419,12 +438,16 @@ __device__ __forceinline__ void pass_tile(const uint64_t* src, uint64_t* dst, co
 #pragma unroll
         for (int i = 0; i < R; ++i) v[i] = csub_lazy(v[i], q2);
     }
+    if constexpr (MUL)
+        if (flags & kPreMul) mul_operand<LG, LR, LO_FIRST, CG>(v, operand + (limb << logn), t, gi, k, cx, vec_ok);
     run_rounds<INV, LG, LR>(v, sm + (gi << LG), k, group_mask<LG, LR>(t.strided, lgtg, gi),
                             lane_shift(t.strided, lgtg), blk, s0, n, cx, q, q2, (flags & kLastPass) != 0);
     if (flags & kPostNorm) {
 #pragma unroll
         for (int i = 0; i < R; ++i) v[i] = INV ? csub_lazy(v[i], q) : csub_lazy(csub_lazy(v[i], q2), q);
     }
+    if constexpr (MUL)
+        if (flags & kPostMul) mul_operand<LG, LR, LO_LAST, CG>(v, operand + (limb << logn), t, gi, k, cx, vec_ok);
     store_global<LG, LR, LO_LAST>(v, ldst, t, gi, round_base<LR>(k, LO_LAST), vec_ok);
 }
 
@@ -438,6 +461,21 @@ __global__ void __launch_bounds__(max_threads(LR)) ntt_pass_kernel(const __grid_
     const uint64_t limb = tile >> lg_tiles;
     pass_tile<INV, LG, LR, false>(a.src, a.dst, a.ctx[limb_mod(limb, a.nctx)], a.logn, a.s0, lgtg, limb,
                                   tile & ((1ull << lg_tiles) - 1), a.flags, sm);
+}
+
+// The same pass with the dyadic product of kPreMul / kPostMul: a kernel of
+// its own, so that the product's registers do not count against the plain
+// passes.
+template <bool INV, int LG, int LR>
+__global__ void __launch_bounds__(max_threads(LR)) ntt_pass_mul_kernel(const __grid_constant__ PassArgs a)
+{
+    extern __shared__ uint64_t sm[];
+    const uint32_t lgtg = __ffs(a.tg) - 1;
+    const uint32_t lg_tiles = a.logn - LG - lgtg;
+    const uint64_t tile = blockIdx.x;
+    const uint64_t limb = tile >> lg_tiles;
+    pass_tile<INV, LG, LR, false, true>(a.src, a.dst, a.ctx[limb_mod(limb, a.nctx)], a.logn, a.s0, lgtg, limb,
+                                        tile & ((1ull << lg_tiles) - 1), a.flags, sm, a.operand);
 }
 
 // Fused column pass of an INTT -> op -> NTT chain: the inverse's last pass

@@ -188,9 +188,27 @@ def product_chain(logn=16, limbs=24, polys=32, reps=10, seed=5):
     ms_f, ms_s = timed(fused), timed(separate)
     same = torch.equal(y, z)
     mul.close()
+    # the two halves: forward then MulMod, MulMod then inverse
+    w = torch.empty_like(x)
+    mul_x = capi.Batch([dict(kind=capi.JOB_MUL, ntts=ntts, count=count, result=w.data_ptr(), operand=x.data_ptr(),
+                             vector=m.data_ptr(), in_f=4, out_f=1)])
+    halves = {}
+    for name, fused_fn, sep_fn in (
+            ("forward_mul", lambda: capi.forward_mul_batch(ntts, y.data_ptr(), x.data_ptr(), m.data_ptr(), count),
+             lambda: (capi.forward_batch(ntts, z.data_ptr(), x.data_ptr(), count, 4, 4), mul.launch(phased=True))),
+            ("mul_inverse", lambda: capi.mul_inverse_batch(ntts, y.data_ptr(), x.data_ptr(), m.data_ptr(), count, 1),
+             lambda: (mul_x.launch(phased=True), capi.inverse_batch(ntts, z.data_ptr(), w.data_ptr(), count, 2, 1)))):
+        if name == "forward_mul":
+            mul = capi.Batch([dict(kind=capi.JOB_MUL, ntts=ntts, count=count, result=z.data_ptr(),
+                                   operand=z.data_ptr(), vector=m.data_ptr(), in_f=4, out_f=1)])
+        a, b = timed(fused_fn), timed(sep_fn)
+        halves[name] = {"fused_ms": a, "separate_calls_ms": b, "speedup": b / a, "same_bits": torch.equal(y, z)}
+        if name == "forward_mul":
+            mul.close()
+    mul_x.close()
     return {"workload": f"NTT -> MulMod -> INTT, N=2^{logn}, {count} limbs ({limbs} primes of 50-59 bits)",
             "fused_ms": ms_f, "separate_calls_ms": ms_s, "speedup": ms_s / ms_f,
-            "fused_rate": 2 * count / (ms_f / 1e3), "unit": UNIT, "same_bits": same}
+            "fused_rate": 2 * count / (ms_f / 1e3), "unit": UNIT, "same_bits": same, **halves}
 
 
 # ------------------------------------------------------------------ uneven

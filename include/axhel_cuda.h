@@ -143,6 +143,26 @@ axhel_status_t axhel_cuda_ntt_chain_mul_batch(const axhel_ntt_t* ntts, uint64_t 
                                               const uint64_t* operand, const uint64_t* multiplicand, uint64_t count,
                                               uint64_t input_mod_factor, uint64_t output_mod_factor, void* stream);
 
+/* Forward transform then dyadic product over a batch (new; SEAL's
+ * dyadic_product_coeffmod on a freshly transformed operand, fused into the
+ * transform's last pass): replaces, per limb,
+ *   ComputeForward(r, x, in_f, 4); EltwiseMulMod(r, r, m, N, q, 4)
+ * (ntt.cpp:173-186, eltwise-mul-mod.cpp:18-94).  Inputs in [0, 4q);
+ * `multiplicand` (device, the layout of operand, values in [0, 4q), in the
+ * forward's bit-reversed order) must not be `result`.  Output [0, q). */
+axhel_status_t axhel_cuda_ntt_forward_mul_batch(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* result,
+                                                const uint64_t* operand, const uint64_t* multiplicand,
+                                                uint64_t count, void* stream);
+/* Dyadic product then inverse transform over a batch (new; the product
+ * fused into the inverse's first pass): replaces, per limb,
+ *   EltwiseMulMod(r, x, m, N, q, 4); ComputeInverse(r, r, 2, out_f)
+ * (eltwise-mul-mod.cpp:18-94, ntt.cpp:192-204).  Operand and `multiplicand`
+ * in [0, 4q), bit-reversed order; `multiplicand` must not be `result`.
+ * Output natural order, [0, 2q) for out_f == 2, else [0, q). */
+axhel_status_t axhel_cuda_ntt_mul_inverse_batch(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* result,
+                                                const uint64_t* operand, const uint64_t* multiplicand,
+                                                uint64_t count, uint64_t output_mod_factor, void* stream);
+
 /* Fused NTT -> MulMod -> INTT over a batch (new; the polynomial product in
  * evaluation form, SEAL's multiply_plain): one kernel chain replaces
  *   ComputeForward(x, x, in_f, 4); EltwiseMulMod(x, x, m, N, q, 4);

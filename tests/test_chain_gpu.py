@@ -109,3 +109,42 @@ def test_product_matches_call_sequence(cuda, oracle, n):
         np.testing.assert_array_equal(host(d), exp, err_msg=f"in place, out_f={out_f}")
     with pytest.raises(cuda.AxhelError):  # the multiplicand may not be the result
         cuda.product_batch(ntts, ptr(dm), ptr(d), ptr(dm), count, 4, 1)
+
+
+@pytest.mark.parametrize("n", [8, 1024, 4096, 16384, 65536, 131072])
+@pytest.mark.parametrize("count", [1, 5, 80])
+def test_forward_mul_and_mul_inverse_match_call_sequences(cuda, oracle, n, count):
+    """The dyadic product fused after a forward transform equals
+    ComputeForward(x, 4, 4) -> EltwiseMulMod(., m, 4), and fused ahead of an
+    inverse equals EltwiseMulMod(x, m, 4) -> ComputeInverse(2, out_f), limb by
+    limb; one limb and a few take the one-launch cluster form at 2^10..2^15,
+    80 limbs the pass form."""
+    if n * count > (1 << 21):
+        count = max(1, (1 << 21) // n)
+    L = 3
+    ms = moduli(oracle, n, L, 47)
+    ntts = [cuda.NTT(n, q, psi) for q, psi in ms]
+    tabs = [oracle.tables(n, q, psi) for q, psi in ms]
+    st = oracle.rng(SEED ^ 0xF3A1 ^ n ^ count)
+    x = np.concatenate([oracle.random_vector(st, n, 4 * ms[i % L][0]) for i in range(count)])
+    m = np.concatenate([oracle.random_vector(st, n, 4 * ms[i % L][0]) for i in range(count)])
+    segs = [slice(i * n, (i + 1) * n) for i in range(count)]
+    exp_f = np.concatenate([oracle.mul(oracle.forward(x[s], ms[i % L][0], tabs[i % L][0], 4, 4), m[s],
+                                       ms[i % L][0], 4) for i, s in enumerate(segs)])
+    d, o, dm = dev(x), dev_empty(x.size), dev(m)
+    cuda.forward_mul_batch(ntts, ptr(o), ptr(d), ptr(dm), count)
+    np.testing.assert_array_equal(host(o), exp_f, err_msg="forward then MulMod, out of place")
+    cuda.forward_mul_batch(ntts, ptr(d), ptr(d), ptr(dm), count)
+    np.testing.assert_array_equal(host(d), exp_f, err_msg="forward then MulMod, in place")
+    for out_f in (2, 1):
+        exp_i = np.concatenate([oracle.inverse(oracle.mul(x[s], m[s], ms[i % L][0], 4), ms[i % L][0],
+                                               tabs[i % L][1], tabs[i % L][2], 2, out_f) for i, s in enumerate(segs)])
+        d = dev(x)
+        cuda.mul_inverse_batch(ntts, ptr(o), ptr(d), ptr(dm), count, out_f)
+        np.testing.assert_array_equal(host(o), exp_i, err_msg=f"MulMod then inverse, out_f={out_f}")
+        cuda.mul_inverse_batch(ntts, ptr(d), ptr(d), ptr(dm), count, out_f)
+        np.testing.assert_array_equal(host(d), exp_i, err_msg=f"MulMod then inverse in place, out_f={out_f}")
+    with pytest.raises(cuda.AxhelError):  # the multiplicand may not be the result
+        cuda.forward_mul_batch(ntts, ptr(dm), ptr(d), ptr(dm), count)
+    with pytest.raises(cuda.AxhelError):
+        cuda.mul_inverse_batch(ntts, ptr(dm), ptr(d), ptr(dm), count, 1)
