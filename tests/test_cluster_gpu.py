@@ -116,3 +116,44 @@ def test_cluster_form_matches_pass_form(cuda, oracle, logn):
     np.testing.assert_array_equal(outs[0][0], outs[1][0])
     np.testing.assert_array_equal(outs[0][1], outs[1][1])
     np.testing.assert_array_equal(outs[0][0], oracle.forward(x, qs[0], tabs[0][0], 4, 4))
+
+
+@pytest.mark.parametrize("logn", [10, 12, 14, 16])
+@pytest.mark.parametrize("count", [1, 40])
+def test_transforms_on_8_byte_aligned_pointers(cuda, oracle, logn, count):
+    """Operands that are 8- but not 16-byte aligned (the reference accepts any
+    uint64_t pointer) take the scalar-access path of the pass and cluster
+    kernels and of the fused product: same bits as the oracle."""
+    import torch
+
+    n = 1 << logn
+    params, tabs, qs = moduli(oracle, n, 2)
+    ntts = [cuda.NTT(n, q, psi) for q, psi in params]
+    st = oracle.rng(SEED ^ 0xA11 ^ logn ^ count)
+    x = np.concatenate([oracle.random_vector(st, n, 4 * qs[i % 2]) for i in range(count)])
+    m = np.concatenate([oracle.random_vector(st, n, 4 * qs[i % 2]) for i in range(count)])
+    segs = [slice(i * n, (i + 1) * n) for i in range(count)]
+
+    def odd(a):  # a device copy starting 8 bytes into its allocation
+        t = torch.empty(a.size + 1, dtype=torch.int64, device="cuda")
+        t[1:].copy_(torch.from_numpy(a.view(np.int64)))
+        return t
+
+    def back(t):
+        return t[1:].cpu().numpy().view(np.uint64)
+
+    def p(t):
+        return t.data_ptr() + 8
+
+    d, o, dm = odd(x), odd(np.zeros_like(x)), odd(m)
+    assert p(d) % 16 == 8
+    ef = np.concatenate([oracle.forward(x[s], qs[i % 2], tabs[i % 2][0], 4, 4) for i, s in enumerate(segs)])
+    cuda.forward_batch(ntts, p(o), p(d), count, 4, 4)
+    np.testing.assert_array_equal(back(o), ef)
+    ei = np.concatenate([oracle.inverse(oracle.reduce(ef[s], qs[i % 2], 4, 2), qs[i % 2], tabs[i % 2][1],
+                                        tabs[i % 2][2], 2, 1) for i, s in enumerate(segs)])
+    cuda.inverse_batch(ntts, p(o), p(o), count, 4, 1)
+    np.testing.assert_array_equal(back(o), ei)
+    efm = np.concatenate([oracle.mul(ef[s], m[s], qs[i % 2], 4) for i, s in enumerate(segs)])
+    cuda.forward_mul_batch(ntts, p(o), p(d), p(dm), count)
+    np.testing.assert_array_equal(back(o), efm)
