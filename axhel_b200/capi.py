@@ -527,17 +527,22 @@ def plan_get(inverse, logn, count):
     return [(lg[i], lr[i], tg[i]) for i in range(npass.value)]
 
 
-def cluster_plan_set(inverse, logn, lga=0, lr=0, csize=0, max_limbs=0):
-    """Single-launch cluster form of a transform of up to `max_limbs` limbs
-    (lga = 0 restores the built-in choice; max_limbs = 0 turns it off)."""
-    check(lib().axhel_cuda_cluster_plan_set(int(inverse), logn, lga, lr, csize, max_limbs), "cluster_plan_set")
+CLUSTER_FORWARD, CLUSTER_INVERSE, CLUSTER_CHAIN, CLUSTER_PRODUCT = 0, 1, 2, 3
 
 
-def cluster_plan_get(inverse, logn):
-    """(lga, lr, csize, max_limbs) of the cluster form for N = 2^logn."""
+def cluster_plan_set(kind, logn, lga=0, lr=0, csize=0, max_limbs=0):
+    """Single-launch cluster form of up to `max_limbs` limbs for `kind`
+    (CLUSTER_FORWARD / _INVERSE transforms, or a bool for those two;
+    CLUSTER_CHAIN / _PRODUCT fused chains); lga = 0 restores the built-in
+    choice, max_limbs = 0 turns it off."""
+    check(lib().axhel_cuda_cluster_plan_set(int(kind), logn, lga, lr, csize, max_limbs), "cluster_plan_set")
+
+
+def cluster_plan_get(kind, logn):
+    """(lga, lr, csize, max_limbs) of the cluster form of `kind` for N = 2^logn."""
     a, b, c = u32(), u32(), u32()
     m = u64()
-    check(lib().axhel_cuda_cluster_plan_get(int(inverse), logn, C.byref(a), C.byref(b), C.byref(c), C.byref(m)),
+    check(lib().axhel_cuda_cluster_plan_get(int(kind), logn, C.byref(a), C.byref(b), C.byref(c), C.byref(m)),
           "cluster_plan_get")
     return a.value, b.value, c.value, m.value
 

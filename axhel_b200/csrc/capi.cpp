@@ -463,7 +463,8 @@ axhel_status_t transform(bool inverse, const axhel_ntt_t* ntts, uint64_t n_ntts,
     // a few limbs: both passes in one launch, one cluster per limb (unless a
     // pass plan was set explicitly for this degree)
     ClusterCfg cc;
-    if (!plan_overridden(inverse, a.logn) && cluster_plan(inverse, a.logn, count, &cc)) {
+    if (!plan_overridden(inverse, a.logn) &&
+        cluster_plan(inverse ? kClusterInverse : kClusterForward, a.logn, count, &cc)) {
         a.src = operand;
         a.dst = result;
         a.s0 = 0;
@@ -490,6 +491,20 @@ axhel_status_t chain(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* result,
     if (op == kChainFma && !scalars) return fail(AXHEL_ERR_INVALID, "null scalars");
     c.pass.count = count;
     const uint32_t logn = c.pass.logn;
+    // a few limbs: the whole chain in one launch, one cluster per limb
+    ClusterCfg cc;
+    if (!plan_overridden(true, logn) && cluster_plan(kClusterChain, logn, count, &cc)) {
+        c.pass.src = operand;
+        c.pass.dst = result;
+        c.pass.flags = (in_f == 4 ? (uint32_t)kPreCsub2q : 0u) | (out_f != 4 ? (uint32_t)kPostNorm : 0u);
+        c.operand = vec;
+        c.op = op;
+        c.op_factor = 2;
+        if (op == kChainFma)
+            for (uint64_t i = 0; i < n_ntts; ++i) c.scalar[i] = scalars[i];
+        const cudaError_t e = launch_ntt_cluster_fused(false, cc, c, S(stream));
+        return e == cudaSuccess ? AXHEL_OK : cuda_fail(e, "chain (cluster)");
+    }
     const NttPlan inv = plan_for(true, logn, count);
     // forward passes after the fused one: the inverse's earlier passes, reversed
     NttPlan fwd{};
@@ -563,6 +578,18 @@ axhel_status_t product(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* resul
     if (vec == result) return fail(AXHEL_ERR_INVALID, "the multiplicand must not be the result buffer");
     c.pass.count = count;
     const uint32_t logn = c.pass.logn;
+    // a few limbs: the whole product in one launch, one cluster per limb
+    ClusterCfg cc;
+    if (!plan_overridden(true, logn) && cluster_plan(kClusterProduct, logn, count, &cc)) {
+        c.pass.src = operand;
+        c.pass.dst = result;
+        c.pass.flags = out_f != 2 ? (uint32_t)kPostNorm : 0u;
+        c.operand = vec;
+        c.op = kChainMul;
+        c.op_factor = 4;
+        const cudaError_t e = launch_ntt_cluster_fused(true, cc, c, S(stream));
+        return e == cudaSuccess ? AXHEL_OK : cuda_fail(e, "product (cluster)");
+    }
     const NttPlan inv = plan_for(true, logn, count);
     cudaStream_t s = S(stream);
     // forward passes before the fused one: the inverse plan's passes npass-1 .. 1
@@ -793,26 +820,28 @@ axhel_status_t axhel_cuda_plan_get(int inverse, uint32_t logn, uint64_t count, u
     return AXHEL_OK;
 }
 
-axhel_status_t axhel_cuda_cluster_plan_set(int inverse, uint32_t logn, uint32_t lga, uint32_t lr, uint32_t csize,
+axhel_status_t axhel_cuda_cluster_plan_set(int kind, uint32_t logn, uint32_t lga, uint32_t lr, uint32_t csize,
                                            uint64_t max_limbs)
 {
+    if (kind < 0 || kind > 3) return fail(AXHEL_ERR_INVALID, "cluster kind: 0 forward, 1 inverse, 2 chain, 3 product");
     if (logn < 10 || logn > 17) return fail(AXHEL_ERR_UNSUPPORTED, "cluster form covers log degree 10..17");
     if (lga == 0) {
-        cluster_plan_override(inverse != 0, logn, nullptr);
+        cluster_plan_override(kind, logn, nullptr);
         return AXHEL_OK;
     }
     const ClusterCfg c{(int)lga, (int)lr, (int)csize, max_limbs};
-    if (max_limbs && !cluster_cfg_valid(logn, c))
+    if (max_limbs && !cluster_cfg_valid(kind, logn, c))
         return fail(AXHEL_ERR_UNSUPPORTED, "cluster configuration not compiled or not valid for this degree");
-    cluster_plan_override(inverse != 0, logn, &c);
+    cluster_plan_override(kind, logn, &c);
     return AXHEL_OK;
 }
 
-axhel_status_t axhel_cuda_cluster_plan_get(int inverse, uint32_t logn, uint32_t* lga, uint32_t* lr, uint32_t* csize,
+axhel_status_t axhel_cuda_cluster_plan_get(int kind, uint32_t logn, uint32_t* lga, uint32_t* lr, uint32_t* csize,
                                            uint64_t* max_limbs)
 {
     if (!lga || !lr || !csize || !max_limbs) return fail(AXHEL_ERR_INVALID, "null output");
-    const ClusterCfg c = cluster_plan_current(inverse != 0, logn);
+    if (kind < 0 || kind > 3) return fail(AXHEL_ERR_INVALID, "cluster kind: 0 forward, 1 inverse, 2 chain, 3 product");
+    const ClusterCfg c = cluster_plan_current(kind, logn);
     *lga = (uint32_t)c.lga;
     *lr = (uint32_t)c.lr;
     *csize = (uint32_t)c.csize;

@@ -80,19 +80,23 @@ cudaError_t launch_chain_pass(const PassCfg& inv_cfg, const ChainArgs& a, cudaSt
 cudaError_t launch_product_pass(const PassCfg& cfg, const ChainArgs& a, cudaStream_t s);
 bool pass_supported(const PassCfg& cfg);
 
-// Single-launch transform of a few limbs, one thread-block cluster per limb
-// (ntt_cluster.cu): first-pass stages, register stages, CTAs per cluster,
-// and the largest limb count that takes this form.
+// Single-launch forms of a few limbs, one thread-block cluster per limb
+// (ntt_cluster.cu): first-pass (transforms) or row (fused chains) stages,
+// register stages, CTAs per cluster, and the largest limb count that takes
+// this form; per kind: forward, inverse, INTT -> op -> NTT chain, NTT ->
+// MulMod -> INTT product.
+enum ClusterKind : int { kClusterForward = 0, kClusterInverse = 1, kClusterChain = 2, kClusterProduct = 3 };
 struct ClusterCfg {
     int lga, lr, csize;
     uint64_t max_limbs;
 };
-bool cluster_cfg_valid(uint32_t logn, const ClusterCfg& c);
-// The cluster form for (dir, logN, limbs), if it applies.
-bool cluster_plan(bool inverse, uint32_t logn, uint64_t count, ClusterCfg* out);
-void cluster_plan_override(bool inverse, uint32_t logn, const ClusterCfg* c);  // nullptr clears
-ClusterCfg cluster_plan_current(bool inverse, uint32_t logn);
+bool cluster_cfg_valid(int kind, uint32_t logn, const ClusterCfg& c);
+// The cluster form for (kind, logN, limbs), if it applies.
+bool cluster_plan(int kind, uint32_t logn, uint64_t count, ClusterCfg* out);
+void cluster_plan_override(int kind, uint32_t logn, const ClusterCfg* c);  // nullptr clears
+ClusterCfg cluster_plan_current(int kind, uint32_t logn);
 cudaError_t launch_ntt_cluster(bool inverse, const ClusterCfg& c, const PassArgs& a, cudaStream_t s);
+cudaError_t launch_ntt_cluster_fused(bool product, const ClusterCfg& c, const ChainArgs& a, cudaStream_t s);
 
 // Planner (plan.cpp): default plan for (dir, logN, limbs); autotuned table if loaded.
 NttPlan plan_for(bool inverse, uint32_t logn, uint64_t limbs);

@@ -316,11 +316,205 @@ __global__ void __launch_bounds__(max_threads(LR)) ntt_cluster_kernel(const __gr
     store_global<LGB, LR, LO_LAST>(v, ldst, tB, giB, round_base<LR>(kB, LO_LAST), vec_ok);
 }
 
+// ---- fused chains in one launch
+//
+// INTT -> MulMod/FMAMod -> NTT (the chain kernels' job) and NTT -> MulMod ->
+// INTT (the product kernels' job) of one limb per cluster, in three phases
+// with two exchanges through distributed shared memory.  With N = 2^(LGR +
+// LGC), "rows" are the 2^LGC contiguous groups of 2^LGR words and "columns"
+// the 2^LGR groups of stride 2^LGR; CTA k holds row chunk k or the columns
+// [k, k+1) * 2^(LGR-c).
+//   chain:   inverse rows (stages 0..LGR-1) | columns: inverse stages
+//            LGR..logn-1 with N^-1, the op, forward stages 0..LGC-1 | forward
+//            rows (stages LGC..logn-1)
+//   product: forward columns (stages 0..LGC-1) | rows: forward stages
+//            LGC..logn-1, MulMod<4>, inverse stages 0..LGR-1 | inverse columns
+//            (stages LGR..logn-1 with N^-1)
+// The middle phase is the chain / product tile's (the inverse's last round
+// and the forward's first hold the same register bits, and the reverse), so
+// every result equals the three-launch chains and the call sequences they
+// replace.  Shared memory: 3 * N/C words (round exchanges, the first landing
+// area, the second landing area).
+
+namespace {
+
+// Registers of round LO of tile t (LG-stage groups) into the landing area of
+// their owners in the next phase: rows (chunk owners) or columns.
+template <int LG, int LR, int LO, bool TO_COLUMNS, int LGR>
+__device__ __forceinline__ void scatter(const uint64_t (&v)[1 << LR], const Tile& t, uint32_t gi, uint32_t k,
+                                        uint32_t lgchunk, uint32_t lgtg_cols, uint64_t* landing,
+                                        cg::cluster_group& cl)
+{
+    const uint32_t rb = round_base<LR>(k, LO);
+#pragma unroll
+    for (int i = 0; i < (1 << LR); ++i) {
+        const uint64_t r = rb + ((uint64_t)i << LO);
+        const uint64_t p = t.strided ? t.base + gi + (r << t.lgS) : t.base + ((uint64_t)gi << LG) + r;
+        uint32_t owner, off;
+        landing_of<TO_COLUMNS, LGR>(p, lgchunk, lgtg_cols, owner, off);
+        cl.map_shared_rank(landing, owner)[off] = v[i];
+    }
+}
+
+// The tile itself, compacted, as a landing area: columns as rows of
+// 2^lgtg_cols words, row chunks as they are.
+__device__ __forceinline__ Tile landing_tile(Tile t, uint32_t lgtg_cols)
+{
+    t.base = 0;
+    if (t.strided) t.lgS = lgtg_cols;
+    return t;
+}
+
+}  // namespace
+
+template <bool PRODUCT, int LGR, int LGC, int LR>
+__global__ void __launch_bounds__(max_threads(LR)) ntt_cluster_fused_kernel(const __grid_constant__ ChainArgs c)
+{
+    extern __shared__ uint64_t sm[];
+    constexpr int R = 1 << LR;
+    constexpr uint32_t logn = LGR + LGC;
+    constexpr int NRR = num_rounds<LGR, LR>(), NRC = num_rounds<LGC, LR>();
+    const PassArgs& a = c.pass;
+    cg::cluster_group cl = cg::this_cluster();
+    cluster_arrive_relaxed();
+    const uint32_t rank = cl.block_rank();
+    const uint32_t lc = __ffs(cl.num_blocks()) - 1;
+    const uint64_t limb = blockIdx.x >> lc;
+    const uint32_t lgchunk = logn - lc;
+    const uint32_t lgtgR = LGC - lc, lgtgC = LGR - lc;  // rows / columns per CTA (log2)
+    uint64_t* scratch = sm;
+    uint64_t* landing1 = sm + (1u << lgchunk);
+    uint64_t* landing2 = sm + (2u << lgchunk);
+    const uint32_t mi = limb_mod(limb, a.nctx);
+    const ModCtx* cx = a.ctx[mi];
+    const uint64_t q = cx->q, q2 = cx->q2, mu = cx->mu;
+    const uint32_t shift = cx->shift;
+    const uint64_t n = 1ull << logn;
+    const uint64_t* lsrc = a.src + (limb << logn);
+    uint64_t* ldst = a.dst + (limb << logn);
+    const uint64_t* lop = c.operand ? c.operand + (limb << logn) : nullptr;
+    const bool vec_ok = ((reinterpret_cast<uintptr_t>(a.src) | reinterpret_cast<uintptr_t>(a.dst) |
+                          reinterpret_cast<uintptr_t>(c.operand)) & 15) == 0;
+    const Tile tR = make_tile<LGR>(0, lgtgR, limb, rank);
+    const Tile tC = make_tile<LGC>(LGR, lgtgC, limb, rank);
+    uint64_t v[R];
+    uint32_t gi, k;
+
+    if constexpr (!PRODUCT) {
+        // ---- inverse rows: stages [0, LGR)
+        thread_role<LGR, LR>(tR, gi, k);
+        load_global<LGR, LR, round_lo<true, LGR, LR, 0>()>(v, lsrc, tR, gi,
+                                                           round_base<LR>(k, round_lo<true, LGR, LR, 0>()), vec_ok);
+        if (a.flags & kPreCsub2q) {
+#pragma unroll
+            for (int i = 0; i < R; ++i) v[i] = csub_lazy(v[i], q2);
+        }
+        run_rounds<true, LGR, LR>(v, scratch + (gi << LGR), k, group_mask<LGR, LR>(false, lgtgR, gi),
+                                  lane_shift(false, lgtgR), tile_blk<LGR>(tR, gi), 0, n, cx, q, q2, false);
+        cluster_wait();
+        scatter<LGR, LR, round_lo<true, LGR, LR, NRR - 1>(), true, LGR>(v, tR, gi, k, lgchunk, lgtgC, landing1, cl);
+        cl.sync();
+
+        // ---- columns: inverse stages [LGR, logn) with N^-1, the op, forward stages [0, LGC)
+        constexpr int LO_IN = round_lo<true, LGC, LR, 0>();
+        constexpr int LO_MID = round_lo<true, LGC, LR, NRC - 1>();
+        static_assert(LO_MID == round_lo<false, LGC, LR, 0>(), "inverse last round and forward first round differ");
+        thread_role<LGC, LR>(tC, gi, k);
+        uint64_t* smg = scratch + (gi << LGC);
+        const uint32_t hmask = group_mask<LGC, LR>(true, lgtgC, gi), lsh = lane_shift(true, lgtgC);
+        load_global<LGC, LR, LO_IN>(v, landing1, landing_tile(tC, lgtgC), gi, round_base<LR>(k, LO_IN), true);
+        run_rounds<true, LGC, LR>(v, smg, k, hmask, lsh, tile_blk<LGC>(tC, gi), LGR, n, cx, q, q2, true);
+        const uint32_t rb = round_base<LR>(k, LO_MID);
+        // EltwiseMulModNative<2> / EltwiseFMAModNative<2> on the inverse's [0, 2q) output
+        if (c.op == kChainMul) {
+            uint64_t m[R];
+            load_global<LGC, LR, LO_MID>(m, lop, tC, gi, rb, vec_ok);
+#pragma unroll
+            for (int i = 0; i < R; ++i)
+                v[i] = barrett_mul(reduce_input<2>(v[i], q), reduce_input<2>(m[i], q), q, mu, shift);
+        } else if (c.op == kChainFma) {
+            const uint64_t sc = reduce_input<2>(c.scalar[mi], q);
+#pragma unroll
+            for (int i = 0; i < R; ++i) v[i] = barrett_mul(reduce_input<2>(v[i], q), sc, q, mu, shift);
+            if (lop) {
+                uint64_t m[R];
+                load_global<LGC, LR, LO_MID>(m, lop, tC, gi, rb, vec_ok);
+#pragma unroll
+                for (int i = 0; i < R; ++i) v[i] = csub(v[i] + reduce_input<2>(m[i], q), q);
+            }
+        }
+        fwd_stages<LGC, LR, 0>(v, rb, 0, 0, cx->fwd, q, q2);
+        fwd_rest<LGC, LR>(std::make_integer_sequence<int, NRC - 1>{}, v, smg, k, hmask, lsh, 0, 0, cx->fwd, q, q2);
+        scatter<LGC, LR, round_lo<false, LGC, LR, NRC - 1>(), false, LGR>(v, tC, gi, k, lgchunk, lgtgC, landing2,
+                                                                           cl);
+        cl.sync();
+
+        // ---- forward rows: stages [LGC, logn)
+        thread_role<LGR, LR>(tR, gi, k);
+        load_global<LGR, LR, round_lo<false, LGR, LR, 0>()>(v, landing2, landing_tile(tR, lgtgC), gi,
+                                                            round_base<LR>(k, round_lo<false, LGR, LR, 0>()), true);
+        run_rounds<false, LGR, LR>(v, scratch + (gi << LGR), k, group_mask<LGR, LR>(false, lgtgR, gi),
+                                   lane_shift(false, lgtgR), tile_blk<LGR>(tR, gi), LGC, n, cx, q, q2, false);
+        if (a.flags & kPostNorm) {
+#pragma unroll
+            for (int i = 0; i < R; ++i) v[i] = csub_lazy(csub_lazy(v[i], q2), q);
+        }
+        store_global<LGR, LR, round_lo<false, LGR, LR, NRR - 1>()>(
+            v, ldst, tR, gi, round_base<LR>(k, round_lo<false, LGR, LR, NRR - 1>()), vec_ok);
+    } else {
+        // ---- forward columns: stages [0, LGC)
+        thread_role<LGC, LR>(tC, gi, k);
+        load_global<LGC, LR, round_lo<false, LGC, LR, 0>()>(v, lsrc, tC, gi,
+                                                            round_base<LR>(k, round_lo<false, LGC, LR, 0>()), vec_ok);
+        run_rounds<false, LGC, LR>(v, scratch + (gi << LGC), k, group_mask<LGC, LR>(true, lgtgC, gi),
+                                   lane_shift(true, lgtgC), tile_blk<LGC>(tC, gi), 0, n, cx, q, q2, false);
+        cluster_wait();
+        scatter<LGC, LR, round_lo<false, LGC, LR, NRC - 1>(), false, LGR>(v, tC, gi, k, lgchunk, lgtgC, landing1,
+                                                                           cl);
+        cl.sync();
+
+        // ---- rows: forward stages [LGC, logn), MulMod<4>, inverse stages [0, LGR)
+        constexpr int LO_IN = round_lo<false, LGR, LR, 0>();
+        constexpr int LO_MID = round_lo<false, LGR, LR, NRR - 1>();
+        static_assert(LO_MID == round_lo<true, LGR, LR, 0>(), "forward last round and inverse first round differ");
+        thread_role<LGR, LR>(tR, gi, k);
+        uint64_t* smg = scratch + (gi << LGR);
+        const uint32_t hmask = group_mask<LGR, LR>(false, lgtgR, gi), lsh = lane_shift(false, lgtgR);
+        const uint64_t blk = tile_blk<LGR>(tR, gi);
+        load_global<LGR, LR, LO_IN>(v, landing1, landing_tile(tR, lgtgC), gi, round_base<LR>(k, LO_IN), true);
+        run_rounds<false, LGR, LR>(v, smg, k, hmask, lsh, blk, LGC, n, cx, q, q2, false);
+        {
+            uint64_t m[R];
+            load_global<LGR, LR, LO_MID>(m, lop, tR, gi, round_base<LR>(k, LO_MID), vec_ok);
+#pragma unroll
+            for (int i = 0; i < R; ++i)
+                v[i] = barrett_mul(reduce_input<4>(v[i], q), reduce_input<4>(m[i], q), q, mu, shift);
+        }
+        run_rounds<true, LGR, LR>(v, smg, k, hmask, lsh, blk, 0, n, cx, q, q2, false);
+        scatter<LGR, LR, round_lo<true, LGR, LR, NRR - 1>(), true, LGR>(v, tR, gi, k, lgchunk, lgtgC, landing2, cl);
+        cl.sync();
+
+        // ---- inverse columns: stages [LGR, logn) with N^-1
+        constexpr int LO_C = round_lo<true, LGC, LR, 0>();
+        constexpr int LO_OUT = round_lo<true, LGC, LR, NRC - 1>();
+        thread_role<LGC, LR>(tC, gi, k);
+        load_global<LGC, LR, LO_C>(v, landing2, landing_tile(tC, lgtgC), gi, round_base<LR>(k, LO_C), true);
+        run_rounds<true, LGC, LR>(v, scratch + (gi << LGC), k, group_mask<LGC, LR>(true, lgtgC, gi),
+                                  lane_shift(true, lgtgC), tile_blk<LGC>(tC, gi), LGR, n, cx, q, q2, true);
+        if (a.flags & kPostNorm) {
+#pragma unroll
+            for (int i = 0; i < R; ++i) v[i] = csub_lazy(v[i], q);
+        }
+        store_global<LGC, LR, LO_OUT>(v, ldst, tC, gi, round_base<LR>(k, LO_OUT), vec_ok);
+    }
+}
+
 // ------------------------------------------------------------------ host side
 
 namespace {
 
 using ClusterFn = void (*)(const PassArgs);
+using FusedFn = void (*)(const ChainArgs);
 
 struct Entry {
     int lga, lgb, lr;
@@ -356,18 +550,62 @@ const Entry* find_entry(int lga, int lgb, int lr)
     return nullptr;
 }
 
-// Built-in choice per direction and log2 N (10..17): first-pass stages,
-// register stages, cluster size, and the largest limb count that takes the
-// cluster form -- the fastest on a B200 by device time per transform
-// (CUDA-graph replay).  One limb, forward / inverse, against the pass form:
-// 2^10 3.0 / 3.2 us (6.7 / 4.7), 2^11 3.2 / 3.3 (5.0 / 5.6), 2^12 3.4 / 3.5
-// (6.5 / 6.6), 2^13 3.7 / 3.7 (6.7 / 7.2), 2^14 4.7 / 4.9 (7.1 / 7.7), 2^15
-// 7.0 / 7.3 (7.6 / 7.5).  From 2^16 one limb's work needs more than the 16
-// SMs of a cluster and the pass form (all SMs) is faster, as it is from 16 /
-// 4 limbs up at 2^14 / 2^15; at 2^10..2^13 the cluster form is still ahead
-// at 64 limbs, the largest count measured.
-ClusterCfg default_cfg(bool inverse, uint32_t logn)
+// The fused chain / product kernels: (row stages, column stages, register stages).
+struct FusedEntry {
+    int lgr, lgc, lr;
+    FusedFn fn[2];  // [product]
+};
+
+template <int A, int B, int L>
+FusedEntry fused_entry()
 {
+    return FusedEntry{A, B, L, {ntt_cluster_fused_kernel<false, A, B, L>, ntt_cluster_fused_kernel<true, A, B, L>}};
+}
+
+const FusedEntry kFused[] = {
+    fused_entry<5, 5, 2>(), fused_entry<6, 5, 2>(), fused_entry<5, 6, 2>(), fused_entry<6, 6, 2>(),
+    fused_entry<7, 6, 2>(), fused_entry<6, 7, 2>(), fused_entry<7, 7, 2>(), fused_entry<8, 7, 2>(),
+    fused_entry<7, 8, 2>(),
+};
+constexpr int kNumFused = sizeof(kFused) / sizeof(kFused[0]);
+
+const FusedEntry* find_fused(int lgr, int lgc, int lr)
+{
+    for (const FusedEntry& e : kFused)
+        if (e.lgr == lgr && e.lgc == lgc && e.lr == lr) return &e;
+    return nullptr;
+}
+
+// Built-in choice per kind and log2 N (10..17): first-pass (transforms) or
+// row (fused chains) stages, register stages, cluster size, and the largest
+// limb count that takes the cluster form -- the fastest on a B200 by device
+// time per call (CUDA-graph replay).  Transforms of one limb, forward /
+// inverse, against the pass form: 2^10 3.0 / 3.2 us (6.7 / 4.7), 2^11 3.2 /
+// 3.3 (5.0 / 5.6), 2^12 3.4 / 3.5 (6.5 / 6.6), 2^13 3.7 / 3.7 (6.7 / 7.2),
+// 2^14 4.7 / 4.9 (7.1 / 7.7), 2^15 7.0 / 7.3 (7.6 / 7.5).  From 2^16 one
+// limb's work needs more than the 16 SMs of a cluster and the pass form (all
+// SMs) is faster, as it is from 16 / 4 limbs up at 2^14 / 2^15; at
+// 2^10..2^13 the cluster form is still ahead at 64 limbs, the largest count
+// measured.
+ClusterCfg default_cfg(int kind, uint32_t logn)
+{
+    // Fused chain / product of one limb against the three pass launches:
+    // 2^10 5.7 / 6.0 us (7.8 / 7.5), 2^11 6.1 / 5.7 (9.8 / 9.0), 2^12 6.5 /
+    // 6.7 (11.4 / 11.2), 2^13 7.0 / 6.3 (11.6 / 12.1), 2^14 8.7 / 8.5 (13.3 /
+    // 14.9), 2^15 12.8 / 13.0 (12.8 / 14.1); still ahead at 64 limbs up to
+    // 2^12, behind from about 32 / 8 / 8 limbs at 2^13 / 2^14 / 2^15.
+    if (kind == kClusterChain || kind == kClusterProduct) {
+        switch (logn) {
+        case 10: return ClusterCfg{5, 2, 4, 64};
+        case 11: return ClusterCfg{6, 2, 8, 64};
+        case 12: return ClusterCfg{6, 2, 8, 64};
+        case 13: return ClusterCfg{7, 2, 16, 16};
+        case 14: return ClusterCfg{7, 2, 16, 8};
+        case 15: return ClusterCfg{7, 2, 16, 4};
+        default: return ClusterCfg{0, 0, 0, 0};
+        }
+    }
+    const bool inverse = kind == kClusterInverse;
     switch (logn) {
     case 10: return ClusterCfg{5, 2, 2, 64};
     case 11: return ClusterCfg{6, 2, 4, 64};
@@ -382,64 +620,98 @@ ClusterCfg default_cfg(bool inverse, uint32_t logn)
 }
 
 std::mutex g_mu;
-bool g_set[2][18] = {};
-ClusterCfg g_over[2][18] = {};
-// per entry and device: shared-memory / cluster-size attributes set
+bool g_set[4][18] = {};
+ClusterCfg g_over[4][18] = {};
+// per kernel and device: shared-memory / cluster-size attributes set
 std::mutex g_attr_mu;
 uint64_t g_attr_done[kNumEntries][2][2] = {};
+uint64_t g_fused_attr_done[kNumFused][2] = {};
 
 int entry_index(const Entry* e) { return (int)(e - kEntries); }
+int fused_index(const FusedEntry* e) { return (int)(e - kFused); }
+
+bool fused_kind(int kind) { return kind == kClusterChain || kind == kClusterProduct; }
+
+// Sets the launch attributes of `fn` once per device (bit `dev` of `done`).
+cudaError_t ensure_attrs(const void* fn, uint64_t& done, int dev)
+{
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    if (done >> dev & 1) return cudaSuccess;
+    cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (err == cudaSuccess) err = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (err == cudaSuccess) done |= 1ull << dev;
+    return err;
+}
+
+cudaError_t launch_cluster(const void* fn, void* args, uint64_t blocks, uint32_t threads, size_t smem, int csize,
+                           cudaStream_t s)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)blocks, 1, 1);
+    cfg.blockDim = dim3(threads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)csize;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    void* argv[] = {args};
+    const cudaError_t err = cudaLaunchKernelExC(&cfg, fn, argv);
+    return err != cudaSuccess ? err : cudaGetLastError();
+}
 
 }  // namespace
 
-bool cluster_cfg_valid(uint32_t logn, const ClusterCfg& c)
+bool cluster_cfg_valid(int kind, uint32_t logn, const ClusterCfg& c)
 {
-    if (logn < 10 || logn > 17 || c.max_limbs == 0) return false;
+    if (kind < 0 || kind > 3 || logn < 10 || logn > 17 || c.max_limbs == 0) return false;
     const int lgb = (int)logn - c.lga;
-    if (!find_entry(c.lga, lgb, c.lr)) return false;
+    const bool fused = fused_kind(kind);
+    if (fused ? !find_fused(c.lga, lgb, c.lr) : !find_entry(c.lga, lgb, c.lr)) return false;
     if (c.csize < 2 || c.csize > 16 || (c.csize & (c.csize - 1))) return false;
     const int lc = __builtin_ctz(c.csize);
     if (lc > c.lga || lc > lgb) return false;
     const int lgthreads = (int)logn - lc - c.lr;
     if (lgthreads < 5 || (1 << lgthreads) > max_threads(c.lr)) return false;
-    return 2 * (sizeof(uint64_t) << (logn - lc)) <= 227 * 1024;
+    return (fused ? 3 : 2) * (sizeof(uint64_t) << (logn - lc)) <= 227 * 1024;
 }
 
-bool cluster_plan(bool inverse, uint32_t logn, uint64_t count, ClusterCfg* out)
+bool cluster_plan(int kind, uint32_t logn, uint64_t count, ClusterCfg* out)
 {
-    if (logn < 10 || logn > 17) return false;
+    if (kind < 0 || kind > 3 || logn < 10 || logn > 17) return false;
     ClusterCfg c;
     {
         std::lock_guard<std::mutex> lk(g_mu);
-        c = g_set[inverse][logn] ? g_over[inverse][logn] : default_cfg(inverse, logn);
+        c = g_set[kind][logn] ? g_over[kind][logn] : default_cfg(kind, logn);
     }
-    if (count == 0 || count > c.max_limbs || !cluster_cfg_valid(logn, c)) return false;
+    if (count == 0 || count > c.max_limbs || !cluster_cfg_valid(kind, logn, c)) return false;
     *out = c;
     return true;
 }
 
-void cluster_plan_override(bool inverse, uint32_t logn, const ClusterCfg* c)
+void cluster_plan_override(int kind, uint32_t logn, const ClusterCfg* c)
 {
-    if (logn > 17) return;
+    if (kind < 0 || kind > 3 || logn > 17) return;
     std::lock_guard<std::mutex> lk(g_mu);
-    g_set[inverse][logn] = c != nullptr;
-    if (c) g_over[inverse][logn] = *c;
+    g_set[kind][logn] = c != nullptr;
+    if (c) g_over[kind][logn] = *c;
 }
 
-ClusterCfg cluster_plan_current(bool inverse, uint32_t logn)
+ClusterCfg cluster_plan_current(int kind, uint32_t logn)
 {
-    if (logn > 17) return ClusterCfg{0, 0, 0, 0};
+    if (kind < 0 || kind > 3 || logn > 17) return ClusterCfg{0, 0, 0, 0};
     std::lock_guard<std::mutex> lk(g_mu);
-    return g_set[inverse][logn] ? g_over[inverse][logn] : default_cfg(inverse, logn);
+    return g_set[kind][logn] ? g_over[kind][logn] : default_cfg(kind, logn);
 }
 
 cudaError_t launch_ntt_cluster(bool inverse, const ClusterCfg& c, const PassArgs& a, cudaStream_t s)
 {
-    if (!cluster_cfg_valid(a.logn, c)) return cudaErrorInvalidValue;
-    const int lgb = (int)a.logn - c.lga;
-    const Entry* e = find_entry(c.lga, lgb, c.lr);
+    if (!cluster_cfg_valid(inverse ? kClusterInverse : kClusterForward, a.logn, c)) return cudaErrorInvalidValue;
+    const Entry* e = find_entry(c.lga, (int)a.logn - c.lga, c.lr);
     const int lc = __builtin_ctz(c.csize);
-    const size_t smem = 2 * (sizeof(uint64_t) << (a.logn - lc));
     const uint64_t blocks = a.count * (uint64_t)c.csize;
     if (a.count == 0) return cudaSuccess;
     if (blocks > 0x7fffffffull) return cudaErrorInvalidValue;
@@ -448,42 +720,40 @@ cudaError_t launch_ntt_cluster(bool inverse, const ClusterCfg& c, const PassArgs
     // most one CTA per SM (measured faster there up to N = 2^14, slower with
     // several clusters per SM and at 2^15).
     const bool pre = e->fn[inverse][1] && a.logn <= 14 && blocks <= (uint64_t)sm_count();
-    ClusterFn fn = e->fn[inverse][pre];
+    const void* fn = reinterpret_cast<const void*>(e->fn[inverse][pre]);
     int dev = 0;
     cudaError_t err = cudaGetDevice(&dev);
     if (err != cudaSuccess) return err;
     if (dev >= 64) return cudaErrorInvalidDevice;
-    {
-        std::lock_guard<std::mutex> lk(g_attr_mu);
-        uint64_t& done = g_attr_done[entry_index(e)][inverse][pre];
-        if (!(done >> dev & 1)) {
-            err = cudaFuncSetAttribute(reinterpret_cast<const void*>(fn),
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-            if (err == cudaSuccess)
-                err = cudaFuncSetAttribute(reinterpret_cast<const void*>(fn),
-                                           cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-            if (err != cudaSuccess) return err;
-            done |= 1ull << dev;
-        }
-    }
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)blocks, 1, 1);
-    cfg.blockDim = dim3(1u << (a.logn - lc - c.lr), 1, 1);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = (unsigned)c.csize;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    err = ensure_attrs(fn, g_attr_done[entry_index(e)][inverse][pre], dev);
+    if (err != cudaSuccess) return err;
     count_launch();
     ProfScope prof(s, "ntt_%s_cluster lga=%d lr=%d c=%d%s", inverse ? "inv" : "fwd", c.lga, c.lr, c.csize,
                    pre ? " prefetch" : "");
-    void* args[] = {const_cast<PassArgs*>(&a)};
-    err = cudaLaunchKernelExC(&cfg, reinterpret_cast<const void*>(fn), args);
-    return err != cudaSuccess ? err : cudaGetLastError();
+    return launch_cluster(fn, const_cast<PassArgs*>(&a), blocks, 1u << (a.logn - lc - c.lr),
+                          2 * (sizeof(uint64_t) << (a.logn - lc)), c.csize, s);
+}
+
+cudaError_t launch_ntt_cluster_fused(bool product, const ClusterCfg& c, const ChainArgs& a, cudaStream_t s)
+{
+    const uint32_t logn = a.pass.logn;
+    if (!cluster_cfg_valid(product ? kClusterProduct : kClusterChain, logn, c)) return cudaErrorInvalidValue;
+    const FusedEntry* e = find_fused(c.lga, (int)logn - c.lga, c.lr);
+    const int lc = __builtin_ctz(c.csize);
+    const uint64_t blocks = a.pass.count * (uint64_t)c.csize;
+    if (a.pass.count == 0) return cudaSuccess;
+    if (blocks > 0x7fffffffull) return cudaErrorInvalidValue;
+    const void* fn = reinterpret_cast<const void*>(e->fn[product]);
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    if (dev >= 64) return cudaErrorInvalidDevice;
+    err = ensure_attrs(fn, g_fused_attr_done[fused_index(e)][product], dev);
+    if (err != cudaSuccess) return err;
+    count_launch();
+    ProfScope prof(s, "ntt_%s_cluster lgr=%d lr=%d c=%d", product ? "product" : "chain", c.lga, c.lr, c.csize);
+    return launch_cluster(fn, const_cast<ChainArgs*>(&a), blocks, 1u << (logn - lc - c.lr),
+                          3 * (sizeof(uint64_t) << (logn - lc)), c.csize, s);
 }
 
 }  // namespace axhel_impl

@@ -627,12 +627,16 @@ def kernel_case(family):
 
 
 def small_transform_latency(counts=(1, 4, 16, 64), reps=40):
-    """Device time per batched transform of a few limbs, N = 2^10..2^17, in
-    the one-launch cluster form (built-in choice) and in the two-launch pass
-    form: `reps` calls captured in a CUDA graph and replayed (no host launch
-    cost), best of 5 replays, microseconds per call."""
+    """Device time per batched call on a few limbs, N = 2^10..2^17, in the
+    one-launch cluster form (built-in choice) and in the pass form (two
+    launches for a transform, three for a fused chain or product): forward,
+    inverse, INTT -> MulMod -> NTT chain and NTT -> MulMod -> INTT product;
+    `reps` calls captured in a CUDA graph and replayed (no host launch cost),
+    best of 5 replays, microseconds per call."""
     import torch
 
+    names = {capi.CLUSTER_FORWARD: "forward", capi.CLUSTER_INVERSE: "inverse", capi.CLUSTER_CHAIN: "chain_mul",
+             capi.CLUSTER_PRODUCT: "product"}
     rows = []
     for logn in range(10, 18):
         n = 1 << logn
@@ -641,17 +645,27 @@ def small_transform_latency(counts=(1, 4, 16, 64), reps=40):
         for count in counts:
             x = torch.randint(0, 1 << 40, (count * n,), dtype=torch.int64, device="cuda")
             y = torch.empty_like(x)
-            for inverse in (False, True):
-                f, fa = (capi.inverse_batch, (2, 2)) if inverse else (capi.forward_batch, (4, 4))
-                row = {"logn": logn, "count": count, "direction": "inverse" if inverse else "forward"}
-                cfg = capi.cluster_plan_get(inverse, logn)
+            m = torch.randint(0, 1 << 40, (count * n,), dtype=torch.int64, device="cuda")
+            calls = {
+                capi.CLUSTER_FORWARD: lambda st: capi.forward_batch(ntts, y.data_ptr(), x.data_ptr(), count, 4, 4,
+                                                                    st),
+                capi.CLUSTER_INVERSE: lambda st: capi.inverse_batch(ntts, y.data_ptr(), x.data_ptr(), count, 2, 2,
+                                                                    st),
+                capi.CLUSTER_CHAIN: lambda st: capi.chain_mul_batch(ntts, y.data_ptr(), x.data_ptr(), m.data_ptr(),
+                                                                    count, 2, 4, st),
+                capi.CLUSTER_PRODUCT: lambda st: capi.product_batch(ntts, y.data_ptr(), x.data_ptr(), m.data_ptr(),
+                                                                    count, 4, 1, st),
+            }
+            for kind, call in calls.items():
+                row = {"logn": logn, "count": count, "direction": names[kind]}
+                cfg = capi.cluster_plan_get(kind, logn)
                 for form in ("cluster", "passes"):
                     if form == "cluster" and cfg[3] < count:
                         continue
-                    capi.cluster_plan_set(inverse, logn, *cfg[:3], 0 if form == "passes" else max(cfg[3], 1))
+                    if cfg[0]:
+                        capi.cluster_plan_set(kind, logn, *cfg[:3], 0 if form == "passes" else max(cfg[3], 1))
                     s = torch.cuda.Stream()
                     s.wait_stream(torch.cuda.current_stream())
-                    call = lambda st: f(ntts, y.data_ptr(), x.data_ptr(), count, fa[0], fa[1], st)
                     with torch.cuda.stream(s):
                         for _ in range(3):
                             call(s.cuda_stream)
@@ -670,10 +684,11 @@ def small_transform_latency(counts=(1, 4, 16, 64), reps=40):
                         best = min(best, e0.elapsed_time(e1) * 1e3 / reps)
                     del g
                     row[f"{form}_us"] = round(best, 2)
-                capi.cluster_plan_set(inverse, logn)
+                capi.cluster_plan_set(kind, logn)
                 rows.append(row)
     return {"workload": "device time per call, a few limbs of N = 2^10..2^17 (CUDA-graph replay)",
-            "cluster_form": {str(l): capi.cluster_plan_get(False, l) for l in range(10, 18)}, "rows": rows}
+            "cluster_form": {names[k]: {str(l): capi.cluster_plan_get(k, l) for l in range(10, 18)} for k in names},
+            "rows": rows}
 
 
 def main():

@@ -436,17 +436,20 @@ axhel_status_t axhel_cuda_plan_set(int inverse, uint32_t log_degree, uint32_t np
 /* Reads the plan used for (inverse, log2 N, count limbs); arrays of >= 3. */
 axhel_status_t axhel_cuda_plan_get(int inverse, uint32_t log_degree, uint64_t count, uint32_t* npass, uint32_t* lg,
                                    uint32_t* lr, uint32_t* tg);
-/* Single-launch form of a transform of a few limbs (new; no counterpart in
- * the reference, whose transforms run on the host): one thread-block cluster
- * of `csize` CTAs (2..16) per limb, `lga` stages in the first pass, `lr`
- * register stages; the two passes exchange the limb through the cluster's
- * shared memory instead of HBM.  Used for 2^10 <= N <= 2^17 and count <=
- * max_limbs; max_limbs == 0 turns it off for (direction, log2 N), lga == 0
+/* Single-launch forms of a few limbs (new; no counterpart in the reference,
+ * whose transforms run on the host): one thread-block cluster of `csize` CTAs
+ * (2..16) per limb, the passes exchanging the limb through the cluster's
+ * shared memory instead of HBM.  `kind`: 0 forward and 1 inverse transforms
+ * (`lga` first-pass stages), 2 the INTT -> MulMod/FMAMod -> NTT chains and
+ * 3 the NTT -> MulMod -> INTT product (`lga` stages in the contiguous
+ * groups); `lr` register stages.  Used for 2^10 <= N <= 2^17 and count <=
+ * max_limbs; max_limbs == 0 turns it off for (kind, log2 N), lga == 0
  * restores the built-in choice.  A pass plan set by axhel_cuda_plan_set for
- * the same degree takes precedence.  Every choice computes the same bits. */
-axhel_status_t axhel_cuda_cluster_plan_set(int inverse, uint32_t log_degree, uint32_t lga, uint32_t lr,
+ * the same degree (the inverse plan, for kinds 2 and 3) takes precedence.
+ * Every choice computes the same bits. */
+axhel_status_t axhel_cuda_cluster_plan_set(int kind, uint32_t log_degree, uint32_t lga, uint32_t lr,
                                            uint32_t csize, uint64_t max_limbs);
-axhel_status_t axhel_cuda_cluster_plan_get(int inverse, uint32_t log_degree, uint32_t* lga, uint32_t* lr,
+axhel_status_t axhel_cuda_cluster_plan_get(int kind, uint32_t log_degree, uint32_t* lga, uint32_t* lr,
                                            uint32_t* csize, uint64_t* max_limbs);
 /* Loads an autotuner table (text, one plan per line); NULL = the table shipped
  * beside the library.  Returns the number of plans loaded via *loaded. */

@@ -157,3 +157,86 @@ def test_transforms_on_8_byte_aligned_pointers(cuda, oracle, logn, count):
     efm = np.concatenate([oracle.mul(ef[s], m[s], qs[i % 2], 4) for i, s in enumerate(segs)])
     cuda.forward_mul_batch(ntts, p(o), p(d), p(dm), count)
     np.testing.assert_array_equal(back(o), efm)
+
+
+FUSED = [(5, 5, 2), (6, 5, 2), (5, 6, 2), (6, 6, 2), (7, 6, 2), (6, 7, 2), (7, 7, 2), (8, 7, 2), (7, 8, 2)]
+
+
+def fused_configs(logn):
+    """Valid (row stages, lr, csize) of the fused chain / product kernels."""
+    out = []
+    for a, b, lr in FUSED:
+        if a + b != logn:
+            continue
+        for c in (1, 2, 3, 4):
+            lgt = logn - c - lr
+            if c > min(a, b) or lgt < 5 or (1 << lgt) > 512 or 3 * 8 * (1 << (logn - c)) > 227 * 1024:
+                continue
+            out.append((a, lr, 1 << c))
+    return out
+
+
+@pytest.mark.parametrize("logn", [10, 11, 12, 13, 14, 15])
+def test_fused_cluster_chains_bitexact(cuda, oracle, logn):
+    """INTT -> MulMod/FMAMod -> NTT and NTT -> MulMod -> INTT in one cluster
+    launch per limb, every compiled configuration, against the reference call
+    sequences computed by the oracle (lazy and normalized, in place)."""
+    n = 1 << logn
+    L, count = 2, 3
+    params, tabs, qs = moduli(oracle, n, L)
+    ntts = [cuda.NTT(n, q, psi) for q, psi in params]
+    st = oracle.rng(SEED ^ 0xF05E ^ logn)
+    x = np.concatenate([oracle.random_vector(st, n, 4 * qs[i % L]) for i in range(count)])
+    m2 = np.concatenate([oracle.random_vector(st, n, 2 * qs[i % L]) for i in range(count)])
+    m4 = np.concatenate([oracle.random_vector(st, n, 4 * qs[i % L]) for i in range(count)])
+    scalars = [oracle.bounded(st, 2 * q) for q in qs]
+    segs = [slice(i * n, (i + 1) * n) for i in range(count)]
+
+    def chain_exp(op, out_f, k):
+        out = []
+        for i, s in enumerate(segs[:k]):
+            q, (fwd, inv, ninv) = qs[i % L], tabs[i % L]
+            y = oracle.inverse(oracle.reduce(x[s], q, 4, 2), q, inv, ninv, 2, 2)
+            if op == "mul":
+                y = oracle.mul(y, m2[s], q, 2)
+            else:
+                y = oracle.fma(y, scalars[i % L], m2[s] if op == "fma" else None, q, 2)
+            out.append(oracle.forward(y, q, fwd, 1, out_f))
+        return np.concatenate(out)
+
+    def product_exp(out_f, k):
+        out = []
+        for i, s in enumerate(segs[:k]):
+            q, (fwd, inv, ninv) = qs[i % L], tabs[i % L]
+            y = oracle.mul(oracle.forward(x[s], q, fwd, 4, 4), m4[s], q, 4)
+            out.append(oracle.inverse(y, q, inv, ninv, 2, out_f))
+        return np.concatenate(out)
+
+    cfgs = fused_configs(logn)
+    assert cfgs
+    try:
+        for lgr, lr, cs in cfgs:
+            for kind in (cuda.CLUSTER_CHAIN, cuda.CLUSTER_PRODUCT):
+                cuda.cluster_plan_set(kind, logn, lgr, lr, cs, count)
+            tag = f"lgr={lgr} lr={lr} csize={cs}"
+            for k in (1, count):
+                dm2, dm4, o = dev(m2[:k * n]), dev(m4[:k * n]), dev_empty(k * n)
+                for op in ("mul", "fma", "fma_noadd"):
+                    for out_f in (4, 1):
+                        d = dev(x[:k * n])
+                        if op == "mul":
+                            cuda.chain_mul_batch(ntts, ptr(o), ptr(d), ptr(dm2), k, 4, out_f)
+                        else:
+                            cuda.chain_fma_batch(ntts, ptr(d), ptr(d), scalars, ptr(dm2) if op == "fma" else 0, k,
+                                                 4, out_f)
+                            o, d = d, o
+                        np.testing.assert_array_equal(host(o), chain_exp(op, out_f, k),
+                                                      err_msg=f"chain {op} out_f={out_f} k={k} {tag}")
+                for out_f in (2, 1):
+                    d = dev(x[:k * n])
+                    cuda.product_batch(ntts, ptr(d), ptr(d), ptr(dm4), k, 4, out_f)
+                    np.testing.assert_array_equal(host(d), product_exp(out_f, k),
+                                                  err_msg=f"product out_f={out_f} k={k} {tag}")
+    finally:
+        for kind in (cuda.CLUSTER_CHAIN, cuda.CLUSTER_PRODUCT):
+            cuda.cluster_plan_set(kind, logn)

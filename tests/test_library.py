@@ -107,12 +107,19 @@ def test_cluster_plan_override():
     valid, invalid ones are refused, and an override can be cleared."""
     from axhel_b200 import capi
 
-    for inverse in (False, True):
+    for kind in (capi.CLUSTER_FORWARD, capi.CLUSTER_INVERSE, capi.CLUSTER_CHAIN, capi.CLUSTER_PRODUCT):
         for logn in range(10, 18):
-            lga, lr, cs, m = capi.cluster_plan_get(inverse, logn)
+            lga, lr, cs, m = capi.cluster_plan_get(kind, logn)
+            if kind >= capi.CLUSTER_CHAIN and logn > 15:
+                assert (lga, m) == (0, 0)  # no fused cluster kernel compiled for 2^16, 2^17
+                continue
             assert lga >= 5 and cs in (2, 4, 8, 16)
-            capi.cluster_plan_set(inverse, logn, lga, lr, cs, max(m, 1))  # valid as it stands
-            capi.cluster_plan_set(inverse, logn)
+            capi.cluster_plan_set(kind, logn, lga, lr, cs, max(m, 1))  # valid as it stands
+            capi.cluster_plan_set(kind, logn)
+    with pytest.raises(capi.AxhelError):
+        capi.cluster_plan_set(4, 12, 6, 2, 8, 1)  # no such kind
+    with pytest.raises(capi.AxhelError):
+        capi.cluster_plan_set(capi.CLUSTER_CHAIN, 12, 6, 3, 8, 1)  # fused kernels are radix-4 only
     default = capi.cluster_plan_get(False, 12)
     capi.cluster_plan_set(False, 12, 6, 2, 16, 5)
     assert capi.cluster_plan_get(False, 12) == (6, 2, 16, 5)
