@@ -137,11 +137,37 @@ size_t zero_copy_max()
     return std::min(v, pinned_max());
 }
 
+// Whether p is device memory, asked of the driver once per pointer and call:
+// the answer cannot change during a synchronous call, and the query takes a
+// driver lock that several host threads contend for (0.1 us alone, about
+// 3 us each with eight threads calling at once).  An in-place call (SEAL's
+// result == operand) asks once instead of twice.
+struct PtrMemo {
+    const void* p[4];
+    bool dev[4];
+    int n = 0;
+};
+thread_local PtrMemo t_memo;
+
+bool is_device(const void* p)
+{
+    PtrMemo& m = t_memo;
+    for (int i = 0; i < m.n; ++i)
+        if (m.p[i] == p) return m.dev[i];
+    const bool d = axhel_cuda_is_device_pointer(p) != 0;
+    if (m.n < 4) {
+        m.p[m.n] = p;
+        m.dev[m.n] = d;
+        ++m.n;
+    }
+    return d;
+}
+
 // Device view of an input operand: the pointer itself if it is device
 // memory, else a staged copy.
 const uint64_t* input(const uint64_t* p, uint64_t n, int slot)
 {
-    if (!p || axhel_cuda_is_device_pointer(p)) return p;
+    if (!p || is_device(p)) return p;
     const size_t bytes = n * sizeof(uint64_t);
     if (bytes <= zero_copy_max()) {
         std::memcpy(t_bounce.get(slot, n), p, bytes);
@@ -165,9 +191,11 @@ struct Output {
     uint64_t* dev = nullptr;
     uint64_t n = 0;
     bool mapped = false;
+    // Constructed first in every call: starts the call's pointer memo.
     Output(uint64_t* r, uint64_t count) : n(count)
     {
-        if (axhel_cuda_is_device_pointer(r)) {
+        t_memo.n = 0;
+        if (is_device(r)) {
             dev = r;
         } else if (count * sizeof(uint64_t) <= zero_copy_max()) {
             host = r;

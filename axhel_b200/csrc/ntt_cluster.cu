@@ -25,6 +25,7 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <mutex>
 
 #include "launch.h"
@@ -619,13 +620,16 @@ ClusterCfg default_cfg(int kind, uint32_t logn)
     }
 }
 
+// Overrides (axhel_cuda_cluster_plan_set); g_set is read without the lock
+// on every call, the configuration under it only when an override exists.
 std::mutex g_mu;
-bool g_set[4][18] = {};
+std::atomic<bool> g_set[4][18] = {};
 ClusterCfg g_over[4][18] = {};
-// per kernel and device: shared-memory / cluster-size attributes set
+// per kernel and device: shared-memory / cluster-size attributes set (bit
+// `device`), read without the lock once set
 std::mutex g_attr_mu;
-uint64_t g_attr_done[kNumEntries][2][2] = {};
-uint64_t g_fused_attr_done[kNumFused][2] = {};
+std::atomic<uint64_t> g_attr_done[kNumEntries][2][2] = {};
+std::atomic<uint64_t> g_fused_attr_done[kNumFused][2] = {};
 
 int entry_index(const Entry* e) { return (int)(e - kEntries); }
 int fused_index(const FusedEntry* e) { return (int)(e - kFused); }
@@ -633,13 +637,14 @@ int fused_index(const FusedEntry* e) { return (int)(e - kFused); }
 bool fused_kind(int kind) { return kind == kClusterChain || kind == kClusterProduct; }
 
 // Sets the launch attributes of `fn` once per device (bit `dev` of `done`).
-cudaError_t ensure_attrs(const void* fn, uint64_t& done, int dev)
+cudaError_t ensure_attrs(const void* fn, std::atomic<uint64_t>& done, int dev)
 {
+    if (done.load(std::memory_order_acquire) >> dev & 1) return cudaSuccess;
     std::lock_guard<std::mutex> lk(g_attr_mu);
-    if (done >> dev & 1) return cudaSuccess;
+    if (done.load(std::memory_order_relaxed) >> dev & 1) return cudaSuccess;
     cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
     if (err == cudaSuccess) err = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    if (err == cudaSuccess) done |= 1ull << dev;
+    if (err == cudaSuccess) done.fetch_or(1ull << dev, std::memory_order_release);
     return err;
 }
 
@@ -682,10 +687,10 @@ bool cluster_cfg_valid(int kind, uint32_t logn, const ClusterCfg& c)
 bool cluster_plan(int kind, uint32_t logn, uint64_t count, ClusterCfg* out)
 {
     if (kind < 0 || kind > 3 || logn < 10 || logn > 17) return false;
-    ClusterCfg c;
-    {
+    ClusterCfg c = default_cfg(kind, logn);
+    if (g_set[kind][logn].load(std::memory_order_acquire)) {
         std::lock_guard<std::mutex> lk(g_mu);
-        c = g_set[kind][logn] ? g_over[kind][logn] : default_cfg(kind, logn);
+        if (g_set[kind][logn].load(std::memory_order_relaxed)) c = g_over[kind][logn];
     }
     if (count == 0 || count > c.max_limbs || !cluster_cfg_valid(kind, logn, c)) return false;
     *out = c;
@@ -696,15 +701,15 @@ void cluster_plan_override(int kind, uint32_t logn, const ClusterCfg* c)
 {
     if (kind < 0 || kind > 3 || logn > 17) return;
     std::lock_guard<std::mutex> lk(g_mu);
-    g_set[kind][logn] = c != nullptr;
     if (c) g_over[kind][logn] = *c;
+    g_set[kind][logn].store(c != nullptr, std::memory_order_release);
 }
 
 ClusterCfg cluster_plan_current(int kind, uint32_t logn)
 {
     if (kind < 0 || kind > 3 || logn > 17) return ClusterCfg{0, 0, 0, 0};
     std::lock_guard<std::mutex> lk(g_mu);
-    return g_set[kind][logn] ? g_over[kind][logn] : default_cfg(kind, logn);
+    return g_set[kind][logn].load(std::memory_order_relaxed) ? g_over[kind][logn] : default_cfg(kind, logn);
 }
 
 cudaError_t launch_ntt_cluster(bool inverse, const ClusterCfg& c, const PassArgs& a, cudaStream_t s)

@@ -13,6 +13,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <string>
@@ -27,6 +28,7 @@ namespace {
 
 std::mutex g_mu;
 std::map<std::pair<int, uint32_t>, NttPlan> g_override;
+std::atomic<size_t> g_override_count{0};  // g_override.size(), read without the lock
 std::map<std::tuple<int, uint32_t, int>, NttPlan> g_table;
 std::map<uint32_t, int> g_batch_override, g_batch_table;  // logn -> contiguous-pass stages
 bool g_table_tried = false;
@@ -171,6 +173,7 @@ NttPlan plan_for(bool inverse, uint32_t logn, uint64_t limbs)
 
 bool plan_overridden(bool inverse, uint32_t logn)
 {
+    if (g_override_count.load(std::memory_order_acquire) == 0) return false;  // the usual case, no lock
     std::lock_guard<std::mutex> lk(g_mu);
     return g_override.count({inverse ? 1 : 0, logn}) != 0;
 }
@@ -182,6 +185,7 @@ void plan_override(bool inverse, uint32_t logn, const NttPlan* p)
         g_override[{inverse ? 1 : 0, logn}] = *p;
     else
         g_override.erase({inverse ? 1 : 0, logn});
+    g_override_count.store(g_override.size(), std::memory_order_release);
 }
 
 bool batch_row_valid(uint32_t logn, int row)
