@@ -598,6 +598,15 @@ def kernel_case(family):
         for _ in range(3):
             capi.forward_batch([t], x.data_ptr(), x.data_ptr(), 1, 4, 4)
             capi.inverse_batch([t], x.data_ptr(), x.data_ptr(), 1, 4, 1)
+    elif family == "cluster_chain":  # one limb of N = 2^12: INTT -> MulMod -> NTT and NTT -> MulMod -> INTT
+        n = 1 << 12
+        q, psi = params.rns_moduli(n, 1, 50, 59)[0]
+        t = capi.NTT(n, q, psi)
+        x = _dev(rng.integers(0, q, n, dtype=np.uint64))
+        m = _dev(rng.integers(0, q, n, dtype=np.uint64))
+        for _ in range(3):
+            capi.chain_mul_batch([t], x.data_ptr(), x.data_ptr(), m.data_ptr(), 1, 2, 1)
+            capi.product_batch([t], x.data_ptr(), x.data_ptr(), m.data_ptr(), 1, 4, 1)
     elif family == "tables":  # 3 x 24 fresh contexts of N = 2^16
         for lo, hi in ((30, 40), (41, 51), (52, 62)):
             capi.NTT.create_many([(1 << 16, q, psi) for q, psi in params.rns_moduli(1 << 16, 24, lo, hi)])
@@ -696,7 +705,7 @@ def main():
     ap.add_argument("what", choices=["tensor", "uneven", "serve", "eltwise", "case", "product", "latency"])
     ap.add_argument("family", nargs="?", default="eltwise",
                     help="case: eltwise | eltwise_unaligned | tensor | tables | chain | batch | batch_phased | "
-                         "batch_eltwise | peak | cluster")
+                         "batch_eltwise | peak | cluster | cluster_chain")
     ap.add_argument("--seconds", type=float, default=4.0)
     ap.add_argument("--device", action="store_true", help="device-resident request operands")
     ap.add_argument("--persistent", action="store_true", help="one persistent launch per batch")
