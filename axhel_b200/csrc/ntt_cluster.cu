@@ -401,20 +401,28 @@ __global__ void __launch_bounds__(max_threads(LR)) ntt_cluster_fused_kernel(cons
     uint64_t v[R];
     uint32_t gi, k;
 
+    static_assert(prefetch_fits<LGR, LR>() && prefetch_fits<LGC, LR>(), "fused shapes hold a pass's twiddles");
+    // Each half-transform's twiddles are loaded into registers ahead of it
+    // (with the limb, before a cluster barrier, or beside the operand): the
+    // phases run one after another, so this adds no registers to the peak.
     if constexpr (!PRODUCT) {
         // ---- inverse rows: stages [0, LGR)
         thread_role<LGR, LR>(tR, gi, k);
         load_global<LGR, LR, round_lo<true, LGR, LR, 0>()>(v, lsrc, tR, gi,
                                                            round_base<LR>(k, round_lo<true, LGR, LR, 0>()), vec_ok);
-        if (a.flags & kPreCsub2q) {
+        {
+            PassTw<NRR, LR> pt;
+            load_pass_tw<true, LGR, LR, false>(std::make_integer_sequence<int, NRR>{}, pt, k, tile_blk<LGR>(tR, gi), 0,
+                                               n, cx);
+            if (a.flags & kPreCsub2q) {
 #pragma unroll
-            for (int i = 0; i < R; ++i) v[i] = csub_lazy(v[i], q2);
+                for (int i = 0; i < R; ++i) v[i] = csub_lazy(v[i], q2);
+            }
+            run_pass_tw<true, LGR, LR, false>(std::make_integer_sequence<int, NRR>{}, v, pt, scratch + (gi << LGR), k,
+                                              group_mask<LGR, LR>(false, lgtgR, gi), lane_shift(false, lgtgR), q, q2);
         }
-        run_rounds<true, LGR, LR>(v, scratch + (gi << LGR), k, group_mask<LGR, LR>(false, lgtgR, gi),
-                                  lane_shift(false, lgtgR), tile_blk<LGR>(tR, gi), 0, n, cx, q, q2, false);
         cluster_wait();
         scatter<LGR, LR, round_lo<true, LGR, LR, NRR - 1>(), true, LGR>(v, tR, gi, k, lgchunk, lgtgC, landing1, cl);
-        cl.sync();
 
         // ---- columns: inverse stages [LGR, logn) with N^-1, the op, forward stages [0, LGC)
         constexpr int LO_IN = round_lo<true, LGC, LR, 0>();
@@ -423,39 +431,55 @@ __global__ void __launch_bounds__(max_threads(LR)) ntt_cluster_fused_kernel(cons
         thread_role<LGC, LR>(tC, gi, k);
         uint64_t* smg = scratch + (gi << LGC);
         const uint32_t hmask = group_mask<LGC, LR>(true, lgtgC, gi), lsh = lane_shift(true, lgtgC);
-        load_global<LGC, LR, LO_IN>(v, landing1, landing_tile(tC, lgtgC), gi, round_base<LR>(k, LO_IN), true);
-        run_rounds<true, LGC, LR>(v, smg, k, hmask, lsh, tile_blk<LGC>(tC, gi), LGR, n, cx, q, q2, true);
-        const uint32_t rb = round_base<LR>(k, LO_MID);
-        // EltwiseMulModNative<2> / EltwiseFMAModNative<2> on the inverse's [0, 2q) output
-        if (c.op == kChainMul) {
-            uint64_t m[R];
-            load_global<LGC, LR, LO_MID>(m, lop, tC, gi, rb, vec_ok);
-#pragma unroll
-            for (int i = 0; i < R; ++i)
-                v[i] = barrett_mul(reduce_input<2>(v[i], q), reduce_input<2>(m[i], q), q, mu, shift);
-        } else if (c.op == kChainFma) {
-            const uint64_t sc = reduce_input<2>(c.scalar[mi], q);
-#pragma unroll
-            for (int i = 0; i < R; ++i) v[i] = barrett_mul(reduce_input<2>(v[i], q), sc, q, mu, shift);
-            if (lop) {
+        {
+            PassTw<NRC, LR> pt;
+            load_pass_tw<true, LGC, LR, true>(std::make_integer_sequence<int, NRC>{}, pt, k, tile_blk<LGC>(tC, gi), LGR,
+                                              n, cx);
+            cl.sync();
+            load_global<LGC, LR, LO_IN>(v, landing1, landing_tile(tC, lgtgC), gi, round_base<LR>(k, LO_IN), true);
+            run_pass_tw<true, LGC, LR, true>(std::make_integer_sequence<int, NRC>{}, v, pt, smg, k, hmask, lsh, q, q2);
+        }
+        {
+            PassTw<NRC, LR> pt;
+            load_pass_tw<false, LGC, LR, false>(std::make_integer_sequence<int, NRC>{}, pt, k, 0, 0, n, cx);
+            const uint32_t rb = round_base<LR>(k, LO_MID);
+            // EltwiseMulModNative<2> / EltwiseFMAModNative<2> on the inverse's [0, 2q) output
+            if (c.op == kChainMul) {
                 uint64_t m[R];
                 load_global<LGC, LR, LO_MID>(m, lop, tC, gi, rb, vec_ok);
 #pragma unroll
-                for (int i = 0; i < R; ++i) v[i] = csub(v[i] + reduce_input<2>(m[i], q), q);
+                for (int i = 0; i < R; ++i)
+                    v[i] = barrett_mul(reduce_input<2>(v[i], q), reduce_input<2>(m[i], q), q, mu, shift);
+            } else if (c.op == kChainFma) {
+                const uint64_t sc = reduce_input<2>(c.scalar[mi], q);
+#pragma unroll
+                for (int i = 0; i < R; ++i) v[i] = barrett_mul(reduce_input<2>(v[i], q), sc, q, mu, shift);
+                if (lop) {
+                    uint64_t m[R];
+                    load_global<LGC, LR, LO_MID>(m, lop, tC, gi, rb, vec_ok);
+#pragma unroll
+                    for (int i = 0; i < R; ++i) v[i] = csub(v[i] + reduce_input<2>(m[i], q), q);
+                }
             }
+            run_pass_tw<false, LGC, LR, false>(std::make_integer_sequence<int, NRC>{}, v, pt, smg, k, hmask, lsh, q,
+                                               q2);
         }
-        fwd_stages<LGC, LR, 0>(v, rb, 0, 0, cx->fwd, q, q2);
-        fwd_rest<LGC, LR>(std::make_integer_sequence<int, NRC - 1>{}, v, smg, k, hmask, lsh, 0, 0, cx->fwd, q, q2);
         scatter<LGC, LR, round_lo<false, LGC, LR, NRC - 1>(), false, LGR>(v, tC, gi, k, lgchunk, lgtgC, landing2,
                                                                            cl);
-        cl.sync();
 
         // ---- forward rows: stages [LGC, logn)
         thread_role<LGR, LR>(tR, gi, k);
-        load_global<LGR, LR, round_lo<false, LGR, LR, 0>()>(v, landing2, landing_tile(tR, lgtgC), gi,
-                                                            round_base<LR>(k, round_lo<false, LGR, LR, 0>()), true);
-        run_rounds<false, LGR, LR>(v, scratch + (gi << LGR), k, group_mask<LGR, LR>(false, lgtgR, gi),
-                                   lane_shift(false, lgtgR), tile_blk<LGR>(tR, gi), LGC, n, cx, q, q2, false);
+        {
+            PassTw<NRR, LR> pt;
+            load_pass_tw<false, LGR, LR, false>(std::make_integer_sequence<int, NRR>{}, pt, k, tile_blk<LGR>(tR, gi),
+                                                LGC, n, cx);
+            cl.sync();
+            load_global<LGR, LR, round_lo<false, LGR, LR, 0>()>(
+                v, landing2, landing_tile(tR, lgtgC), gi, round_base<LR>(k, round_lo<false, LGR, LR, 0>()), true);
+            run_pass_tw<false, LGR, LR, false>(std::make_integer_sequence<int, NRR>{}, v, pt, scratch + (gi << LGR),
+                                               k, group_mask<LGR, LR>(false, lgtgR, gi), lane_shift(false, lgtgR), q,
+                                               q2);
+        }
         if (a.flags & kPostNorm) {
 #pragma unroll
             for (int i = 0; i < R; ++i) v[i] = csub_lazy(csub_lazy(v[i], q2), q);
@@ -467,12 +491,16 @@ __global__ void __launch_bounds__(max_threads(LR)) ntt_cluster_fused_kernel(cons
         thread_role<LGC, LR>(tC, gi, k);
         load_global<LGC, LR, round_lo<false, LGC, LR, 0>()>(v, lsrc, tC, gi,
                                                             round_base<LR>(k, round_lo<false, LGC, LR, 0>()), vec_ok);
-        run_rounds<false, LGC, LR>(v, scratch + (gi << LGC), k, group_mask<LGC, LR>(true, lgtgC, gi),
-                                   lane_shift(true, lgtgC), tile_blk<LGC>(tC, gi), 0, n, cx, q, q2, false);
+        {
+            PassTw<NRC, LR> pt;
+            load_pass_tw<false, LGC, LR, false>(std::make_integer_sequence<int, NRC>{}, pt, k, tile_blk<LGC>(tC, gi), 0,
+                                                n, cx);
+            run_pass_tw<false, LGC, LR, false>(std::make_integer_sequence<int, NRC>{}, v, pt, scratch + (gi << LGC), k,
+                                               group_mask<LGC, LR>(true, lgtgC, gi), lane_shift(true, lgtgC), q, q2);
+        }
         cluster_wait();
         scatter<LGC, LR, round_lo<false, LGC, LR, NRC - 1>(), false, LGR>(v, tC, gi, k, lgchunk, lgtgC, landing1,
                                                                            cl);
-        cl.sync();
 
         // ---- rows: forward stages [LGC, logn), MulMod<4>, inverse stages [0, LGR)
         constexpr int LO_IN = round_lo<false, LGR, LR, 0>();
@@ -482,26 +510,39 @@ __global__ void __launch_bounds__(max_threads(LR)) ntt_cluster_fused_kernel(cons
         uint64_t* smg = scratch + (gi << LGR);
         const uint32_t hmask = group_mask<LGR, LR>(false, lgtgR, gi), lsh = lane_shift(false, lgtgR);
         const uint64_t blk = tile_blk<LGR>(tR, gi);
-        load_global<LGR, LR, LO_IN>(v, landing1, landing_tile(tR, lgtgC), gi, round_base<LR>(k, LO_IN), true);
-        run_rounds<false, LGR, LR>(v, smg, k, hmask, lsh, blk, LGC, n, cx, q, q2, false);
         {
+            PassTw<NRR, LR> pt;
+            load_pass_tw<false, LGR, LR, false>(std::make_integer_sequence<int, NRR>{}, pt, k, blk, LGC, n, cx);
+            cl.sync();
+            load_global<LGR, LR, LO_IN>(v, landing1, landing_tile(tR, lgtgC), gi, round_base<LR>(k, LO_IN), true);
+            run_pass_tw<false, LGR, LR, false>(std::make_integer_sequence<int, NRR>{}, v, pt, smg, k, hmask, lsh, q,
+                                               q2);
+        }
+        {
+            PassTw<NRR, LR> pt;
+            load_pass_tw<true, LGR, LR, false>(std::make_integer_sequence<int, NRR>{}, pt, k, blk, 0, n, cx);
             uint64_t m[R];
             load_global<LGR, LR, LO_MID>(m, lop, tR, gi, round_base<LR>(k, LO_MID), vec_ok);
 #pragma unroll
             for (int i = 0; i < R; ++i)
                 v[i] = barrett_mul(reduce_input<4>(v[i], q), reduce_input<4>(m[i], q), q, mu, shift);
+            run_pass_tw<true, LGR, LR, false>(std::make_integer_sequence<int, NRR>{}, v, pt, smg, k, hmask, lsh, q, q2);
         }
-        run_rounds<true, LGR, LR>(v, smg, k, hmask, lsh, blk, 0, n, cx, q, q2, false);
         scatter<LGR, LR, round_lo<true, LGR, LR, NRR - 1>(), true, LGR>(v, tR, gi, k, lgchunk, lgtgC, landing2, cl);
-        cl.sync();
 
         // ---- inverse columns: stages [LGR, logn) with N^-1
         constexpr int LO_C = round_lo<true, LGC, LR, 0>();
         constexpr int LO_OUT = round_lo<true, LGC, LR, NRC - 1>();
         thread_role<LGC, LR>(tC, gi, k);
-        load_global<LGC, LR, LO_C>(v, landing2, landing_tile(tC, lgtgC), gi, round_base<LR>(k, LO_C), true);
-        run_rounds<true, LGC, LR>(v, scratch + (gi << LGC), k, group_mask<LGC, LR>(true, lgtgC, gi),
-                                  lane_shift(true, lgtgC), tile_blk<LGC>(tC, gi), LGR, n, cx, q, q2, true);
+        {
+            PassTw<NRC, LR> pt;
+            load_pass_tw<true, LGC, LR, true>(std::make_integer_sequence<int, NRC>{}, pt, k, tile_blk<LGC>(tC, gi), LGR,
+                                              n, cx);
+            cl.sync();
+            load_global<LGC, LR, LO_C>(v, landing2, landing_tile(tC, lgtgC), gi, round_base<LR>(k, LO_C), true);
+            run_pass_tw<true, LGC, LR, true>(std::make_integer_sequence<int, NRC>{}, v, pt, scratch + (gi << LGC), k,
+                                             group_mask<LGC, LR>(true, lgtgC, gi), lane_shift(true, lgtgC), q, q2);
+        }
         if (a.flags & kPostNorm) {
 #pragma unroll
             for (int i = 0; i < R; ++i) v[i] = csub_lazy(v[i], q);
