@@ -632,9 +632,9 @@ const FusedEntry* find_fused(int lgr, int lgc, int lr)
 ClusterCfg default_cfg(int kind, uint32_t logn)
 {
     // Fused chain / product of one limb against the three pass launches:
-    // 2^10 5.7 / 6.0 us (7.8 / 7.5), 2^11 6.1 / 5.7 (9.8 / 9.0), 2^12 6.5 /
-    // 6.7 (11.4 / 11.2), 2^13 7.0 / 6.3 (11.6 / 12.1), 2^14 8.7 / 8.5 (13.3 /
-    // 14.9), 2^15 12.8 / 13.0 (12.8 / 14.1); still ahead at 64 limbs up to
+    // 2^10 5.0 / 5.2 us (7.7 / 7.2), 2^11 5.4 / 5.2 (9.6 / 9.0), 2^12 5.7 /
+    // 5.8 (12.1 / 12.0), 2^13 6.2 / 5.6 (12.2 / 13.0), 2^14 8.2 / 8.1 (13.6 /
+    // 15.2), 2^15 12.3 / 12.6 (13.7 / 14.3); still ahead at 64 limbs up to
     // 2^12, behind from about 32 / 8 / 8 limbs at 2^13 / 2^14 / 2^15.
     if (kind == kClusterChain || kind == kClusterProduct) {
         switch (logn) {
