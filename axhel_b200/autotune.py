@@ -15,11 +15,17 @@ jobs, and writes
 
     B <logn> <contiguous-pass stages>
 
+For the one-launch cluster form of small calls (transforms, fused chains and
+products of a few limbs) it times every compiled (lga, lr, csize) on one
+limb and the limb counts up to which the fastest beats the pass form:
+
+    K <kind> <logn> <lga> <lr> <csize> <max-limbs>
+
 Every candidate computes the same bits (tests/test_ntt_gpu.py::
 test_every_plan_bitexact, tests/test_batch_gpu.py), so the choice only
 affects speed.
 
-    python -m axhel_b200.autotune [--what all|passes|batch] [--logn 12-17] [--buckets 0,3,6,9]
+    python -m axhel_b200.autotune [--what all|passes|batch|cluster] [--logn 12-17] [--buckets 0,3,6,9]
 """
 from __future__ import annotations
 
@@ -181,9 +187,98 @@ def tune_batch(lognums, bytes_per_job=128 << 20, reps=5, verbose=True):
     return lines
 
 
+def graph_time_us(torch, call, reps=30):
+    """Device time per call: `reps` calls captured in a CUDA graph, best of 5
+    replays (no host launch cost: what a small latency-bound call costs)."""
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        for _ in range(3):
+            call(s.cuda_stream)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        for _ in range(reps):
+            call(s.cuda_stream)
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) * 1e3 / reps)
+    del g
+    return best
+
+
+def tune_cluster(lognums, counts=(1, 2, 4, 8, 16, 32, 64), verbose=True):
+    """The one-launch cluster form of small calls (forward, inverse, the
+    INTT -> MulMod -> NTT chain, the NTT -> MulMod -> INTT product): per kind
+    and degree the fastest compiled (lga, lr, csize) on one limb, and the
+    largest limb count up to which it beats the pass form (0: never)."""
+    import torch
+
+    from axhel_b200 import capi, params
+
+    names = {capi.CLUSTER_FORWARD: "forward", capi.CLUSTER_INVERSE: "inverse", capi.CLUSTER_CHAIN: "chain",
+             capi.CLUSTER_PRODUCT: "product"}
+    lines = []
+    for logn in lognums:
+        n = 1 << logn
+        mods = params.rns_moduli(n, 4, 50, 59)
+        ntts = [capi.NTT(n, q, psi) for q, psi in mods]
+        cmax = max(counts)
+        x = torch.randint(0, 1 << 40, (cmax * n,), dtype=torch.int64, device="cuda")
+        y = torch.empty_like(x)
+        m = torch.randint(0, 1 << 40, (cmax * n,), dtype=torch.int64, device="cuda")
+
+        def caller(kind, count):
+            xp, yp, mp = x.data_ptr(), y.data_ptr(), m.data_ptr()
+            if kind == capi.CLUSTER_FORWARD:
+                return lambda st: capi.forward_batch(ntts, yp, xp, count, 4, 4, st)
+            if kind == capi.CLUSTER_INVERSE:
+                return lambda st: capi.inverse_batch(ntts, yp, xp, count, 2, 2, st)
+            if kind == capi.CLUSTER_CHAIN:
+                return lambda st: capi.chain_mul_batch(ntts, yp, xp, mp, count, 2, 4, st)
+            return lambda st: capi.product_batch(ntts, yp, xp, mp, count, 4, 1, st)
+
+        for kind in names:
+            best = None
+            for lga in range(5, 10):
+                for lr in (2, 3, 4):
+                    for cs in (2, 4, 8, 16):
+                        try:
+                            capi.cluster_plan_set(kind, logn, lga, lr, cs, cmax)
+                            us = graph_time_us(torch, caller(kind, 1))
+                        except (capi.AxhelError, RuntimeError):
+                            continue  # not compiled, or not schedulable on this GPU
+                        if best is None or us < best[0]:
+                            best = (us, lga, lr, cs)
+            if best is None:
+                capi.cluster_plan_set(kind, logn)
+                continue
+            _, lga, lr, cs = best
+            max_limbs = 0
+            for count in counts:
+                capi.cluster_plan_set(kind, logn, lga, lr, cs, cmax)
+                t_cluster = graph_time_us(torch, caller(kind, count))
+                capi.cluster_plan_set(kind, logn, lga, lr, cs, 0)
+                t_passes = graph_time_us(torch, caller(kind, count))
+                if t_cluster >= t_passes:
+                    break
+                max_limbs = count
+            capi.cluster_plan_set(kind, logn)
+            lines.append(f"K {kind} {logn} {lga} {lr} {cs} {max_limbs}")
+            if verbose:
+                print(f"{names[kind]} logn={logn}: lga={lga} lr={lr} csize={cs}, one limb {best[0]:.2f} us, "
+                      f"cluster form up to {max_limbs} limbs", flush=True)
+    return lines
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--what", choices=["all", "passes", "batch"], default="all")
+    ap.add_argument("--what", choices=["all", "passes", "batch", "cluster"], default="all")
     ap.add_argument("--logn", default="12-17")
     ap.add_argument("--buckets", default="0,3,5,7,9")
     ap.add_argument("--out", default=TABLE)
@@ -196,18 +291,23 @@ def main():
     if os.path.exists(a.out):
         with open(a.out) as f:
             old = [l.rstrip("\n") for l in f if l.strip() and not l.startswith("#")]
-    # lines of the part not re-tuned are kept
-    keep = [l for l in old if (l.startswith("B") if a.what == "passes" else
-                               (not l.startswith("B")) if a.what == "batch" else False)]
+    # lines of the parts not re-tuned are kept
+    def part(line):
+        return "batch" if line.startswith("B") else "cluster" if line.startswith("K") else "passes"
+
+    keep = [l for l in old if a.what != "all" and part(l) != a.what]
     lines = []
     if a.what in ("all", "passes"):
         lines += tune(lognums, buckets)
     if a.what in ("all", "batch"):
         lines += tune_batch(list(range(10, 18)) if a.what == "all" else lognums)
-    merged = sorted(keep + lines, key=lambda l: (l.startswith("B"), l))
+    if a.what in ("all", "cluster"):
+        lines += tune_cluster(list(range(10, 18)) if a.what == "all" else lognums)
+    merged = sorted(keep + lines, key=lambda l: ({"passes": 0, "batch": 1, "cluster": 2}[part(l)], l))
     with open(a.out, "w") as f:
         f.write("# NTT pass plans chosen by axhel_b200/autotune.py on one B200\n")
         f.write("# inverse logn limb-bucket npass (lg lr tg)...  |  B logn contiguous-pass-stages (batch engine)\n")
+        f.write("# K kind logn lga lr csize max-limbs (cluster form: 0 forward, 1 inverse, 2 chain, 3 product)\n")
         f.write("\n".join(merged) + "\n")
     print(f"wrote {a.out} ({len(lines)} lines tuned, {len(keep)} kept, {time.time() - t:.0f} s)")
 

@@ -95,6 +95,9 @@ bool cluster_cfg_valid(int kind, uint32_t logn, const ClusterCfg& c);
 bool cluster_plan(int kind, uint32_t logn, uint64_t count, ClusterCfg* out);
 void cluster_plan_override(int kind, uint32_t logn, const ClusterCfg* c);  // nullptr clears
 ClusterCfg cluster_plan_current(int kind, uint32_t logn);
+// The autotuner's table entry (`K` lines of ntt_plans.txt), between the
+// override and the built-in choice.
+void cluster_plan_table_set(int kind, uint32_t logn, const ClusterCfg& c);
 cudaError_t launch_ntt_cluster(bool inverse, const ClusterCfg& c, const PassArgs& a, cudaStream_t s);
 cudaError_t launch_ntt_cluster_fused(bool product, const ClusterCfg& c, const ChainArgs& a, cudaStream_t s);
 
@@ -104,6 +107,7 @@ bool plan_valid(const NttPlan& p, uint32_t logn, bool inverse);
 int plan_load(const char* path);
 void plan_override(bool inverse, uint32_t logn, const NttPlan* p);  // nullptr clears
 bool plan_overridden(bool inverse, uint32_t logn);
+void plan_table_ensure();  // loads ntt_plans.txt beside the library once
 // Uneven-batch engine: stages of the contiguous pass of an N = 2^logn job
 // (override > table > default); the strided pass takes the rest.
 bool batch_row_valid(uint32_t logn, int row);

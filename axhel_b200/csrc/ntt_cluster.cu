@@ -666,6 +666,24 @@ ClusterCfg default_cfg(int kind, uint32_t logn)
 std::mutex g_mu;
 std::atomic<bool> g_set[4][18] = {};
 ClusterCfg g_over[4][18] = {};
+// the autotuner's table (ntt_plans.txt), same scheme
+std::atomic<bool> g_tab_set[4][18] = {};
+ClusterCfg g_tab[4][18] = {};
+
+// The configuration for (kind, logn): override > table > built-in.
+ClusterCfg current_cfg(int kind, uint32_t logn)
+{
+    plan_table_ensure();
+    ClusterCfg c = default_cfg(kind, logn);
+    if (g_set[kind][logn].load(std::memory_order_acquire) || g_tab_set[kind][logn].load(std::memory_order_acquire)) {
+        std::lock_guard<std::mutex> lk(g_mu);
+        if (g_set[kind][logn].load(std::memory_order_relaxed))
+            c = g_over[kind][logn];
+        else if (g_tab_set[kind][logn].load(std::memory_order_relaxed))
+            c = g_tab[kind][logn];
+    }
+    return c;
+}
 // per kernel and device: shared-memory / cluster-size attributes set (bit
 // `device`), read without the lock once set
 std::mutex g_attr_mu;
@@ -728,11 +746,7 @@ bool cluster_cfg_valid(int kind, uint32_t logn, const ClusterCfg& c)
 bool cluster_plan(int kind, uint32_t logn, uint64_t count, ClusterCfg* out)
 {
     if (kind < 0 || kind > 3 || logn < 10 || logn > 17) return false;
-    ClusterCfg c = default_cfg(kind, logn);
-    if (g_set[kind][logn].load(std::memory_order_acquire)) {
-        std::lock_guard<std::mutex> lk(g_mu);
-        if (g_set[kind][logn].load(std::memory_order_relaxed)) c = g_over[kind][logn];
-    }
+    const ClusterCfg c = current_cfg(kind, logn);
     if (count == 0 || count > c.max_limbs || !cluster_cfg_valid(kind, logn, c)) return false;
     *out = c;
     return true;
@@ -749,8 +763,15 @@ void cluster_plan_override(int kind, uint32_t logn, const ClusterCfg* c)
 ClusterCfg cluster_plan_current(int kind, uint32_t logn)
 {
     if (kind < 0 || kind > 3 || logn > 17) return ClusterCfg{0, 0, 0, 0};
+    return current_cfg(kind, logn);
+}
+
+void cluster_plan_table_set(int kind, uint32_t logn, const ClusterCfg& c)
+{
+    if (kind < 0 || kind > 3 || logn > 17) return;
     std::lock_guard<std::mutex> lk(g_mu);
-    return g_set[kind][logn].load(std::memory_order_relaxed) ? g_over[kind][logn] : default_cfg(kind, logn);
+    g_tab[kind][logn] = c;
+    g_tab_set[kind][logn].store(true, std::memory_order_release);
 }
 
 cudaError_t launch_ntt_cluster(bool inverse, const ClusterCfg& c, const PassArgs& a, cudaStream_t s)

@@ -94,6 +94,19 @@ int load_table_locked(const char* path)
     int n = 0;
     while (std::fgets(line, sizeof line, fp)) {
         if (line[0] == '#' || line[0] == '\n') continue;
+        if (line[0] == 'K') {  // cluster form: kind logn lga lr csize max_limbs
+            int kind, logn, lga, lr, cs;
+            unsigned long long mx;
+            if (std::sscanf(line + 1, "%d %d %d %d %d %llu", &kind, &logn, &lga, &lr, &cs, &mx) == 6 && kind >= 0 &&
+                kind <= 3 && logn >= 10 && logn <= 17) {
+                const ClusterCfg c{lga, lr, cs, (uint64_t)mx};
+                if (mx == 0 || cluster_cfg_valid(kind, (uint32_t)logn, c)) {
+                    cluster_plan_table_set(kind, (uint32_t)logn, c);
+                    ++n;
+                }
+            }
+            continue;
+        }
         if (line[0] == 'B') {
             int logn, row;
             if (std::sscanf(line + 1, "%d %d", &logn, &row) == 2 && logn > 0 &&
@@ -213,6 +226,15 @@ void batch_row_override(uint32_t logn, int row)
         g_batch_override[logn] = row;
     else
         g_batch_override.erase(logn);
+}
+
+void plan_table_ensure()
+{
+    static std::once_flag once;
+    std::call_once(once, [] {
+        std::lock_guard<std::mutex> lk(g_mu);
+        ensure_table_locked();
+    });
 }
 
 int plan_load(const char* path)

@@ -191,3 +191,28 @@ def test_debug_log_build_compiles(tmp_path):
                     str(exe)], check=True)
     r = subprocess.run([str(exe)], capture_output=True, text=True, check=True)
     assert r.stderr == "[AXHEL] x=1\n"
+
+
+def test_cluster_table_lines(tmp_path):
+    """`K` lines of a plan table set the cluster form per kind and degree
+    (between an override and the built-in choice); invalid ones are skipped.
+    Run in a fresh process: a loaded table stays for the process."""
+    import sys
+
+    t = tmp_path / "plans.txt"
+    t.write_text("K 0 12 6 3 8 5\nK 2 13 7 2 16 3\nK 1 12 6 4 8 1\nK 3 16 8 2 16 2\nK 1 14 7 2 16 0\n")
+    code = f"""
+from axhel_b200 import capi
+assert capi.plan_load({str(t)!r}) == 3, "two lines are invalid"
+assert capi.cluster_plan_get(0, 12) == (6, 3, 8, 5)
+assert capi.cluster_plan_get(2, 13) == (7, 2, 16, 3)
+assert capi.cluster_plan_get(1, 14)[3] == 0          # turned off by the table
+assert capi.cluster_plan_get(1, 12) != (6, 4, 8, 1)  # not compiled: built-in kept
+capi.cluster_plan_set(0, 12, 6, 2, 8, 9)             # an override wins over the table
+assert capi.cluster_plan_get(0, 12) == (6, 2, 8, 9)
+capi.cluster_plan_set(0, 12)                         # cleared: back to the table
+assert capi.cluster_plan_get(0, 12) == (6, 3, 8, 5)
+print("ok")
+"""
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=ROOT, timeout=120)
+    assert r.returncode == 0 and "ok" in r.stdout, r.stderr[-2000:]
