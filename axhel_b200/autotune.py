@@ -244,21 +244,25 @@ def tune_cluster(lognums, counts=(1, 2, 4, 8, 16, 32, 64), verbose=True):
             return lambda st: capi.product_batch(ntts, yp, xp, mp, count, 4, 1, st)
 
         for kind in names:
-            best = None
+            # every compiled shape, timed on 1, 4, 16 and 64 limbs; the one with
+            # the smallest summed time relative to the fastest shape at each
+            # count (the best on one limb alone can be 20-35 % slower on 16)
+            obj = (1, 4, 16, 64)
+            timed = {}
             for lga in range(5, 10):
                 for lr in (2, 3, 4):
                     for cs in (2, 4, 8, 16):
                         try:
                             capi.cluster_plan_set(kind, logn, lga, lr, cs, cmax)
-                            us = graph_time_us(torch, caller(kind, 1))
+                            timed[(lga, lr, cs)] = [graph_time_us(torch, caller(kind, c)) for c in obj]
                         except (capi.AxhelError, RuntimeError):
                             continue  # not compiled, or not schedulable on this GPU
-                        if best is None or us < best[0]:
-                            best = (us, lga, lr, cs)
-            if best is None:
+            if not timed:
                 capi.cluster_plan_set(kind, logn)
                 continue
-            _, lga, lr, cs = best
+            fastest = [min(t[i] for t in timed.values()) for i in range(len(obj))]
+            lga, lr, cs = min(timed, key=lambda c: sum(timed[c][i] / fastest[i] for i in range(len(obj))))
+            best = (timed[(lga, lr, cs)][0],)
             max_limbs = 0
             for count in counts:
                 capi.cluster_plan_set(kind, logn, lga, lr, cs, cmax)

@@ -618,7 +618,9 @@ const FusedEntry* find_fused(int lgr, int lgc, int lr)
     return nullptr;
 }
 
-// Built-in choice per kind and log2 N (10..17): first-pass (transforms) or
+// Built-in choice (where ntt_plans.txt has no `K` line for it; the
+// autotuner's lines reproduce it within noise) per kind and log2 N (10..17):
+// first-pass (transforms) or
 // row (fused chains) stages, register stages, cluster size, and the largest
 // limb count that takes the cluster form -- the fastest on a B200 by device
 // time per call (CUDA-graph replay).  Transforms of one limb, forward /
