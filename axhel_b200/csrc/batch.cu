@@ -498,6 +498,64 @@ axhel_status_t batch_check_job(const axhel_job_t& J, const std::string& who, std
 // Host layout of a batch: fills `host` (to be copied to the device at `base`)
 // and the kernel arguments.  Shared by the allocating and the static-scratch
 // entry points.
+// The specialized kernel for a launch of one transform or chain entry: the
+// pass of the tuned plan (plan_for) that covers the same stages with the
+// same width, with its register depth and tile width; a chain's fused pass
+// as the chain kernel over the inverse plan's last pass (register depth at
+// most 3, as the chain entry point runs it).  Left as a class launch when no
+// tuned pass matches the batch's split.
+static void set_specialized(ClassLaunch& L, const BatchJob& b, const std::vector<const ModCtx*>& ctx,
+                     const std::vector<uint64_t>& sc, uint32_t phase)
+{
+    L.spec = 0;
+    if (L.cls == kClsElt || ctx.empty() || ctx.size() > (size_t)kMaxInlineMods || b.count == 0) return;
+    const PhaseCfg pc = phase_cfg(b, phase);
+    PassArgs a{};
+    a.src = L.first.src;
+    a.dst = L.first.dst;
+    a.count = b.count;
+    a.logn = b.logn;
+    a.s0 = pc.s0;
+    a.flags = L.first.flags;
+    a.nctx = (uint32_t)ctx.size();
+    for (size_t m = 0; m < ctx.size(); ++m) a.ctx[m] = ctx[m];
+    const NttPlan inv = plan_for(true, b.logn, b.count);
+    if (pc.chain) {
+        if (inv.npass < 2) return;
+        PassCfg fc = inv.pass[inv.npass - 1];
+        if (fc.lg != (int)pc.lg) return;
+        if (fc.lr > 3 && fc.lg >= 4 && ((uint64_t)fc.tg << (fc.lg - 3)) <= 512) fc.lr = 3;
+        if (fc.lr > 3) return;
+        a.tg = (uint32_t)fc.tg;
+        L.spec_args = ChainArgs{};
+        L.spec_args.pass = a;
+        L.spec_args.operand = L.first.vec;
+        L.spec_args.op = L.first.op;
+        L.spec_args.op_factor = 2;
+        if (L.first.op == kChainFma) {
+            if (sc.size() != ctx.size()) return;
+            for (size_t m = 0; m < sc.size(); ++m) L.spec_args.scalar[m] = sc[m];
+        }
+        L.spec_cfg = fc;
+        L.spec = 2;
+        return;
+    }
+    const NttPlan pl = pc.inv ? inv : plan_for(false, b.logn, b.count);
+    uint32_t s0 = 0;
+    for (int i = 0; i < pl.npass; ++i) {
+        if (s0 == pc.s0 && pl.pass[i].lg == (int)pc.lg) {
+            a.tg = (uint32_t)pl.pass[i].tg;
+            L.spec_args = ChainArgs{};
+            L.spec_args.pass = a;
+            L.spec_cfg = pl.pass[i];
+            L.spec_inv = pc.inv;
+            L.spec = 1;
+            return;
+        }
+        s0 += (uint32_t)pl.pass[i].lg;
+    }
+}
+
 axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned char* base,
                            std::vector<unsigned char>& host, size_t* zero_off, size_t* zero_bytes, BatchArgs* args,
                            std::vector<axhel_ntt_t>* held, std::string* err, std::vector<ClassLaunch>* classes)
@@ -744,6 +802,8 @@ axhel_status_t batch_build(const axhel_job_t* jobs, uint64_t n_jobs, unsigned ch
         for (size_t i = 0; i < alone.size(); ++i) {
             alone[i].first = targ[alone_idx[i]];
             alone[i].first.tile0 = 0;
+            const uint32_t j = ent[alone_idx[i]].job;
+            set_specialized(alone[i], bj[j], ctxs[j], scal[j], ent[alone_idx[i]].phase);
         }
         cl.insert(cl.end(), alone.begin(), alone.end());
         // phase by phase, the largest launches first (spread over the lanes)
@@ -822,7 +882,8 @@ void lanes_destroy(LaunchLanes* l)
     l->fork = nullptr;
 }
 
-cudaError_t batch_launch_classes(const std::vector<ClassLaunch>& classes, cudaStream_t s, const LaunchLanes* lanes)
+cudaError_t batch_launch_classes(const std::vector<ClassLaunch>& classes, cudaStream_t s, const LaunchLanes* lanes,
+                                 bool specialized)
 {
     for (size_t i = 0; i < classes.size();) {
         size_t j = i;
@@ -843,6 +904,14 @@ cudaError_t batch_launch_classes(const std::vector<ClassLaunch>& classes, cudaSt
             if (!kn.one) return cudaErrorInvalidValue;
             const int l = (int)((k - i) % nl);
             cudaStream_t ls = l == 0 ? s : lanes->st[l - 1];
+            if (specialized && L.spec == 1) {
+                e = launch_ntt_pass(L.spec_inv, L.spec_cfg, L.spec_args.pass, ls);
+                continue;
+            }
+            if (specialized && L.spec == 2) {
+                e = launch_chain_pass(L.spec_cfg, L.spec_args, ls);
+                continue;
+            }
             count_launch();
             ProfScope prof(ls, "batch_class_kernel cls=%u lg=%u", L.cls, L.lg);
             if (L.n_ce == 1)
@@ -944,7 +1013,7 @@ axhel_status_t axhel_cuda_batch_launch_phased(axhel_batch_t b, void* stream)
             cudaGetLastError();
         }
     }
-    if (e == cudaSuccess) e = batch_launch_classes(b->classes, s, b->lanes.fork ? &b->lanes : nullptr);
+    if (e == cudaSuccess) e = batch_launch_classes(b->classes, s, b->lanes.fork ? &b->lanes : nullptr, true);
     if (e != cudaSuccess) return bfail(AXHEL_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
     return AXHEL_OK;
 }

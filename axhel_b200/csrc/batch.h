@@ -85,6 +85,13 @@ struct ClassLaunch {
     const ClassEntry* ce;  // device address, n_ce entries
     uint64_t tiles;
     ClassEntry first;      // host copy of ce[0]: a launch of one entry takes it as a kernel parameter
+    // A launch of one transform or chain entry can instead run as the
+    // specialized pass / chain kernel with the tuned plan's tile shape for
+    // its pass (spec 1: pass kernel, 2: chain kernel; 0: class kernel only).
+    uint32_t spec = 0;
+    bool spec_inv = false;
+    PassCfg spec_cfg{};
+    ChainArgs spec_args{};
 };
 
 struct BatchArgs {
@@ -136,7 +143,7 @@ void lanes_destroy(LaunchLanes* l);
 // and budget).  Concurrent batches on other streams share the SMs tile by
 // tile.  `classes` as filled by batch_build.
 cudaError_t batch_launch_classes(const std::vector<ClassLaunch>& classes, cudaStream_t s,
-                                 const LaunchLanes* lanes);
+                                 const LaunchLanes* lanes, bool specialized = false);
 
 // Records the message returned by axhel_cuda_batch_last_error on this thread.
 void batch_set_error(const std::string& msg);
