@@ -413,6 +413,68 @@ std::vector<axhel_ntt_t> rns_handles(const NTT* ntts, size_t n_ntts, uint64_t* d
     return hs;
 }
 
+// Per-thread events marking the end of each chunk of a pipelined call.
+struct ChunkEvents {
+    std::vector<cudaEvent_t> ev;
+    ~ChunkEvents()
+    {
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    }
+    cudaEvent_t get(size_t i)
+    {
+        while (ev.size() <= i) {
+            cudaEvent_t e = nullptr;
+            check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+            ev.push_back(e);
+        }
+        return ev[i];
+    }
+};
+thread_local ChunkEvents t_events;
+
+// A batch of limbs whose operand and result are both host memory, too large
+// for the mapped route: staged in chunks of limbs (about 2 MiB each), so that
+// the CPU's copies into and out of the pinned buffers overlap the GPU's
+// copies and transform of the neighbouring chunks.  `run(handles, n_handles,
+// data, limbs)` transforms `limbs` limbs in place on the device, limb i with
+// handles[i % n_handles].  Returns false (nothing done) where this does not
+// apply.
+template <class Run>
+bool rns_pipelined(const std::vector<axhel_ntt_t>& hs, uint64_t n, uint64_t* result, const uint64_t* operand,
+                   size_t count, Run run)
+{
+    const size_t words = count * n, bytes_all = words * sizeof(uint64_t);
+    const size_t per = std::max<size_t>(1, (size_t(2) << 20) / (n * sizeof(uint64_t)));
+    const size_t nch = (count + per - 1) / per;
+    t_memo.n = 0;
+    if (nch < 2 || bytes_all <= zero_copy_max() || bytes_all > pinned_max() || is_device(result) ||
+        is_device(operand))
+        return false;
+    uint64_t* hin = t_bounce.get(0, words);
+    uint64_t* hout = t_bounce.get(3, words);
+    uint64_t* d = t_staging.get(0, words);
+    std::vector<axhel_ntt_t> rot(hs.size());
+    for (size_t c = 0; c <= nch; ++c) {
+        if (c < nch) {  // stage chunk c, queue its copies and transform
+            const size_t f = c * per, k = std::min(per, count - f), off = f * n, bytes = k * n * sizeof(uint64_t);
+            std::memcpy(hin + off, operand + off, bytes);
+            check_cuda(cudaMemcpyAsync(d + off, hin + off, bytes, cudaMemcpyHostToDevice, stream()),
+                       "host to device copy");
+            for (size_t j = 0; j < hs.size(); ++j) rot[j] = hs[(f + j) % hs.size()];
+            check(run(rot.data(), rot.size(), d + off, k), "RNS transform");
+            check_cuda(cudaMemcpyAsync(hout + off, d + off, bytes, cudaMemcpyDeviceToHost, stream()),
+                       "device to host copy");
+            check_cuda(cudaEventRecord(t_events.get(c), stream()), "event record");
+        }
+        if (c >= 1) {  // unstage chunk c-1 once its copy back is done
+            const size_t f = (c - 1) * per, k = std::min(per, count - f), off = f * n;
+            check_cuda(cudaEventSynchronize(t_events.get(c - 1)), "event synchronize");
+            std::memcpy(result + off, hout + off, k * n * sizeof(uint64_t));
+        }
+    }
+    return true;
+}
+
 }  // namespace
 
 void ComputeForwardRNS(const NTT* ntts, size_t n_ntts, uint64_t* result, const uint64_t* operand, size_t count,
@@ -421,6 +483,10 @@ void ComputeForwardRNS(const NTT* ntts, size_t n_ntts, uint64_t* result, const u
     if (count == 0) return;
     uint64_t n = 0;
     const std::vector<axhel_ntt_t> hs = rns_handles(ntts, n_ntts, &n);
+    if (rns_pipelined(hs, n, result, operand, count, [&](const axhel_ntt_t* h, size_t nh, uint64_t* p, size_t k) {
+            return axhel_cuda_ntt_forward_batch(h, nh, p, p, k, 1, output_mod_factor, stream());
+        }))
+        return;
     const uint64_t words = (uint64_t)count * n;
     Output out(result, words);
     const uint64_t* a = input(operand, words, 0);
@@ -435,6 +501,10 @@ void ComputeInverseRNS(const NTT* ntts, size_t n_ntts, uint64_t* result, const u
     if (count == 0) return;
     uint64_t n = 0;
     const std::vector<axhel_ntt_t> hs = rns_handles(ntts, n_ntts, &n);
+    if (rns_pipelined(hs, n, result, operand, count, [&](const axhel_ntt_t* h, size_t nh, uint64_t* p, size_t k) {
+            return axhel_cuda_ntt_inverse_batch(h, nh, p, p, k, 2, output_mod_factor, stream());
+        }))
+        return;
     const uint64_t words = (uint64_t)count * n;
     Output out(result, words);
     const uint64_t* a = input(operand, words, 0);

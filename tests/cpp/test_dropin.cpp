@@ -277,11 +277,11 @@ static void test_threads_share_one_ntt()
     for (int k = 0; k < 8; ++k) CHECK(ok[k], "thread %d", k);
 }
 
-static void test_rns_batches()
+static void test_rns_batches(uint64_t n)
 {
     // One call per polynomial instead of one per limb (ntt-rns.hpp): equal to
     // the per-limb calls, host and device pointers, in and out of place.
-    const uint64_t n = 4096;
+    // 15 limbs of N = 65536 (7.5 MiB) are staged in chunks of 4 limbs.
     const size_t L = 5, count = 3 * L;
     std::vector<NTT> ntts;
     std::vector<uint64_t> qs;
@@ -302,7 +302,7 @@ static void test_rns_batches()
         for (size_t i = 0; i < count; ++i)
             ntts[i % L].ComputeForward(want.data() + i * n, x.data() + i * n, 4, out_f);
         unipi::axhel::ComputeForwardRNS(ntts.data(), L, got.data(), x.data(), count, 4, out_f);
-        CHECK(got == want, "ComputeForwardRNS out_f=%llu", (unsigned long long)out_f);
+        CHECK(got == want, "ComputeForwardRNS N=%llu out_f=%llu", (unsigned long long)n, (unsigned long long)out_f);
         unipi::axhel::ComputeForwardRNS(ntts.data(), L, inplace.data(), inplace.data(), count, 4, out_f);
         CHECK(inplace == want, "ComputeForwardRNS in place out_f=%llu", (unsigned long long)out_f);
         for (uint64_t inv_out : {1, 2}) {
@@ -342,7 +342,8 @@ int main()
     test_polymul();
     test_device_pointers();
     test_threads_share_one_ntt();
-    test_rns_batches();
+    test_rns_batches(4096);
+    test_rns_batches(65536);
     if (g_fail) {
         std::fprintf(stderr, "%d failure(s)\n", g_fail);
         return 1;
