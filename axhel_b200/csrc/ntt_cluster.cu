@@ -21,7 +21,14 @@
 //
 // Every butterfly is the pass kernels' (the reference's radix-2 butterflies
 // applied to the same pairs, with the same twiddles, in the same stage
-// order), so results are bit-identical to the two-launch form.
+// order), so results are bit-identical to the two-launch form.  The
+// transform kernel also applies the dyadic product of kPreMul / kPostMul (a
+// MulMod on load / before the store), and the fused kernel further down runs
+// the INTT -> op -> NTT chains and the NTT -> MulMod -> INTT product in one
+// launch with two exchanges.  The host side picks the cluster shape per kind
+// and degree (override > `K` lines of ntt_plans.txt > built-in choice) and
+// takes this form up to a limb count beyond which the pass kernels, which
+// use every SM, are faster.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
