@@ -46,13 +46,16 @@ inline cudaStream_t stream() { return cudaStreamPerThread; }
 // Default bound for staging host operands through pinned buffers.
 constexpr size_t kPinnedStagingMax = size_t(1) << 30;
 // Default bounds for operands the kernels access in the pinned buffers
-// directly (no DMA copy): 256 KiB where the kernel reads them in contiguous
-// runs (element-wise calls, the inverse transform's first pass), 128 KiB for
-// the forward transform, whose first pass reads strided columns -- short
-// PCIe requests that cost more than a DMA copy from 2^15 words up (with eight
-// threads calling, 210 against 136 us per call at N = 2^15).
-constexpr size_t kZeroCopyMax = size_t(256) << 10;
-constexpr size_t kZeroCopyMaxStrided = size_t(128) << 10;
+// directly (no DMA copy).  Element-wise kernels read and write them once in
+// contiguous runs: 512 KiB (MulMod at N = 2^16: 105 against 120 us per call
+// by DMA).  The inverse transform reads contiguous rows, but from 2^16 words
+// it runs as two passes over the buffers: 256 KiB.  The forward transform's
+// first pass reads strided columns, short PCIe requests that cost more than
+// a DMA copy from 2^15 words up (with eight threads calling, 210 against
+// 136 us per call at N = 2^15): 128 KiB.
+constexpr size_t kZeroCopyEltwise = size_t(512) << 10;
+constexpr size_t kZeroCopyInverse = size_t(256) << 10;
+constexpr size_t kZeroCopyForward = size_t(128) << 10;
 
 // Growable per-thread device staging buffers (one per operand slot).
 struct Staging {
@@ -131,14 +134,14 @@ size_t pinned_max()
 // Host operands up to this many bytes are not copied to the device at all:
 // the kernels read them from, and write results to, the mapped pinned
 // buffers over PCIe.  For a small call that saves a DMA copy each way, whose
-// set-up costs more than moving the data.  `strided`: the forward
-// transform's bound (see above).  Environment variable AXHEL_ZERO_COPY_MAX
-// (bytes; 0 = never), read once, sets both.
-size_t zero_copy_max(bool strided = false)
+// set-up costs more than moving the data.  `deflt`: the operation's bound
+// (above).  Environment variable AXHEL_ZERO_COPY_MAX (bytes; 0 = never), read
+// once, sets all of them.
+size_t zero_copy_max(size_t deflt)
 {
     static const char* env = std::getenv("AXHEL_ZERO_COPY_MAX");
     static const size_t v = env ? (size_t)std::strtoull(env, nullptr, 10) : 0;
-    return std::min(env ? v : (strided ? kZeroCopyMaxStrided : kZeroCopyMax), pinned_max());
+    return std::min(env ? v : deflt, pinned_max());
 }
 
 // Whether p is device memory, asked of the driver once per pointer and call:
@@ -169,11 +172,11 @@ bool is_device(const void* p)
 
 // Device view of an input operand: the pointer itself if it is device
 // memory, else a staged copy.
-const uint64_t* input(const uint64_t* p, uint64_t n, int slot, bool strided = false)
+const uint64_t* input(const uint64_t* p, uint64_t n, int slot, size_t zc = kZeroCopyEltwise)
 {
     if (!p || is_device(p)) return p;
     const size_t bytes = n * sizeof(uint64_t);
-    if (bytes <= zero_copy_max(strided)) {
+    if (bytes <= zero_copy_max(zc)) {
         std::memcpy(t_bounce.get(slot, n), p, bytes);
         return t_bounce.dev[slot];
     }
@@ -196,12 +199,12 @@ struct Output {
     uint64_t n = 0;
     bool mapped = false;
     // Constructed first in every call: starts the call's pointer memo.
-    Output(uint64_t* r, uint64_t count, bool strided = false) : n(count)
+    Output(uint64_t* r, uint64_t count, size_t zc = kZeroCopyEltwise) : n(count)
     {
         t_memo.n = 0;
         if (is_device(r)) {
             dev = r;
-        } else if (count * sizeof(uint64_t) <= zero_copy_max(strided)) {
+        } else if (count * sizeof(uint64_t) <= zero_copy_max(zc)) {
             host = r;
             t_bounce.get(3, count);
             dev = t_bounce.dev[3];
@@ -363,8 +366,8 @@ void NTT::ComputeForward(uint64_t* result, const uint64_t* operand, uint64_t inp
         check(axhel_cuda_ntt_refresh_external(impl_->handle, reinterpret_cast<const uint64_t*>(impl_->ext_fwd),
                                               nullptr, nullptr, stream()),
               "NTT external tables");
-    Output out(result, n, true);
-    const uint64_t* a = input(operand, n, 0, true);
+    Output out(result, n, kZeroCopyForward);
+    const uint64_t* a = input(operand, n, 0, kZeroCopyForward);
     AXHEL_LOG("NTT::ComputeForward -> CUDA, N=" << n << ", out_factor=" << output_mod_factor
                                                  << (out.host ? ", host operands" : ", device operands"));
     check(axhel_cuda_ntt_forward(impl_->handle, out.dev, a, input_mod_factor, output_mod_factor, stream()),
@@ -382,8 +385,8 @@ void NTT::ComputeInverse(uint64_t* result, const uint64_t* operand, uint64_t inp
                                               reinterpret_cast<const uint64_t*>(impl_->ext_inv), ninv, stream()),
               "NTT external tables");
     }
-    Output out(result, n);
-    const uint64_t* a = input(operand, n, 0);
+    Output out(result, n, kZeroCopyInverse);
+    const uint64_t* a = input(operand, n, 0, kZeroCopyInverse);
     AXHEL_LOG("NTT::ComputeInverse -> CUDA, N=" << n << ", out_factor=" << output_mod_factor
                                                  << (out.host ? ", host operands" : ", device operands"));
     check(axhel_cuda_ntt_inverse(impl_->handle, out.dev, a, input_mod_factor, output_mod_factor, stream()),
@@ -445,13 +448,13 @@ thread_local ChunkEvents t_events;
 // apply.
 template <class Run>
 bool rns_pipelined(const std::vector<axhel_ntt_t>& hs, uint64_t n, uint64_t* result, const uint64_t* operand,
-                   size_t count, bool strided, Run run)
+                   size_t count, size_t zc, Run run)
 {
     const size_t words = count * n, bytes_all = words * sizeof(uint64_t);
     const size_t per = std::max<size_t>(1, (size_t(2) << 20) / (n * sizeof(uint64_t)));
     const size_t nch = (count + per - 1) / per;
     t_memo.n = 0;
-    if (nch < 2 || bytes_all <= zero_copy_max(strided) || bytes_all > pinned_max() || is_device(result) ||
+    if (nch < 2 || bytes_all <= zero_copy_max(zc) || bytes_all > pinned_max() || is_device(result) ||
         is_device(operand))
         return false;
     uint64_t* hin = t_bounce.get(0, words);
@@ -487,14 +490,14 @@ void ComputeForwardRNS(const NTT* ntts, size_t n_ntts, uint64_t* result, const u
     if (count == 0) return;
     uint64_t n = 0;
     const std::vector<axhel_ntt_t> hs = rns_handles(ntts, n_ntts, &n);
-    if (rns_pipelined(hs, n, result, operand, count, true,
+    if (rns_pipelined(hs, n, result, operand, count, kZeroCopyForward,
                       [&](const axhel_ntt_t* h, size_t nh, uint64_t* p, size_t k) {
                           return axhel_cuda_ntt_forward_batch(h, nh, p, p, k, 1, output_mod_factor, stream());
                       }))
         return;
     const uint64_t words = (uint64_t)count * n;
-    Output out(result, words, true);
-    const uint64_t* a = input(operand, words, 0, true);
+    Output out(result, words, kZeroCopyForward);
+    const uint64_t* a = input(operand, words, 0, kZeroCopyForward);
     check(axhel_cuda_ntt_forward_batch(hs.data(), n_ntts, out.dev, a, count, 1, output_mod_factor, stream()),
           "ComputeForwardRNS");
     out.finish();
@@ -506,14 +509,14 @@ void ComputeInverseRNS(const NTT* ntts, size_t n_ntts, uint64_t* result, const u
     if (count == 0) return;
     uint64_t n = 0;
     const std::vector<axhel_ntt_t> hs = rns_handles(ntts, n_ntts, &n);
-    if (rns_pipelined(hs, n, result, operand, count, false,
+    if (rns_pipelined(hs, n, result, operand, count, kZeroCopyInverse,
                       [&](const axhel_ntt_t* h, size_t nh, uint64_t* p, size_t k) {
                           return axhel_cuda_ntt_inverse_batch(h, nh, p, p, k, 2, output_mod_factor, stream());
                       }))
         return;
     const uint64_t words = (uint64_t)count * n;
-    Output out(result, words);
-    const uint64_t* a = input(operand, words, 0);
+    Output out(result, words, kZeroCopyInverse);
+    const uint64_t* a = input(operand, words, 0, kZeroCopyInverse);
     // input factor 2: the per-limb ComputeInverse's contract (inputs in [0, 2q)), no fused reduction
     check(axhel_cuda_ntt_inverse_batch(hs.data(), n_ntts, out.dev, a, count, 2, output_mod_factor, stream()),
           "ComputeInverseRNS");

@@ -19,8 +19,8 @@ def cuda_include():
 
 
 # Host operands take three routes: small ones are read and written by the
-# kernels in the mapped pinned buffers (by default up to 256 KiB, 128 KiB
-# for the forward transform), larger
+# kernels in the mapped pinned buffers (by default up to 512 KiB for
+# element-wise calls, 256 / 128 KiB for the inverse / forward transform), larger
 # ones go by DMA through the pinned buffers, or, with pinned staging off,
 # straight from the pageable memory.
 STAGING = {
