@@ -48,7 +48,8 @@ constexpr size_t kPinnedStagingMax = size_t(1) << 30;
 // Default bounds for operands the kernels access in the pinned buffers
 // directly (no DMA copy).  Element-wise kernels read and write them once in
 // contiguous runs: 512 KiB (MulMod at N = 2^16: 105 against 120 us per call
-// by DMA).  The inverse transform reads contiguous rows, but from 2^16 words
+// by DMA; at 2^17 the mapped route gains 3 % on one thread and loses 20 %
+// with eight threads calling).  The inverse transform reads contiguous rows, but from 2^16 words
 // it runs as two passes over the buffers: 256 KiB.  The forward transform's
 // first pass reads strided columns, short PCIe requests that cost more than
 // a DMA copy from 2^15 words up (with eight threads calling, 210 against
