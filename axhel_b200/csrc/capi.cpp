@@ -434,6 +434,16 @@ axhel_status_t run_plan(bool inverse, const NttPlan& plan, PassArgs a, const uin
 // `mul` (optional): the dyadic product with it fused into the transform --
 // ahead of an inverse (MulMod<4> on load, so inputs in [0, 4q)) or after a
 // forward (MulMod<4> of the lazy [0, 4q) output; canonical result).
+// A cluster launch the GPU cannot place (a cluster needs its CTAs on the SMs
+// of one GPC at once; a partitioned or smaller GPU may not have them): the
+// caller falls back to the pass kernels.  Clears the error.
+bool cluster_unschedulable(cudaError_t e)
+{
+    if (e != cudaErrorInvalidClusterSize) return false;  // "cluster misconfiguration"
+    cudaGetLastError();
+    return true;
+}
+
 axhel_status_t transform(bool inverse, const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* result,
                          const uint64_t* operand, uint64_t count, uint64_t in_f, uint64_t out_f, bool batch_api,
                          void* stream, const uint64_t* mul = nullptr)
@@ -471,7 +481,10 @@ axhel_status_t transform(bool inverse, const axhel_ntt_t* ntts, uint64_t n_ntts,
         a.tg = 0;
         a.flags = first | last | kLastPass;
         const cudaError_t e = launch_ntt_cluster(inverse, cc, a, S(stream));
-        return e == cudaSuccess ? AXHEL_OK : cuda_fail(e, inverse ? "inverse NTT (cluster)" : "forward NTT (cluster)");
+        if (e == cudaSuccess) return AXHEL_OK;
+        if (!cluster_unschedulable(e))
+            return cuda_fail(e, inverse ? "inverse NTT (cluster)" : "forward NTT (cluster)");
+        // the GPU cannot place the cluster (fewer SMs per GPC): the pass form
     }
     const NttPlan plan = plan_for(inverse, a.logn, count);
     return run_plan(inverse, plan, a, operand, result, first, last, S(stream));
@@ -503,7 +516,8 @@ axhel_status_t chain(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* result,
         if (op == kChainFma)
             for (uint64_t i = 0; i < n_ntts; ++i) c.scalar[i] = scalars[i];
         const cudaError_t e = launch_ntt_cluster_fused(false, cc, c, S(stream));
-        return e == cudaSuccess ? AXHEL_OK : cuda_fail(e, "chain (cluster)");
+        if (e == cudaSuccess) return AXHEL_OK;
+        if (!cluster_unschedulable(e)) return cuda_fail(e, "chain (cluster)");
     }
     const NttPlan inv = plan_for(true, logn, count);
     // forward passes after the fused one: the inverse's earlier passes, reversed
@@ -588,7 +602,8 @@ axhel_status_t product(const axhel_ntt_t* ntts, uint64_t n_ntts, uint64_t* resul
         c.op = kChainMul;
         c.op_factor = 4;
         const cudaError_t e = launch_ntt_cluster_fused(true, cc, c, S(stream));
-        return e == cudaSuccess ? AXHEL_OK : cuda_fail(e, "product (cluster)");
+        if (e == cudaSuccess) return AXHEL_OK;
+        if (!cluster_unschedulable(e)) return cuda_fail(e, "product (cluster)");
     }
     const NttPlan inv = plan_for(true, logn, count);
     cudaStream_t s = S(stream);
